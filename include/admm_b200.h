@@ -1,0 +1,217 @@
+/*
+ * admm_b200.h -- C ABI of the B200 ADMM substep backend (libadmm_b200.so).
+ *
+ * The library is a drop-in for the reference's GPU ADMM backend
+ * (ADMMBackendGPU / ADMMImplGPU, src/solver/backend_gpu/admm_backend_gpu.h:13,
+ * src/solver/backend_gpu/admm_impl_gpu.h:38) and its GPU collision detector
+ * (BVH_GPU, src/contact/collision_detection_cuda.h:45).  Every entry point takes
+ * plain pointers and sizes; host float buffers are row-major N x 3, the same
+ * bytes as ADU::Matf_X3::data() (src/mutils/common_types.h:20,33).
+ *
+ * Every call returns 0 on success or a negative ADMM_ERR_* code; nothing in the
+ * library exits the process (the reference exits on CUDA errors,
+ * src/mutils/cuda_tools.cuh:37-46).  One handle owns one CUDA stream and all of
+ * its device memory; calls on one handle must be serialised by the caller,
+ * different handles are independent.
+ */
+#ifndef ADMM_B200_H
+#define ADMM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ADMM_B200_ABI_VERSION 1
+
+/* status codes */
+#define ADMM_OK                    0
+#define ADMM_ERR_INVALID          -1  /* bad argument / inconsistent description      */
+#define ADMM_ERR_CUDA             -2  /* a CUDA runtime call failed                    */
+#define ADMM_ERR_OOM              -3  /* device allocation failed                      */
+#define ADMM_ERR_CONTACT_OVERFLOW -4  /* more contacts than max_contacts (clamped)     */
+#define ADMM_ERR_STACK_OVERFLOW   -5  /* BVH traversal stack depth exceeded            */
+#define ADMM_ERR_NAN              -6  /* non-finite value in the state                 */
+#define ADMM_ERR_NOT_CONVERGED    -7  /* residual tolerance not reached at max_iter    */
+#define ADMM_ERR_NO_DEVICE        -8  /* no usable sm_100 device                       */
+#define ADMM_ERR_STATE            -9  /* call out of order (e.g. step before create)   */
+
+typedef struct AdmmB200 AdmmB200; /* opaque handle */
+
+/*
+ * Scene / constraint description.  Mirrors what ADMMImplGPU receives through
+ * Solver::init(verts, mass, dt) (src/solver/solver.h:66-90),
+ * add_constraints/addPins (solver.h:96,150), ADMMSolverConfig
+ * (src/solver/core/admm_config.h:13-54) and the BVH_GPU geometry
+ * (collision_detection_cuda.cpp:39-83).  Constraint rows are laid out as in
+ * mesh_to_constraint.h:94-151: each type occupies a contiguous block of rows
+ * starting at *_start_row (tri 2 rows, tet 3, bending 1, pin 1 per constraint).
+ * All pointers are host pointers; the library copies what it needs in create.
+ */
+typedef struct AdmmB200Desc {
+    int32_t abi_version;          /* ADMM_B200_ABI_VERSION */
+    int32_t n_vert;               /* all vertices, dynamic first               */
+    int32_t n_dyn;                /* static_vert_begin                         */
+    int32_t n_rows;               /* m_nCDim (set_constraint_dim)               */
+    const float*   x0;            /* [n_vert*3] initial positions               */
+    const float*   v0;            /* [n_vert*3] initial velocities, may be NULL */
+    const float*   mass;          /* [n_vert] lumped mass                       */
+    const int32_t* is_fixed;      /* [n_vert] 1 = pinned (addPins), may be NULL */
+    /* triangle strain (triangle_constraint.h:24-62) */
+    int32_t n_tri, tri_start_row;
+    const int32_t* tri_inds;      /* [n_tri*3] */
+    const float*   tri_binv;      /* [n_tri*4] row-major 2x2 Binv */
+    const float*   tri_w;         /* [n_tri]   w = sqrt(k*area)   */
+    /* tetrahedral strain (tetrahedral_constraint.h:22-56) */
+    int32_t n_tet, tet_start_row;
+    const int32_t* tet_inds;      /* [n_tet*4] */
+    const float*   tet_binv;      /* [n_tet*9] row-major 3x3 Binv */
+    const float*   tet_w;         /* [n_tet]   w = sqrt(k*volume) */
+    /* Laplacian bending (bending_constraint.h:24-78): CSR, entry 0 = middle vertex */
+    int32_t n_bend, bend_start_row;
+    const int32_t* bend_offsets;  /* [n_bend+1] */
+    const int32_t* bend_inds;     /* [bend_offsets[n_bend]] */
+    const float*   bend_coeffs;   /* [bend_offsets[n_bend]] D-row coefficients */
+    const float*   bend_rest_norm;/* [n_bend] rest mean-curvature norm, may be NULL (= 0) */
+    const float*   bend_w;        /* [n_bend] */
+    /* pins (pin_constraint.h:18-57) */
+    int32_t n_pin, pin_start_row;
+    const int32_t* pin_inds;      /* [n_pin] */
+    const float*   pin_pos;       /* [n_pin*3] */
+    const float*   pin_w;         /* [n_pin] w = sqrt(k) */
+    /* collision geometry (MeshData::surface_tris/_edges/_vinds) */
+    int32_t n_surf_tri, n_surf_edge, n_surf_vert;
+    const int32_t* surf_tris;     /* [n_surf_tri*3]  */
+    const int32_t* surf_edges;    /* [n_surf_edge*2] */
+    const int32_t* surf_verts;    /* [n_surf_vert]   */
+    const float*   contact_w;     /* [n_vert] w_c per vertex (solver_config_applier.cpp:34-47) */
+    /* tuning (ADMMSolverConfig) */
+    float dt, g, mu, kappa, beta, thickness;
+    int32_t admm_max_iter, dcd_interval, gs_max_iter, jacobi_iter;
+    int32_t max_contacts;         /* contact slots (dcd.narrow.max_collision) */
+    int32_t enable_contact, warmstart_ue, warmstart_uc;
+    /* convergence control (no reference counterpart: the reference never
+     * computes a residual, admm_impl_cpu.h:126,167).  residual_tol <= 0 runs
+     * exactly admm_max_iter iterations like ADMMImplGPU::step. */
+    float residual_tol;
+    int32_t residual_check_every;
+} AdmmB200Desc;
+
+/* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */
+typedef struct AdmmStepStats {
+    int64_t frame;
+    double  step_ms;          /* host wall time of the step call             */
+    int32_t n_contacts;       /* contacts of the last DCD of the step         */
+    int32_t admm_iters;       /* ADMM iterations run                          */
+    double  primal_residual;  /* FP64 reductions, see admm_b200_residuals     */
+    double  dual_residual;
+    int32_t status;           /* ADMM_OK or a warning code (overflow, ...)    */
+    int32_t peak_contacts;
+} AdmmStepStats;
+
+/* --- lifecycle ----------------------------------------------------------- */
+
+/* Replaces ADMMImplGPU::convert_constraint2device + init + precompute
+ * (admm_impl_gpu.cu:61-254) and BVH_GPU::init (collision_detection_cuda.cpp:39-83). */
+int  admm_b200_create(const AdmmB200Desc* desc, int device, AdmmB200** out);
+/* Frees the handle and every device buffer it owns. */
+void admm_b200_destroy(AdmmB200* h);
+/* Human-readable text of a status code. */
+const char* admm_b200_errstr(int code);
+/* Text of the last error on this handle (CUDA error string, argument name). */
+const char* admm_b200_last_error(const AdmmB200* h);
+
+/* --- stepping (IADMMBackend::step, admm_backend.h:17; ADMMImplGPU::step, admm_impl_gpu.cu:256-344) --- */
+
+/* Runs n_steps substeps on the handle's stream (graph-replayed after the first
+ * call).  stats may be NULL; when given it receives the last step's numbers
+ * (this synchronises the stream). */
+int  admm_b200_step(AdmmB200* h, int n_steps, AdmmStepStats* stats);
+/* Enqueue n_steps substeps without synchronising (no stats). */
+int  admm_b200_step_async(AdmmB200* h, int n_steps);
+/* Block until all work on the handle's stream is done. */
+int  admm_b200_sync(AdmmB200* h);
+
+/* --- state (Solver::getVertices/getVelocities, solver.h:120-138; ADMMImplGPU::reset, admm_impl_gpu.cu:151-155) --- */
+
+int  admm_b200_set_state(AdmmB200* h, const float* x_rowmajor, const float* v_rowmajor, int n);
+int  admm_b200_get_state(AdmmB200* h, float* x_rowmajor, float* v_rowmajor, int n);
+/* Restores the creation state and zeroes both dual variables. */
+int  admm_b200_reset(AdmmB200* h);
+/* Device pointers of the handle's row-major float4 state (x, v), for callers
+ * that keep data on the GPU; valid until destroy. */
+int  admm_b200_device_state(AdmmB200* h, void** x_float4, void** v_float4);
+
+/* --- ADMM internals, for parity tests and the fused dual/local step --- */
+
+#define ADMM_BUF_X        0  /* [n_vert]  current positions (x_curr)   */
+#define ADMM_BUF_X0       1  /* [n_vert]  step-start positions          */
+#define ADMM_BUF_V        2  /* [n_vert]  velocities                    */
+#define ADMM_BUF_P        3  /* [n_vert]  contact velocities p          */
+#define ADMM_BUF_UC       4  /* [n_dyn]   contact dual Uc               */
+#define ADMM_BUF_UE       5  /* [n_rows]  elastic dual Ue               */
+#define ADMM_BUF_Z        6  /* [n_rows]  prox output z                 */
+#define ADMM_BUF_B        7  /* [n_dyn]   global-step right-hand side   */
+#define ADMM_BUF_MXT      8  /* [n_vert]  M * x_tilde                   */
+/* Copy one N x 3 buffer (row-major floats) between host and device. */
+int  admm_b200_read_buffer(AdmmB200* h, int which, float* out_rowmajor, int n);
+int  admm_b200_write_buffer(AdmmB200* h, int which, const float* in_rowmajor, int n);
+
+/* One local step z = prox(D*x + Ue) on the current buffers
+ * (LocalProjectorGPU::project_elastic -> ADMMImplGPU::do_project_elastic,
+ * admm_impl_gpu.cu:52-59). */
+int  admm_b200_local_step(AdmmB200* h);
+/* The global step: b from z, Ue, p, Uc (admm_impl_gpu.cu:307-318), then
+ * jacobi_iter Jacobi sweeps on A (cu_jacobi_global, jacobi_solver.cu:141-180). */
+int  admm_b200_global_step(AdmmB200* h);
+/* Only the Jacobi sweeps on the current b and x (LinearSolverGPU::solve). */
+int  admm_b200_jacobi(AdmmB200* h, int sweeps);
+/* Pre-integration (do_pre_integration, jacobi_solver.cu:183-233). */
+int  admm_b200_pre_integration(AdmmB200* h);
+
+/* The contact sub-problem on the last detection (ADMMImplGPU::compute_Scc +
+ * project_feasible_parallel, admm_impl_gpu.cu:296-303 and contact_solver.cu:402-431):
+ * p = (x - x0 + Uc)/h, warm start, gs_max_iter friction-cone projections. */
+int  admm_b200_contact_step(AdmmB200* h);
+
+/* --- collision detection (ICollisionDetector, src/contact/icollision_detector.h:19-47) --- */
+
+/* LBVH build + DCD on the handle's current x (BVH_GPU::update(Real*) + dcd(),
+ * collision_detection_cuda.cpp:126-154) followed by the contact conversion
+ * (convert_DCD_info, contact_solver.cu:158-185).  *count receives the contact
+ * count (may exceed max_contacts, in which case ADMM_ERR_CONTACT_OVERFLOW is
+ * returned and only max_contacts are stored). */
+int  admm_b200_detect(AdmmB200* h, int* count);
+/* ICollisionDetector::detect(pos): upload host positions, then detect. */
+int  admm_b200_detect_host(AdmmB200* h, const float* x_rowmajor, int n, int* count);
+/* Contacts of the last detection: pairs (v,f0,f1,f2) for point-triangle or
+ * (e0a,e0b,e1a,e1b) for edge-edge, like BVH_GPU::d_collisonPairs; optional
+ * outputs may be NULL.  bary = float4 (contact_solver.cu:139-141), normal and
+ * point = float3, gap = h_cN. */
+int  admm_b200_contacts(AdmmB200* h, int32_t* pairs_int4, float* bary4, float* normal3,
+                        float* point3, float* gap, int cap, int* count);
+/* contact_count / max_slots / peak_contact_count / clear of ICollisionDetector. */
+int  admm_b200_contact_count(AdmmB200* h, int* count);
+int  admm_b200_max_slots(AdmmB200* h, int* slots);
+int  admm_b200_peak_contact_count(AdmmB200* h, int* peak);
+int  admm_b200_clear_contacts(AdmmB200* h);
+
+/* --- residuals (no reference counterpart) ---
+ * primal = sqrt(sum_rows |w (Dx - z)|^2 + sum_dyn |w_c (x - x0 - h p)|^2), FP64;
+ * dual   = sqrt(sum_rows |w (z - z_prev)|^2 + ...), FP64 on the GPU. */
+int  admm_b200_residuals(AdmmB200* h, double* primal, double* dual);
+
+/* --- timing --- */
+/* Device time (CUDA events on the handle's stream) of the last
+ * admm_b200_step call, and per-phase totals of kernel time when profiling is
+ * enabled with admm_b200_set_profiling. */
+int  admm_b200_last_step_device_ms(AdmmB200* h, float* ms);
+int  admm_b200_set_profiling(AdmmB200* h, int enabled);
+/* Number of kernels one substep launches (for launch accounting). */
+int  admm_b200_kernels_per_step(AdmmB200* h, int* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ADMM_B200_H */

@@ -1,0 +1,239 @@
+"""ctypes front-end of the oracle -- TEST INFRASTRUCTURE ONLY.
+
+The oracle (``liboracle_admm.so``, built from ``oracle/admm_oracle.cpp``) is a CPU
+restatement of the reference's GPU ADMM substep.  It is the checker of the CUDA
+library: only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this module.  ``ref_pin`` exposes the reference's own
+``svd_fast3.cuh`` / ``dist_g.cuh`` compiled on the host (``oracle/_ref``), when it
+has been built, for pinning the oracle.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_admm.so")
+REF_PIN_PATH = os.path.join(HERE, "_ref", "libref_pin.so")
+
+_lib = None
+_ref = None
+
+_f = ctypes.POINTER(ctypes.c_float)
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int32)
+
+
+def build(force: bool = False) -> None:
+    """Compile the oracle (and the reference pin library if the reference tree is present)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", HERE, "OCXX=g++"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_step.restype = ctypes.c_int
+        L.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_int, _d, _d, _i]
+        L.orc_reset.argtypes = [ctypes.c_void_p]
+        L.orc_read.argtypes = [ctypes.c_void_p, ctypes.c_int, _d, ctypes.c_int]
+        L.orc_write.argtypes = [ctypes.c_void_p, ctypes.c_int, _d, ctypes.c_int]
+        for fn in ("orc_local_step", "orc_pre_integration", "orc_rhs", "orc_contact_step"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p]
+        L.orc_jacobi.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_detect.restype = ctypes.c_int
+        L.orc_detect.argtypes = [ctypes.c_void_p]
+        L.orc_contacts.restype = ctypes.c_int
+        L.orc_contacts.argtypes = [ctypes.c_void_p, _i, _d, _d, _d, _d, ctypes.c_int]
+        L.orc_dcd.restype = ctypes.c_int
+        L.orc_dcd.argtypes = [_f, ctypes.c_int, _i, ctypes.c_int, _i, ctypes.c_int, _i, ctypes.c_int,
+                              ctypes.c_float, _i, _f, ctypes.c_int]
+        L.orc_svd3_d.argtypes = [_d, _d, _d, _d]
+        for fn in ("orc_prox_tet_d", "orc_prox_tri_d"):
+            getattr(L, fn).argtypes = [_d]
+        for fn in ("orc_prox_tet_f", "orc_prox_tri_f"):
+            getattr(L, fn).argtypes = [_f]
+        L.orc_dcd_pt_f.argtypes = [_f, _f, _f, _f, _f]
+        L.orc_dcd_ee_f.argtypes = [_f, _f, _f, _f, _f]
+        L.orc_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def ref_pin():
+    """The reference's own SVD / narrow phase compiled on the host, or None."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_PIN_PATH):
+            return None
+        R = ctypes.CDLL(REF_PIN_PATH)
+        R.ref_svd3.argtypes = [_f, _f, _f, _f]
+        R.ref_dcd_pt_f.argtypes = [_f, _f, _f, _f, _f]
+        R.ref_dcd_ee_f.argtypes = [_f, _f, _f, _f, _f]
+        _ref = R
+    return _ref
+
+
+def _p(a: np.ndarray, ct):
+    return a.ctypes.data_as(ct)
+
+
+class Oracle:
+    """Stateful oracle over the same scene description as the CUDA library."""
+
+    def __init__(self, desc_holder, double: bool = True):
+        self._holder = desc_holder  # keeps the numpy arrays behind the desc alive
+        self.h = lib().orc_create(ctypes.byref(desc_holder.desc), 1 if double else 0)
+        self.n_vert = desc_holder.desc.n_vert
+        self.n_dyn = desc_holder.desc.n_dyn
+        self.n_rows = desc_holder.desc.n_rows
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        pr = ctypes.c_double()
+        du = ctypes.c_double()
+        nc = ctypes.c_int32()
+        it = lib().orc_step(self.h, n, ctypes.byref(pr), ctypes.byref(du), ctypes.byref(nc))
+        return {"iters": it, "primal": pr.value, "dual": du.value, "n_contacts": nc.value}
+
+    def reset(self):
+        lib().orc_reset(self.h)
+
+    def rows(self, which: int) -> int:
+        from parallel_admm_b200 import backend as B
+        return {B.BUF_UC: self.n_dyn, B.BUF_B: self.n_dyn, B.BUF_UE: self.n_rows,
+                B.BUF_Z: self.n_rows}.get(which, self.n_vert)
+
+    def read(self, which: int) -> np.ndarray:
+        n = self.rows(which)
+        out = np.zeros((n, 3), np.float64)
+        if lib().orc_read(self.h, which, _p(out, _d), n) != 0:
+            raise ValueError("bad buffer")
+        return out
+
+    def write(self, which: int, a: np.ndarray):
+        n = self.rows(which)
+        a = np.ascontiguousarray(a, np.float64).reshape(n, 3)
+        if lib().orc_write(self.h, which, _p(a, _d), n) != 0:
+            raise ValueError("bad buffer")
+
+    def local_step(self):
+        lib().orc_local_step(self.h)
+
+    def pre_integration(self):
+        lib().orc_pre_integration(self.h)
+
+    def rhs(self):
+        lib().orc_rhs(self.h)
+
+    def jacobi(self, sweeps: int):
+        lib().orc_jacobi(self.h, sweeps)
+
+    def contact_step(self):
+        lib().orc_contact_step(self.h)
+
+    def detect(self) -> int:
+        return lib().orc_detect(self.h)
+
+    def contacts(self):
+        nc = lib().orc_contacts(self.h, None, None, None, None, None, 0)
+        pairs = np.zeros((max(nc, 1), 4), np.int32)
+        bary = np.zeros((max(nc, 1), 4))
+        nrm = np.zeros((max(nc, 1), 3))
+        pt = np.zeros((max(nc, 1), 3))
+        gap = np.zeros(max(nc, 1))
+        lib().orc_contacts(self.h, _p(pairs, _i), _p(bary, _d), _p(nrm, _d), _p(pt, _d), _p(gap, _d), nc)
+        return {"pairs": pairs[:nc], "bary": bary[:nc], "normal": nrm[:nc], "point": pt[:nc], "gap": gap[:nc]}
+
+
+def dcd(x: np.ndarray, surf_verts, surf_tris, surf_edges, thickness: float, cap: Optional[int] = None):
+    """All contact pairs (int4) on float32 positions, in the oracle's order."""
+    x = np.ascontiguousarray(x, np.float32)
+    sv = np.ascontiguousarray(surf_verts, np.int32)
+    st = np.ascontiguousarray(surf_tris, np.int32)
+    se = np.ascontiguousarray(surf_edges, np.int32)
+    L = lib()
+    n = L.orc_dcd(_p(x, _f), len(x), _p(sv, _i), len(sv), _p(st, _i), len(st), _p(se, _i), len(se),
+                  float(thickness), None, None, 0)
+    pairs = np.zeros((max(n, 1), 4), np.int32)
+    dist = np.zeros(max(n, 1), np.float32)
+    L.orc_dcd(_p(x, _f), len(x), _p(sv, _i), len(sv), _p(st, _i), len(st), _p(se, _i), len(se),
+              float(thickness), _p(pairs, _i), _p(dist, _f), n)
+    return pairs[:n], dist[:n]
+
+
+def dcd_pt(p, t0, t1, t2, ref: bool = False) -> np.ndarray:
+    out = np.zeros(11, np.float32)
+    args = [np.ascontiguousarray(a, np.float32) for a in (p, t0, t1, t2)]
+    fn = ref_pin().ref_dcd_pt_f if ref else lib().orc_dcd_pt_f
+    fn(*[_p(a, _f) for a in args], _p(out, _f))
+    return out
+
+
+def dcd_ee(p0, p1, q0, q1, ref: bool = False) -> np.ndarray:
+    out = np.zeros(11, np.float32)
+    args = [np.ascontiguousarray(a, np.float32) for a in (p0, p1, q0, q1)]
+    fn = ref_pin().ref_dcd_ee_f if ref else lib().orc_dcd_ee_f
+    fn(*[_p(a, _f) for a in args], _p(out, _f))
+    return out
+
+
+def svd3_ref(F: np.ndarray):
+    F = np.ascontiguousarray(F, np.float32).reshape(9)
+    U = np.zeros(9, np.float32)
+    S = np.zeros(3, np.float32)
+    V = np.zeros(9, np.float32)
+    ref_pin().ref_svd3(_p(F, _f), _p(U, _f), _p(S, _f), _p(V, _f))
+    return U.reshape(3, 3), S, V.reshape(3, 3)
+
+
+def svd3(F: np.ndarray):
+    F = np.ascontiguousarray(F, np.float64).reshape(9)
+    U = np.zeros(9)
+    S = np.zeros(3)
+    V = np.zeros(9)
+    lib().orc_svd3_d(_p(F, _d), _p(U, _d), _p(S, _d), _p(V, _d))
+    return U.reshape(3, 3), S, V.reshape(3, 3)
+
+
+def prox_tet(z9, double: bool = True) -> np.ndarray:
+    if double:
+        a = np.ascontiguousarray(z9, np.float64).copy()
+        lib().orc_prox_tet_d(_p(a, _d))
+    else:
+        a = np.ascontiguousarray(z9, np.float32).copy()
+        lib().orc_prox_tet_f(_p(a, _f))
+    return a
+
+
+def prox_tri(z6, double: bool = True) -> np.ndarray:
+    if double:
+        a = np.ascontiguousarray(z6, np.float64).copy()
+        lib().orc_prox_tri_d(_p(a, _d))
+    else:
+        a = np.ascontiguousarray(z6, np.float32).copy()
+        lib().orc_prox_tri_f(_p(a, _f))
+    return a
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()

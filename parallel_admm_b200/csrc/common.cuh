@@ -1,0 +1,60 @@
+// common.cuh -- shared device helpers for the B200 ADMM substep.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define ADMM_DEV __device__ __forceinline__
+
+namespace admm {
+
+constexpr int kWarp = 32;
+
+ADMM_DEV float4 f4(float x, float y, float z, float w = 0.f) { return make_float4(x, y, z, w); }
+ADMM_DEV float4 add3(float4 a, float4 b) { return f4(a.x + b.x, a.y + b.y, a.z + b.z); }
+ADMM_DEV float4 sub3(float4 a, float4 b) { return f4(a.x - b.x, a.y - b.y, a.z - b.z); }
+ADMM_DEV float4 scale3(float4 a, float s) { return f4(a.x * s, a.y * s, a.z * s); }
+ADMM_DEV float dot3(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Non-contracting operations: every call is one IEEE round-to-nearest float
+// operation, in the order written (the narrow phase must match the oracle bit
+// for bit, and the oracle is compiled with -ffp-contract=off).
+ADMM_DEV float fadd(float a, float b) { return __fadd_rn(a, b); }
+ADMM_DEV float fsub(float a, float b) { return __fsub_rn(a, b); }
+ADMM_DEV float fmul(float a, float b) { return __fmul_rn(a, b); }
+ADMM_DEV float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+ADMM_DEV float fsqrt(float a) { return __fsqrt_rn(a); }
+
+// float <-> order-preserving uint32 for atomicMin/atomicMax on floats
+ADMM_DEV uint32_t float_to_ordered(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+ADMM_DEV float ordered_to_float(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+template <class T>
+ADMM_DEV T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of a double; result valid in thread 0.  Uses blockDim.x/32
+// doubles of shared memory passed in by the caller.
+ADMM_DEV double block_sum(double v, double* sh) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        r = lane < nw ? sh[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+}  // namespace admm

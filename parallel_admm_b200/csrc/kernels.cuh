@@ -1,0 +1,393 @@
+// kernels.cuh -- per-iteration ADMM kernels (local step, dual updates, RHS,
+// Jacobi sweeps, integration, residuals).
+#pragma once
+#include "prox.cuh"
+#include "scene_dev.cuh"
+
+namespace admm {
+
+constexpr int kLocalThreads = 128;
+constexpr int kVertThreads = 128;
+
+// ---------------------------------------------------------------------------
+// Local step, fused with the elastic dual update of the previous iteration.
+//   LOCAL_DUAL : Ue += D x - z            (admm_impl_gpu.cu:322-324)
+//   LOCAL_PROX : z = prox(D x + Ue), y = z - Ue   (admm_impl_gpu.cu:52-59, 308)
+// D x is evaluated from the vertex positions directly: F = E * Binv for
+// triangles and tets (the rows of D are G = S * Binv, triangle_constraint.h:64-95,
+// tetrahedral_constraint.h:58-89), the stored coefficients for bending and 1 for
+// pins.  Blocks [0, tet_blocks) do tets, then triangles, bending, pins.
+// ---------------------------------------------------------------------------
+enum : int { LOCAL_PROX = 1, LOCAL_DUAL = 2 };
+
+template <int MODE, int NR>
+ADMM_DEV void finish_rows(const DevScene& s, int row, const float (&dx)[3 * NR], float (&zz)[3 * NR],
+                          float4 (&ue)[NR]) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        ue[r] = s.ue[row + r];
+        if (MODE & LOCAL_DUAL) {
+            const float4 zo = s.z[row + r];
+            ue[r].x = (dx[3 * r + 0] - zo.x) + ue[r].x;
+            ue[r].y = (dx[3 * r + 1] - zo.y) + ue[r].y;
+            ue[r].z = (dx[3 * r + 2] - zo.z) + ue[r].z;
+            ue[r].w = 0.f;
+        }
+        zz[3 * r + 0] = dx[3 * r + 0] + ue[r].x;
+        zz[3 * r + 1] = dx[3 * r + 1] + ue[r].y;
+        zz[3 * r + 2] = dx[3 * r + 2] + ue[r].z;
+    }
+}
+
+template <int MODE, int NR>
+ADMM_DEV void store_rows(const DevScene& s, int row, const float (&zz)[3 * NR], const float4 (&ue)[NR]) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        if (MODE & LOCAL_DUAL) s.ue[row + r] = ue[r];
+        if (MODE & LOCAL_PROX) {
+            const float4 zr = f4(zz[3 * r], zz[3 * r + 1], zz[3 * r + 2]);
+            s.z[row + r] = zr;
+            s.y[row + r] = f4(zr.x - ue[r].x, zr.y - ue[r].y, zr.z - ue[r].z);
+        }
+    }
+}
+
+ADMM_DEV void tet_dx(const float4* __restrict__ x, const DevScene& s, int c, float (&dx)[9]) {
+    const int4 id = s.tet_inds[c];
+    const float4 p0 = x[id.x], p1 = x[id.y], p2 = x[id.z], p3 = x[id.w];
+    const float4 e0 = sub3(p1, p0), e1 = sub3(p2, p0), e2 = sub3(p3, p0);
+    const float4 B0 = s.tet_b0[c], B1 = s.tet_b1[c], B2 = s.tet_b2[c];
+    const float b[3][3] = {{B0.x, B0.y, B0.z}, {B1.x, B1.y, B1.z}, {B2.x, B2.y, B2.z}};
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        dx[3 * r + 0] = e0.x * b[0][r] + e1.x * b[1][r] + e2.x * b[2][r];
+        dx[3 * r + 1] = e0.y * b[0][r] + e1.y * b[1][r] + e2.y * b[2][r];
+        dx[3 * r + 2] = e0.z * b[0][r] + e1.z * b[1][r] + e2.z * b[2][r];
+    }
+}
+
+ADMM_DEV void tri_dx(const float4* __restrict__ x, const DevScene& s, int c, float (&dx)[6]) {
+    const int4 id = s.tri_inds[c];
+    const float4 p0 = x[id.x], p1 = x[id.y], p2 = x[id.z];
+    const float4 e0 = sub3(p1, p0), e1 = sub3(p2, p0);
+    const float4 B = s.tri_binv[c];  // B00 B01 B10 B11
+    dx[0] = e0.x * B.x + e1.x * B.z;
+    dx[1] = e0.y * B.x + e1.y * B.z;
+    dx[2] = e0.z * B.x + e1.z * B.z;
+    dx[3] = e0.x * B.y + e1.x * B.w;
+    dx[4] = e0.y * B.y + e1.y * B.w;
+    dx[5] = e0.z * B.y + e1.z * B.w;
+}
+
+ADMM_DEV void bend_dx(const float4* __restrict__ x, const DevScene& s, int c, float (&dx)[3]) {
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    const int b = s.bend_off[c], e = s.bend_off[c + 1];
+    for (int k = b; k < e; k++) {
+        const float w = s.bend_coef[k];
+        const float4 p = x[s.bend_inds[k]];
+        ax += w * p.x;
+        ay += w * p.y;
+        az += w * p.z;
+    }
+    dx[0] = ax; dx[1] = ay; dx[2] = az;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kLocalThreads) k_local(DevScene s, int tet_blocks, int tri_blocks, int bend_blocks) {
+    int blk = blockIdx.x;
+    if (blk < tet_blocks) {
+        const int c = blk * kLocalThreads + threadIdx.x;
+        if (c >= s.ntet) return;
+        float dx[9], zz[9];
+        float4 ue[3];
+        tet_dx(s.x, s, c, dx);
+        const int row = s.tet_sr + 3 * c;
+        finish_rows<MODE, 3>(s, row, dx, zz, ue);
+        if (MODE & LOCAL_PROX) prox_tet(zz);
+        store_rows<MODE, 3>(s, row, zz, ue);
+        return;
+    }
+    blk -= tet_blocks;
+    if (blk < tri_blocks) {
+        const int c = blk * kLocalThreads + threadIdx.x;
+        if (c >= s.ntri) return;
+        float dx[6], zz[6];
+        float4 ue[2];
+        tri_dx(s.x, s, c, dx);
+        const int row = s.tri_sr + 2 * c;
+        finish_rows<MODE, 2>(s, row, dx, zz, ue);
+        if (MODE & LOCAL_PROX) prox_tri(zz);
+        store_rows<MODE, 2>(s, row, zz, ue);
+        return;
+    }
+    blk -= tri_blocks;
+    if (blk < bend_blocks) {
+        const int c = blk * kLocalThreads + threadIdx.x;
+        if (c >= s.nbend) return;
+        float dx[3], zz[3];
+        float4 ue[1];
+        bend_dx(s.x, s, c, dx);
+        const int row = s.bend_sr + c;
+        finish_rows<MODE, 1>(s, row, dx, zz, ue);
+        if (MODE & LOCAL_PROX) prox_bend(zz, s.bend_rest[c]);
+        store_rows<MODE, 1>(s, row, zz, ue);
+        return;
+    }
+    blk -= bend_blocks;
+    {
+        const int c = blk * kLocalThreads + threadIdx.x;
+        if (c >= s.npin) return;
+        const float4 p = s.x[s.pin_inds[c]];
+        float dx[3] = {p.x, p.y, p.z}, zz[3];
+        float4 ue[1];
+        const int row = s.pin_sr + c;
+        finish_rows<MODE, 1>(s, row, dx, zz, ue);
+        if (MODE & LOCAL_PROX) {
+            const float4 q = s.pin_pos[c];
+            zz[0] = q.x; zz[1] = q.y; zz[2] = q.z;
+        }
+        store_rows<MODE, 1>(s, row, zz, ue);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pre-integration (do_integration_kernel, jacobi_solver.cu:183-215), plus the
+// p <- v copy of the static range (admm_impl_gpu.cu:282).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kVertThreads) k_pre_integration(DevScene s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    float4 x0 = s.x0[i], v = s.v[i], x;
+    if (s.fixed[i] == 0) {
+        if (i < s.nd) {
+            v.y -= s.g * s.dt;
+            x = f4(x0.x + v.x * s.dt, x0.y + v.y * s.dt, x0.z + v.z * s.dt);
+        } else {
+            x = f4(x0.x, x0.y, x0.z);
+        }
+    } else {
+        v = f4(0.f, 0.f, 0.f);
+        x = f4(x0.x, x0.y, x0.z);
+    }
+    const float m = s.mass[i];
+    s.v[i] = v;
+    s.x[i] = x;
+    s.mxt[i] = f4(m * x.x, m * x.y, m * x.z);
+    if (i >= s.nd) s.p[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Contact velocities, fused with the contact dual update of the previous
+// iteration and the warm start of the contact projection:
+//   DUALC : Uc += (x - x0) - h p           (admm_impl_gpu.cu:326-331)
+//   p = ((x - x0) + Uc) / h                (admm_impl_gpu.cu:296-298)
+//   WARM  : p += sum_c Gamma_c,i r_c        (update_p_kernel, contact_solver.cu:316-335)
+// ---------------------------------------------------------------------------
+template <bool DUALC, bool WARM>
+__global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.nd) return;
+    const float4 x = s.x[i], x0 = s.x0[i];
+    float4 uc = s.uc[i];
+    if (DUALC) {
+        const float4 p = s.p[i];
+        uc.x = uc.x + ((x.x - x0.x) - p.x * s.dt);
+        uc.y = uc.y + ((x.y - x0.y) - p.y * s.dt);
+        uc.z = uc.z + ((x.z - x0.z) - p.z * s.dt);
+        s.uc[i] = uc;
+    }
+    float4 p = f4(((x.x - x0.x) + uc.x) * s.dt_inv, ((x.y - x0.y) + uc.y) * s.dt_inv,
+                  ((x.z - x0.z) + uc.z) * s.dt_inv);
+    if (WARM) {
+        const int b = s.vstart[i], e = s.vstart[i + 1];
+        for (int k = b; k < e; k++) {
+            const int slot = s.vlist[k];
+            const int c = slot >> 2;
+            const float4 gm = s.gamma[c];
+            const float g = (slot & 3) == 0 ? gm.x : (slot & 3) == 1 ? gm.y : (slot & 3) == 2 ? gm.z : gm.w;
+            const float4 r = s.rc[c];
+            p.x += g * r.x;
+            p.y += g * r.y;
+            p.z += g * r.z;
+        }
+    }
+    s.p[i] = p;
+}
+
+// ---------------------------------------------------------------------------
+// Right-hand side (admm_impl_gpu.cu:307-318):
+//   b = M x~ + h^2 D^T W^2 (z - Ue) [+ h^2 W_c (h p + x0 - Uc)]
+// as a gather over the sliced-ELL copy of h^2 D^T W^2.  SAVE_PREV also keeps
+// x before the solve (for the dual residual).
+// ---------------------------------------------------------------------------
+template <bool SAVE_PREV>
+__global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.nd) return;
+    const int sl = i / kSlice, lane = i % kSlice;
+    const int b = s.R.ptr[sl], e = s.R.ptr[sl + 1];
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int k = b + lane; k < e; k += kSlice) {
+        const int c = s.R.col[k];
+        if (c < 0) break;
+        const float w = s.R.val[k];
+        const float4 yy = s.y[c];
+        ax += w * yy.x;
+        ay += w * yy.y;
+        az += w * yy.z;
+    }
+    const float4 m = s.mxt[i];
+    float4 bi = f4(m.x + ax, m.y + ay, m.z + az);
+    if (s.contact) {
+        const float4 p = s.p[i], x0 = s.x0[i], uc = s.uc[i];
+        const float wc = s.dt2wc[i];
+        bi.x = bi.x + wc * ((p.x * s.dt + x0.x) - uc.x);
+        bi.y = bi.y + wc * ((p.y * s.dt + x0.y) - uc.y);
+        bi.z = bi.z + wc * ((p.z * s.dt + x0.z) - uc.z);
+    }
+    s.b[i] = bi;
+    if (SAVE_PREV) s.xprev[i] = s.x[i];
+}
+
+// ---------------------------------------------------------------------------
+// One Jacobi sweep (JacobiFunctor, jacobi_solver.cu:52-98):
+//   dst_i = (b_i - sum_{j != i} a_ij src_j) / a_ii
+// over the sliced-ELL copy of the off-diagonal part of A.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kVertThreads) k_jacobi(DevScene s, const float4* __restrict__ src,
+                                                         float4* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.nd) return;
+    const int sl = i / kSlice, lane = i % kSlice;
+    const int b = s.A.ptr[sl], e = s.A.ptr[sl + 1];
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int k = b + lane; k < e; k += kSlice) {
+        const int c = s.A.col[k];
+        if (c < 0) break;
+        const float w = s.A.val[k];
+        const float4 xx = src[c];
+        ax += xx.x * w;
+        ay += xx.y * w;
+        az += xx.z * w;
+    }
+    const float4 bi = s.b[i];
+    const float d = s.a_diag[i];
+    dst[i] = f4((bi.x - ax) / d, (bi.y - ay) / d, (bi.z - az) / d);
+}
+
+__global__ void k_copy_dyn(DevScene s, const float4* __restrict__ src, float4* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < s.nd) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// End of step: the last contact dual update, then do_post_process_kernel
+// (jacobi_solver.cu:236-252): v = (x - x0)/h on dynamic vertices, x0 = x.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kVertThreads) k_vertex_final(DevScene s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    const float4 x = s.x[i], x0 = s.x0[i];
+    if (i < s.nd) {
+        if (s.contact) {
+            const float4 p = s.p[i];
+            float4 uc = s.uc[i];
+            uc.x = uc.x + ((x.x - x0.x) - p.x * s.dt);
+            uc.y = uc.y + ((x.y - x0.y) - p.y * s.dt);
+            uc.z = uc.z + ((x.z - x0.z) - p.z * s.dt);
+            s.uc[i] = uc;
+        }
+        s.v[i] = f4((x.x - x0.x) * s.dt_inv, (x.y - x0.y) * s.dt_inv, (x.z - x0.z) * s.dt_inv);
+    }
+    s.x0[i] = f4(x.x, x.y, x.z);
+}
+
+// ---------------------------------------------------------------------------
+// Residuals, FP64, after the global solve of an iteration (before its dual
+// update).  With r_e = D x - z, r_c = x - x0 - h p (contact surface only):
+//   primal^2 = sum w^2 |D x - z|^2 + sum w_c |x - x0 - h p|^2
+//   dual^2   = sum w^2 |D (x - x_prev)|^2 + sum w_c |x - x_prev|^2
+//   scale^2  = sum w^2 |z|^2 + sum w_c |x - x0|^2
+// Accumulated into s.res[0..2] (zeroed by the caller).
+// ---------------------------------------------------------------------------
+template <int NR>
+ADMM_DEV void res_rows(const DevScene& s, int row, const float (&dx)[3 * NR], const float (&dp)[3 * NR],
+                       double& pr, double& du, double& sc) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        const double w = s.wrow[row + r];
+        const double w2 = w * w;
+        const float4 z = s.z[row + r];
+        const double e0 = (double)dx[3 * r] - z.x, e1 = (double)dx[3 * r + 1] - z.y, e2 = (double)dx[3 * r + 2] - z.z;
+        const double d0 = (double)dx[3 * r] - dp[3 * r], d1 = (double)dx[3 * r + 1] - dp[3 * r + 1],
+                     d2 = (double)dx[3 * r + 2] - dp[3 * r + 2];
+        pr += w2 * (e0 * e0 + e1 * e1 + e2 * e2);
+        du += w2 * (d0 * d0 + d1 * d1 + d2 * d2);
+        sc += w2 * ((double)z.x * z.x + (double)z.y * z.y + (double)z.z * z.z);
+    }
+}
+
+__global__ void __launch_bounds__(kLocalThreads) k_residual(DevScene s, int tet_blocks, int tri_blocks,
+                                                           int bend_blocks, int pin_blocks) {
+    __shared__ double sh[kLocalThreads / 32];
+    double pr = 0.0, du = 0.0, sc = 0.0;
+    int blk = blockIdx.x;
+    const float4* xp = s.xprev;
+    if (blk < tet_blocks) {
+        const int c = blk * kLocalThreads + threadIdx.x;
+        if (c < s.ntet) {
+            float dx[9], dp[9];
+            tet_dx(s.x, s, c, dx);
+            tet_dx(xp, s, c, dp);
+            res_rows<3>(s, s.tet_sr + 3 * c, dx, dp, pr, du, sc);
+        }
+    } else if ((blk -= tet_blocks) < tri_blocks) {
+        const int c = blk * kLocalThreads + threadIdx.x;
+        if (c < s.ntri) {
+            float dx[6], dp[6];
+            tri_dx(s.x, s, c, dx);
+            tri_dx(xp, s, c, dp);
+            res_rows<2>(s, s.tri_sr + 2 * c, dx, dp, pr, du, sc);
+        }
+    } else if ((blk -= tri_blocks) < bend_blocks) {
+        const int c = blk * kLocalThreads + threadIdx.x;
+        if (c < s.nbend) {
+            float dx[3], dp[3];
+            bend_dx(s.x, s, c, dx);
+            bend_dx(xp, s, c, dp);
+            res_rows<1>(s, s.bend_sr + c, dx, dp, pr, du, sc);
+        }
+    } else if ((blk -= bend_blocks) < pin_blocks) {
+        const int c = blk * kLocalThreads + threadIdx.x;
+        if (c < s.npin) {
+            const float4 a = s.x[s.pin_inds[c]], bp = xp[s.pin_inds[c]];
+            float dx[3] = {a.x, a.y, a.z}, dp[3] = {bp.x, bp.y, bp.z};
+            res_rows<1>(s, s.pin_sr + c, dx, dp, pr, du, sc);
+        }
+    } else {
+        blk -= pin_blocks;
+        const int i = blk * kLocalThreads + threadIdx.x;
+        if (s.contact && i < s.nd && s.dt2wc[i] > 0.f) {
+            const double w = s.cw[i];
+            const float4 x = s.x[i], x0 = s.x0[i], p = s.p[i], q = xp[i];
+            const double r0 = ((double)x.x - x0.x) - (double)s.dt * p.x;
+            const double r1 = ((double)x.y - x0.y) - (double)s.dt * p.y;
+            const double r2 = ((double)x.z - x0.z) - (double)s.dt * p.z;
+            const double d0 = (double)x.x - q.x, d1 = (double)x.y - q.y, d2 = (double)x.z - q.z;
+            const double s0 = (double)x.x - x0.x, s1 = (double)x.y - x0.y, s2 = (double)x.z - x0.z;
+            pr += w * (r0 * r0 + r1 * r1 + r2 * r2);
+            du += w * (d0 * d0 + d1 * d1 + d2 * d2);
+            sc += w * (s0 * s0 + s1 * s1 + s2 * s2);
+        }
+    }
+    pr = block_sum(pr, sh);
+    du = block_sum(du, sh);
+    sc = block_sum(sc, sh);
+    if (threadIdx.x == 0) {
+        atomicAdd(&s.res[0], pr);
+        atomicAdd(&s.res[1], du);
+        atomicAdd(&s.res[2], sc);
+    }
+}
+
+}  // namespace admm

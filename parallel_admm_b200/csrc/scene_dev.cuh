@@ -1,0 +1,102 @@
+// scene_dev.cuh -- device-side view of one ADMM scene (all pointers device).
+#pragma once
+#include "common.cuh"
+
+namespace admm {
+
+constexpr int kSlice = 32;          // sliced-ELL slice height (one warp)
+constexpr int kStackDepth = 64;     // BVH traversal stack (lbvh.cu:1698 uses 64)
+
+// Sliced ELL (Monakov et al. 2010): rows in slices of kSlice; slice s stores
+// width[s] columns column-major at ptr[s] (entry k of row r at ptr[s] + k*kSlice + r%kSlice).
+struct SlicedEll {
+    int rows = 0;
+    int nslices = 0;
+    const int* ptr = nullptr;    // [nslices+1] offsets (multiples of kSlice)
+    const int* col = nullptr;
+    const float* val = nullptr;
+};
+
+struct BvhDev {
+    int n = 0;                   // leaves
+    float4* box_lo = nullptr;    // [2n-1]: internal nodes [0, n-1), leaves [n-1, 2n-1)
+    float4* box_up = nullptr;
+    int* left = nullptr;         // [n-1]
+    int* right = nullptr;        // [n-1]
+    int* parent = nullptr;       // [2n-1]
+    int* leaf_elem = nullptr;    // [n] element id of sorted leaf i
+    uint32_t* flags = nullptr;   // [n-1] refit arrival counters
+    unsigned long long* keys = nullptr;   // [n] sort keys
+    unsigned long long* keys_alt = nullptr;
+    int* vals = nullptr;         // [n] element ids (sort payload)
+    int* vals_alt = nullptr;
+    float4* elem_lo = nullptr;   // [n] unsorted element boxes
+    float4* elem_up = nullptr;
+    uint32_t* scene = nullptr;   // [6] ordered-float min xyz, max xyz
+};
+
+struct DevScene {
+    int n = 0, nd = 0, m = 0;
+    int ntri = 0, ntet = 0, nbend = 0, npin = 0;
+    int tri_sr = 0, tet_sr = 0, bend_sr = 0, pin_sr = 0;
+    float dt = 0, dt_inv = 0, g = 0, mu = 0, eps = 0, gam = 0, thickness = 0;
+    int contact = 0;
+    // vertex state (float4 rows, w unused)
+    float4 *x = nullptr, *x0 = nullptr, *v = nullptr, *p = nullptr, *mxt = nullptr;
+    float4 *b = nullptr, *uc = nullptr, *xprev = nullptr, *jac[2] = {nullptr, nullptr};
+    const float* mass = nullptr;
+    const int* fixed = nullptr;
+    const float* dt2wc = nullptr;    // [nd] h^2 w_c (0 off the contact surface)
+    const float* cw = nullptr;       // [n] w_c
+    const float* cwinv = nullptr;    // [n] 1/w_c (0 for static vertices)
+    // constraints
+    const int4* tri_inds = nullptr;
+    const float4* tri_binv = nullptr;     // (B00, B01, B10, B11)
+    const int4* tet_inds = nullptr;
+    const float4* tet_b0 = nullptr;       // Binv rows (xyz)
+    const float4* tet_b1 = nullptr;
+    const float4* tet_b2 = nullptr;
+    const int* bend_off = nullptr;
+    const int* bend_inds = nullptr;
+    const float* bend_coef = nullptr;
+    const float* bend_rest = nullptr;
+    const int* pin_inds = nullptr;
+    const float4* pin_pos = nullptr;
+    const float* wrow = nullptr;          // [m] w per row
+    float4 *z = nullptr, *ue = nullptr, *y = nullptr;   // y = z - Ue
+    // matrices
+    SlicedEll A;                          // off-diagonal part of the system matrix
+    const float* a_diag = nullptr;
+    SlicedEll R;                          // h^2 D^T W^2 (rows = dynamic vertices)
+    // contacts
+    int cap = 0;
+    int* nc = nullptr;                    // [1] device contact count (clamped to cap)
+    int* nc_raw = nullptr;                // [1] unclamped count
+    int* err = nullptr;                   // [4] error flags: overflow, stack, nan
+    int4* pairs = nullptr;
+    float4* bary = nullptr;
+    float4* nrm = nullptr;                // normal xyz, w = h_cN - thickness
+    float4* point = nullptr;
+    float4* gamma = nullptr;              // Gamma_c per contact slot
+    float4* kc = nullptr;
+    float4* rc = nullptr;
+    float4* du = nullptr;
+    int* vcnt = nullptr;                  // [n] contacts per vertex
+    int* vfill = nullptr;                 // [n]
+    int* vstart = nullptr;                // [n+1]
+    int* vlist = nullptr;                 // [4*cap] contact*4 + slot, sorted per vertex
+    // collision geometry
+    int nst = 0, nse = 0, nsv = 0;
+    const int4* st = nullptr;             // surface triangles (w unused)
+    const int2* se = nullptr;             // surface edges
+    const int* sv = nullptr;              // surface vertices
+    BvhDev bf, be;                        // face tree, edge tree
+    int* qcount = nullptr;                // [nsv + nse] per-query pair counts
+    int* qoff = nullptr;                  // [nsv + nse + 1] exclusive offsets
+    int* scan_tmp = nullptr;              // block sums for scans
+    // residuals: [0] primal^2, [1] dual^2, [2] scale^2
+    double* res = nullptr;
+    int* done = nullptr;
+};
+
+}  // namespace admm

@@ -1,0 +1,270 @@
+"""Parity of the CUDA substep (through the C ABI) against the oracle.
+
+Tolerances (FP32 kernels against the FP64 oracle, on the same inputs):
+* local step z, global step x, contact p: max |err| <= 1e-5 * max(1, max|ref|)
+  (the per-step bound of the spec);
+* one full substep: positions within 1e-5 relative (max |dx| / extent of the body);
+* 20 substeps with contact: within 1e-3 relative;
+* contact pair sets on identical float positions: identical (bit-exact integer sets).
+"""
+import numpy as np
+import pytest
+
+from parallel_admm_b200 import backend as B
+from parallel_admm_b200 import scene
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-5
+TOL_LONG = 1e-3
+
+
+def _setup(sc, **over):
+    from oracle import oracle as O
+    h = B.Handle(sc, **over)
+    o = O.Oracle(h.holder, double=True)
+    return h, o
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b).max() / max(1.0, np.abs(b).max())
+
+
+def _perturbed(sc, amp, seed=0):
+    rng = np.random.default_rng(seed)
+    x = sc.verts.astype(np.float64).copy()
+    x[:sc.n_dyn] += rng.normal(scale=amp, size=(sc.n_dyn, 3))
+    return x
+
+
+def _crumpled_cloth(nx=24, seed=3):
+    """A cloth folded onto itself so that PT and EE contacts exist."""
+    sc = scene.cloth_on_box(nx, seed=seed)
+    x = sc.verts.astype(np.float64).copy()
+    n = sc.n_dyn
+    u = x[:n, 0] - x[:n, 0].min()
+    # fold along x: second half lifted and mirrored over the first half
+    fold = u > 0.5 * u.max()
+    x[:n, 0] = np.where(fold, x[:n, 0].min() + u.max() - u, x[:n, 0])
+    x[:n, 1] = np.where(fold, x[:n, 1] + sc.params.thickness * 0.6, x[:n, 1])
+    rng = np.random.default_rng(seed)
+    x[:n] += rng.normal(scale=sc.params.thickness * 0.2, size=(n, 3))
+    return sc, x.astype(np.float32)
+
+
+@pytest.mark.parametrize("name", ["cloth", "cube"])
+def test_local_step_parity(name):
+    sc = scene.cloth_on_box(32) if name == "cloth" else scene.cube_on_ground(12)
+    h, o = _setup(sc)
+    x = _perturbed(sc, 2e-3, seed=1)
+    rng = np.random.default_rng(2)
+    ue = rng.normal(scale=1e-2, size=(sc.n_rows, 3))
+    for tgt in (h, o):
+        tgt.write(B.BUF_X, x)
+        tgt.write(B.BUF_UE, ue)
+        tgt.local_step()
+    zg = h.read(B.BUF_Z)
+    zo = o.read(B.BUF_Z)
+    assert np.isfinite(zg).all()
+    assert _rel(zg, zo) <= TOL_STEP, _rel(zg, zo)
+
+
+@pytest.mark.parametrize("name", ["cloth", "cube"])
+def test_global_step_parity(name):
+    sc = scene.cloth_on_box(32) if name == "cloth" else scene.cube_on_ground(12)
+    h, o = _setup(sc)
+    o.pre_integration()
+    o.write(B.BUF_X, _perturbed(sc, 1e-3, seed=4) + (o.read(B.BUF_X) - sc.verts))
+    o.local_step()
+    rng = np.random.default_rng(5)
+    o.write(B.BUF_UC, rng.normal(scale=1e-3, size=(sc.n_dyn, 3)))
+    p = np.zeros((sc.n_vert, 3))
+    p[:sc.n_dyn] = rng.normal(scale=0.1, size=(sc.n_dyn, 3))
+    o.write(B.BUF_P, p)
+    for b in (B.BUF_X, B.BUF_X0, B.BUF_V, B.BUF_P, B.BUF_UC, B.BUF_UE, B.BUF_Z, B.BUF_MXT):
+        h.write(b, o.read(b))
+    h.global_step()
+    o.rhs()
+    o.jacobi(sc.params.jacobi_iter)
+    assert _rel(h.read(B.BUF_B), o.read(B.BUF_B)) <= TOL_STEP
+    assert _rel(h.read(B.BUF_X), o.read(B.BUF_X)) <= TOL_STEP
+
+
+def _pairset(pairs, canon=True):
+    out = set()
+    for p in np.asarray(pairs):
+        out.add(tuple(int(v) for v in p))
+    return out
+
+
+@pytest.mark.parametrize("case", ["cloth_fold", "cube_squeezed", "cloth_flat_on_box"])
+def test_dcd_pairs_bitexact(case):
+    from oracle import oracle as O
+    if case == "cloth_fold":
+        sc, x = _crumpled_cloth()
+    elif case == "cube_squeezed":
+        sc = scene.cube_on_ground(10)
+        x = sc.verts.copy()
+        # squash the cube into the ground so that PT and EE contacts appear
+        x[:sc.n_dyn, 1] = (x[:sc.n_dyn, 1] - x[:sc.n_dyn, 1].min()) * 0.5 - 0.25 * sc.params.thickness
+        rng = np.random.default_rng(7)
+        x[:sc.n_dyn] += rng.normal(scale=0.2 * sc.params.thickness, size=(sc.n_dyn, 3)).astype(np.float32)
+    else:
+        sc = scene.cloth_on_box(32)
+        x = sc.verts.copy()
+        x[:sc.n_dyn, 1] = 0.5 + 0.5 * sc.params.thickness  # lying on the box top
+    x = np.ascontiguousarray(x, np.float32)
+    h = B.Handle(sc)
+    n = h.detect(x)
+    ref_pairs, _ = O.dcd(x, sc.surf_verts, sc.surf_tris, sc.surf_edges, sc.params.thickness)
+    assert n == len(ref_pairs)
+    assert n > 0
+    got = h.contacts()
+    assert _pairset(got["pairs"]) == _pairset(ref_pairs)
+    assert len(_pairset(got["pairs"])) == n  # no duplicates
+
+
+def test_contact_conversion_and_step_parity():
+    sc, x = _crumpled_cloth()
+    h, o = _setup(sc)
+    x64 = x.astype(np.float64)
+    rng = np.random.default_rng(11)
+    uc = rng.normal(scale=1e-4, size=(sc.n_dyn, 3))
+    for tgt in (h, o):
+        tgt.write(B.BUF_X, x64)
+        tgt.write(B.BUF_UC, uc)
+    n = h.detect()
+    assert n == o.detect() and n > 0
+    gc, oc = h.contacts(), o.contacts()
+    # align by pair tuple
+    gi = {tuple(p): i for i, p in enumerate(gc["pairs"].tolist())}
+    perm = np.array([gi[tuple(p)] for p in oc["pairs"].tolist()])
+    assert np.abs(gc["bary"][perm] - oc["bary"]).max() <= 1e-5
+    assert np.abs(gc["normal"][perm] - oc["normal"]).max() <= 1e-4
+    assert np.abs(gc["gap"][perm] - oc["gap"]).max() <= 1e-6
+    h.contact_step()
+    o.contact_step()
+    pg, po = h.read(B.BUF_P), o.read(B.BUF_P)
+    assert _rel(pg[:sc.n_dyn], po[:sc.n_dyn]) <= 1e-4
+
+
+def test_full_step_cloth_parity():
+    sc = scene.cloth_on_box(32)
+    h, o = _setup(sc)
+    ext = np.ptp(sc.verts[:sc.n_dyn], axis=0).max()
+    for k in range(3):
+        h.step(1)
+        o.step(1)
+        xg, _ = h.get_state()
+        xo = o.read(B.BUF_X0)
+        err = np.abs(xg - xo).max() / ext
+        assert err <= TOL_STEP * (k + 1), (k, err)
+
+
+def test_full_step_cube_contact_parity():
+    """The cube right at impact (1 m drop speed), FP32 GPU vs FP64 oracle."""
+    sc = scene.cube_on_ground(10, drop=0.0)
+    v0 = np.zeros_like(sc.verts)
+    v0[:sc.n_dyn, 1] = -np.sqrt(2 * 9.8 * 1.0)
+    x0 = sc.verts.copy()
+    x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.03
+    h, o = _setup(sc)
+    h.set_state(x0, v0)
+    o.write(B.BUF_X0, x0)
+    o.write(B.BUF_V, v0)
+    o.write(B.BUF_X, x0)
+    ext = np.ptp(x0[:sc.n_dyn], axis=0).max()
+    ncs = []
+    for k in range(4):
+        sg = h.step(1)
+        so = o.step(1)
+        ncs.append((sg["n_contacts"], so["n_contacts"]))
+        xg, vg = h.get_state()
+        xo = o.read(B.BUF_X0)
+        err = np.abs(xg - xo).max() / ext
+        assert err <= TOL_LONG, (k, err, ncs)
+    assert max(c[0] for c in ncs) > 0
+
+
+def test_long_run_cloth_1e3():
+    sc = scene.cloth_on_box(16)
+    h, o = _setup(sc)
+    h.step(20)
+    o.step(20)
+    xg, _ = h.get_state()
+    xo = o.read(B.BUF_X0)
+    ext = np.ptp(sc.verts[:sc.n_dyn], axis=0).max()
+    assert np.abs(xg - xo).max() / ext <= TOL_LONG
+
+
+def test_residuals_match_oracle():
+    sc = scene.cloth_on_box(16)
+    h, o = _setup(sc)
+    sg = h.step(2)
+    so = o.step(2)
+    for key in ("primal", "dual"):
+        a, b = sg[key], so[key]
+        assert np.isfinite(a)
+        assert abs(a - b) <= 0.05 * abs(b) + 1e-7, (key, a, b)
+
+
+def test_determinism_and_reset():
+    sc, _ = _crumpled_cloth(16)
+    h1 = B.Handle(sc)
+    h2 = B.Handle(sc)
+    h1.step(5)
+    h2.step(5)
+    a, _ = h1.get_state()
+    b, _ = h2.get_state()
+    assert np.array_equal(a, b)
+    h1.reset()
+    h1.step(5)
+    c, _ = h1.get_state()
+    assert np.array_equal(a, c)
+
+
+def test_contact_overflow_is_reported_and_clamped():
+    sc, x = _crumpled_cloth(16)
+    sc.params.max_contacts = 8
+    h = B.Handle(sc)
+    cnt = h.detect(x, allow=(B.ERR_CONTACT_OVERFLOW,))
+    assert cnt > 8
+    c = h.contacts()
+    assert len(c["pairs"]) == 8
+    st = h.step(1, allow=(B.ERR_CONTACT_OVERFLOW,))
+    assert st["n_contacts"] <= 8
+    assert np.isfinite(h.get_state()[0]).all()
+
+
+def test_no_contact_scene_and_contact_disabled():
+    sc = scene.cloth_on_box(8)
+    sc.params.enable_contact = False
+    h, o = _setup(sc)
+    h.step(2)
+    o.step(2)
+    assert np.abs(h.get_state()[0] - o.read(B.BUF_X0)).max() <= 1e-5
+
+
+def test_backend_contract_call_order():
+    sc = scene.cloth_on_box(8)
+    be = B.ADMMBackendB200()
+    be.apply_config(admm_max_iter=10)
+    be.add_constraints(sc)
+    be.addPins([0])
+    be.set_constraint_dim(sc.n_rows)
+    be.finalize_constraints()
+    be.init(sc.verts, sc.mass, sc.params.dt)
+    be.set_sync_to_host(False)
+    for _ in range(3):
+        be.step()
+    assert len(be.step_metrics) == 3
+    assert be.step_metrics[-1]["admm_iters"] == 10
+    v = be.getVertices()
+    assert v.shape == (sc.n_vert, 3) and np.isfinite(v).all()
+    det = be.collision_detector()
+    det.detect(be.getVertices())
+    assert det.points().shape == (det.max_slots(), 3)
+    be.reset()
+    assert np.allclose(be.getVertices(), sc.verts)
