@@ -1,0 +1,356 @@
+"""Benchmark of the B200 ADMM substep: simulated steps/s on one or more GPUs.
+
+Workload (default): the tetrahedralised cube, 20^3 cells (9261 vertices, 40000
+tets, 5 tets/cell, edge 0.5 m), dropped 1 m onto a ground quad, 30 ADMM
+iterations per substep, dt = 1/100 s, frames 0..K-1 of the drop (K = 200 by
+default: the whole 200-frame run, free fall, impact with thousands of contacts,
+rebound).  Synthetic, seeded scene (seed 0: E = 1.88e5, nu = 0.4).
+
+One "step" is one full substep (IADMMBackend::step): pre-integration, 30 ADMM
+iterations with a DCD (LBVH build + traversal) every 5 iterations, contact
+projection (10 Jacobi passes), 20 Jacobi sweeps of the global solve, dual
+updates, post-process -- replayed as one CUDA graph.  The scene's working set
+(~30 MB) fits in L2, so L2 is flushed (a 256 MiB write) between timed steps.
+
+Multi-GPU: the substep of one coupled body does not shard (contacts and the
+global solve couple every vertex every iteration), so --gpus N runs N
+independent replicas, one per rank, with no collective in the data path
+("scaling": "weak"); value = total steps of all ranks / max over ranks of the
+device time.
+
+`--impl reference` times the CPU restatement of the reference's GPU-backend
+algorithm (the oracle, OpenMP on all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "cube": dict(fn="cube_on_ground", kw=dict(n=20, seed=0),
+                 workload="tet cube 20^3 cells (9261 verts, 40000 tets), 1 m drop onto ground, "
+                          "30 ADMM iters/step, DCD every 5, dt=1/100"),
+    "cloth": dict(fn="cloth_on_box", kw=dict(nx=32, seed=0),
+                  workload="cloth 32x32 (1024 verts, 1922 tris) over a unit box, 20 ADMM iters/step, dt=1/200"),
+    "sheets": dict(fn="sheets_on_sphere", kw=dict(nx=512, layers=4, seed=0),
+                   workload="4 x 512^2 cloth sheets on a sphere r=0.3, 40 ADMM iters/step, dt=1/300"),
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_scene(cfg):
+    from parallel_admm_b200 import scene
+    c = CONFIGS[cfg]
+    return getattr(scene, c["fn"])(**c["kw"])
+
+
+def pair_nnz(sc):
+    """Off-diagonal non-zeros of A (vertex pairs coupled by a constraint)."""
+    pairs = set()
+
+    def add(ids):
+        ids = [int(i) for i in ids]
+        for a in ids:
+            for b in ids:
+                if a != b:
+                    pairs.add((a, b))
+    for t in sc.tet_inds:
+        add(t)
+    for t in sc.tri_inds:
+        add(t)
+    for c in range(len(sc.bend_w)):
+        add(sc.bend_inds[sc.bend_offsets[c]:sc.bend_offsets[c + 1]])
+    return len(pairs)
+
+
+def algorithmic_bytes(sc, kernel):
+    """Bytes one launch must move at minimum (each array touched once, FP32, gathers once per element)."""
+    n, nd, m = sc.n_vert, sc.n_dyn, sc.n_rows
+    if kernel == "local":
+        # per row: Ue r+w, z r+w, y w (12 B each); per tet: inds 16 + Binv 36; per tri: 12 + 16;
+        # bending: (ring+1)*(4 idx + 4 coef); pins: 4 + 12; x gathered once per vertex
+        ring = int(sc.bend_offsets[-1]) if len(sc.bend_w) else 0
+        return (60 * m + 52 * len(sc.tet_inds) + 28 * len(sc.tri_inds) + 8 * ring +
+                16 * len(sc.pin_inds) + 12 * nd)
+    if kernel == "jacobi":
+        nnz = pair_nnz(sc)
+        # diag 4 + b 12 + x_out 12 per row, (4 val + 4 col) per off-diagonal, x_in gathered once
+        return 28 * nd + 8 * nnz + 12 * nd
+    if kernel == "rhs":
+        nnz_d = 4 * 3 * len(sc.tet_inds) + 3 * 2 * len(sc.tri_inds) + int(
+            sc.bend_offsets[-1] if len(sc.bend_w) else 0) + len(sc.pin_inds)
+        return 8 * nnz_d + 12 * m + 12 * nd * 5
+    raise ValueError(kernel)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(sc, h, frames, stride):
+    """The oracle (FP32 restatement of the reference GPU-backend algorithm) on the host cores.
+
+    Stratified sample of the workload: the GPU replays frames 0..frames-1; at every
+    `stride`-th frame its full state (x, v, both duals) is copied into the oracle, which
+    is timed for one substep.  Returns steps/s over the sampled substeps.
+    """
+    from oracle import oracle as O
+    from parallel_admm_b200 import backend as B
+    o = O.Oracle(h.holder, double=False)
+    h.reset()
+    secs = 0.0
+    n = 0
+    for f in range(frames):
+        if f % stride == 0:
+            x, v = h.get_state()
+            for buf, a in ((B.BUF_X0, x), (B.BUF_X, x), (B.BUF_V, v), (B.BUF_UE, h.read(B.BUF_UE)),
+                           (B.BUF_UC, h.read(B.BUF_UC))):
+                o.write(buf, a.astype(np.float64))
+            t = time.perf_counter()
+            o.step(1)
+            secs += time.perf_counter() - t
+            n += 1
+        h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+    return n / secs, O.num_threads(), secs, n
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sc = make_scene(args.config)
+    from oracle import oracle as O
+    from parallel_admm_b200 import backend as B
+    holder = B.DescHolder(sc)
+    o = O.Oracle(holder, double=False)
+    o.step(min(args.warmup, 3))
+    o.reset()
+    k = min(args.steps, args.ref_steps)
+    t = time.perf_counter()
+    o.step(k)
+    dt = time.perf_counter() - t
+    value = k / dt
+    sample = f"frames 0..{k - 1} of the workload ({k} of {args.steps} steps; CPU time bounded)"
+    line = {
+        "impl": "reference", "metric": "sim steps/s (ADMM substep, fixed reference iteration counts)",
+        "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": k, "warmup": min(args.warmup, 3),
+        "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": {"workload": CONFIGS[args.config]["workload"]},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cube", choices=sorted(CONFIGS))
+    ap.add_argument("--probe", default="local", choices=["local", "jacobi", "rhs"])
+    ap.add_argument("--cpu-stride", type=int, default=10, help="CPU-baseline sample: one substep every N frames")
+    ap.add_argument("--ref-steps", type=int, default=200, help="cap on steps timed by --impl reference")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="also print a per-phase kernel-time breakdown")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from parallel_admm_b200 import backend as B
+
+    sc = make_scene(args.config)
+    h = B.Handle(sc, device=local)
+    h.set_probe(args.probe)
+    kernels = h.kernels_per_step()
+    for _ in range(args.warmup):
+        h.step(1, allow=(B.ERR_CONTACT_OVERFLOW,))
+    h.probe_time()
+    h.reset()
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    dev_ms = []
+    contacts = []
+    peak = 0
+    status = 0
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with ClockSampler(local) as clk:
+        barrier()
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            st = h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+            dev_ms.append(h.last_step_device_ms())
+            contacts.append(st["n_contacts"])
+            peak = max(peak, st["peak"])
+            status = status or st["status"]
+        barrier()
+    clocks = clk.summary()
+    probe_ms, probe_n = h.probe_time()
+    total_ms = float(np.sum(dev_ms))
+    t = torch.tensor([total_ms], device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_total_ms = float(t.item())
+    ms_per_step = max_total_ms / args.steps
+    value = world * args.steps / (max_total_ms / 1e3)
+
+    # end to end through the public C ABI: pinned host buffers in, one substep, host buffers out
+    h.reset()
+    x_in = torch.from_numpy(sc.verts.copy()).pin_memory().numpy()
+    v_in = torch.zeros((sc.n_vert, 3), dtype=torch.float32).pin_memory().numpy()
+    x_out = torch.zeros((sc.n_vert, 3), dtype=torch.float32).pin_memory().numpy()
+    v_out = torch.zeros((sc.n_vert, 3), dtype=torch.float32).pin_memory().numpy()
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h.step_host(x_in, v_in, x_out, v_out)
+        e2e_s += time.perf_counter() - t0
+        x_in[:] = x_out
+        v_in[:] = v_out
+    te = torch.tensor([e2e_s], device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps / float(te.item())
+    bytes_io = 2 * sc.n_vert * 3 * 4
+
+    phases = None
+    if args.profile and rank == 0:
+        h.reset()
+        h.set_profiling(True)
+        h.step(min(args.steps, 20), allow=(B.ERR_CONTACT_OVERFLOW,))
+        phases = h.phase_times()
+        h.set_profiling(False)
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    peak_gbs, peak_kind = load_peaks()
+    alg = algorithmic_bytes(sc, args.probe)
+    achieved = alg / (probe_ms * 1e-3) / 1e9 if probe_ms > 0 else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(args.config, {}).get(args.probe)
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        v, cores, secs, n = cpu_baseline(sc, h, args.steps, args.cpu_stride)
+        cpu = {"value": v, "unit": "steps/s", "cores": cores, "kind": "port",
+               "sample": f"{n} substeps, one at every {args.cpu_stride}th frame of frames 0..{args.steps - 1}, "
+                         f"each from the GPU run's state; {secs:.1f} s of CPU time (oracle FP32, OpenMP)"}
+    line = {
+        "metric": "sim steps/s (ADMM substep, fixed reference iteration counts)",
+        "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": CONFIGS[args.config]["workload"], "n_vert": sc.n_vert, "n_rows": sc.n_rows,
+                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) between timed steps",
+                   "contacts_mean": float(np.mean(contacts)), "contacts_peak": int(peak)},
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
+        "gpu_launches": kernels * args.steps,
+        "roofline": {"bound": "hbm", "kernel": args.probe, "achieved": achieved, "peak": peak_gbs,
+                     "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": (achieved / peak_gbs) if achieved else None, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg, "mean_launch_ms": probe_ms, "launches_timed": probe_n},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "status": status,
+    }
+    if phases is not None:
+        line["phases"] = phases
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

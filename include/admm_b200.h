@@ -96,6 +96,15 @@ typedef struct AdmmB200Desc {
      * exactly admm_max_iter iterations like ADMMImplGPU::step. */
     float residual_tol;
     int32_t residual_check_every;
+    /* BVH maintenance within a substep: 0 = full rebuild at every DCD (what
+     * BVH_GPU::update does, collision_detection_cuda.cpp:126-144); 1 = rebuild at
+     * the first DCD of a substep and refit the same tree at the later ones.  The
+     * contact set does not depend on the tree, only the traversal cost does. */
+    int32_t bvh_refit;
+    /* Lanes per row of the sliced-ELL matrices (1, 2, 4 or 8); 0 = chosen by the
+     * autotuner at create (cached per process and matrix shape, so handles of the
+     * same scene sum in the same order). */
+    int32_t ell_lanes;
 } AdmmB200Desc;
 
 /* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */
@@ -202,14 +211,53 @@ int  admm_b200_clear_contacts(AdmmB200* h);
  * dual   = sqrt(sum_rows |w (z - z_prev)|^2 + ...), FP64 on the GPU. */
 int  admm_b200_residuals(AdmmB200* h, double* primal, double* dual);
 
+/* --- host-buffer stepping (the reference's per-step host sync,
+ * ADMMImplGPU::step with sync_to_host, admm_impl_gpu.cu:337-340) ---
+ * Copies x_in/v_in (row-major n x 3, pinned host memory for full speed; v_in
+ * may be NULL = keep the device velocities) to the device, runs one substep and
+ * copies the new positions and velocities back into x_out/v_out.  Synchronous. */
+int  admm_b200_step_host(AdmmB200* h, const float* x_in, const float* v_in, float* x_out, float* v_out, int n);
+
 /* --- timing --- */
-/* Device time (CUDA events on the handle's stream) of the last
- * admm_b200_step call, and per-phase totals of kernel time when profiling is
- * enabled with admm_b200_set_profiling. */
+/* Phases of a substep (for admm_b200_phase_times). */
+#define ADMM_PHASE_PRE       0
+#define ADMM_PHASE_DCD       1
+#define ADMM_PHASE_LOCAL     2
+#define ADMM_PHASE_CONTACT   3
+#define ADMM_PHASE_RHS       4
+#define ADMM_PHASE_JACOBI    5
+#define ADMM_PHASE_RESIDUAL  6
+#define ADMM_PHASE_FINAL     7
+#define ADMM_NUM_PHASES      8
+/* Kernel classes that a graph probe can time (admm_b200_set_probe). */
+#define ADMM_KERNEL_NONE            0
+#define ADMM_KERNEL_LOCAL           1
+#define ADMM_KERNEL_JACOBI          2
+#define ADMM_KERNEL_RHS             3
+#define ADMM_KERNEL_CONTACT_DU      4
+#define ADMM_KERNEL_CONTACT_GATHER  5
+#define ADMM_KERNEL_DCD_VF          6
+#define ADMM_KERNEL_DCD_EE          7
+
+/* Device time (CUDA events on the handle's stream) per substep of the last
+ * admm_b200_step call. */
 int  admm_b200_last_step_device_ms(AdmmB200* h, float* ms);
+/* enabled = 1: later steps run eagerly (no graph) with one CUDA event pair per
+ * kernel launch; admm_b200_phase_times returns the summed kernel time and the
+ * launch count of each ADMM_PHASE_* since the last call (and resets them). */
 int  admm_b200_set_profiling(AdmmB200* h, int enabled);
+int  admm_b200_phase_times(AdmmB200* h, double* ms, int64_t* launches, int n_phases);
+/* Capture CUDA event pairs into the step graph around the launches of one
+ * ADMM_KERNEL_* class (the first 64 launches of a substep); after each
+ * synchronous admm_b200_step the durations are accumulated, and
+ * admm_b200_probe_time returns their mean (ms per launch) and count, then resets. */
+int  admm_b200_set_probe(AdmmB200* h, int kernel_class);
+int  admm_b200_probe_time(AdmmB200* h, double* mean_ms, int64_t* count);
 /* Number of kernels one substep launches (for launch accounting). */
 int  admm_b200_kernels_per_step(AdmmB200* h, int* n);
+/* Autotuner choices made at create: lanes per row of the sliced-ELL copies of
+ * A (Jacobi) and h^2 D^T W^2 (right-hand side), and the measured ms per launch. */
+int  admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float* ms_r);
 
 #ifdef __cplusplus
 }

@@ -34,6 +34,9 @@ ERR_NO_DEVICE = -8
 ERR_STATE = -9
 
 BUF_X, BUF_X0, BUF_V, BUF_P, BUF_UC, BUF_UE, BUF_Z, BUF_B, BUF_MXT = range(9)
+PHASES = ("pre", "dcd", "local", "contact", "rhs", "jacobi", "residual", "final")
+KERNELS = {"none": 0, "local": 1, "jacobi": 2, "rhs": 3, "contact_du": 4, "contact_gather": 5,
+           "dcd_vf": 6, "dcd_ee": 7}
 
 _f = ctypes.POINTER(ctypes.c_float)
 _i = ctypes.POINTER(ctypes.c_int32)
@@ -67,6 +70,7 @@ class AdmmB200Desc(ctypes.Structure):
         ("jacobi_iter", ctypes.c_int32), ("max_contacts", ctypes.c_int32),
         ("enable_contact", ctypes.c_int32), ("warmstart_ue", ctypes.c_int32), ("warmstart_uc", ctypes.c_int32),
         ("residual_tol", ctypes.c_float), ("residual_check_every", ctypes.c_int32),
+        ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32),
     ]
 
 
@@ -127,6 +131,8 @@ class DescHolder:
         d.enable_contact = int(p.enable_contact)
         d.warmstart_ue, d.warmstart_uc = int(p.warmstart_ue), int(p.warmstart_uc)
         d.residual_tol, d.residual_check_every = 0.0, 0
+        d.bvh_refit = int(p.bvh_refit)
+        d.ell_lanes = int(p.ell_lanes)
         for k, v in overrides.items():
             setattr(d, k, v)
         self.desc = d
@@ -174,6 +180,11 @@ def lib():
             "admm_b200_last_step_device_ms": (ctypes.c_int, [vp, _f]),
             "admm_b200_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
             "admm_b200_kernels_per_step": (ctypes.c_int, [vp, _i]),
+            "admm_b200_step_host": (ctypes.c_int, [vp, _f, _f, _f, _f, ctypes.c_int]),
+            "admm_b200_phase_times": (ctypes.c_int, [vp, _d, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]),
+            "admm_b200_set_probe": (ctypes.c_int, [vp, ctypes.c_int]),
+            "admm_b200_probe_time": (ctypes.c_int, [vp, _d, ctypes.POINTER(ctypes.c_int64)]),
+            "admm_b200_tuning": (ctypes.c_int, [vp, _i, _i, _f, _f]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -193,7 +204,8 @@ def exported_symbols():
         "admm_b200_contact_step", "admm_b200_detect", "admm_b200_detect_host", "admm_b200_contacts",
         "admm_b200_contact_count", "admm_b200_max_slots", "admm_b200_peak_contact_count",
         "admm_b200_clear_contacts", "admm_b200_residuals", "admm_b200_last_step_device_ms",
-        "admm_b200_set_profiling", "admm_b200_kernels_per_step",
+        "admm_b200_set_profiling", "admm_b200_kernels_per_step", "admm_b200_step_host",
+        "admm_b200_phase_times", "admm_b200_set_probe", "admm_b200_probe_time", "admm_b200_tuning",
     ]
 
 
@@ -329,6 +341,39 @@ class Handle:
         n = ctypes.c_int32()
         self.check(lib().admm_b200_kernels_per_step(self.h, ctypes.byref(n)), "kernels_per_step")
         return n.value
+
+    def step_host(self, x_in: np.ndarray, v_in: Optional[np.ndarray], x_out: np.ndarray,
+                  v_out: Optional[np.ndarray]) -> int:
+        """One substep from/to host arrays (pinned for full speed), copies inside the call."""
+        return self.check(lib().admm_b200_step_host(
+            self.h, _p(x_in), None if v_in is None else _p(v_in), _p(x_out),
+            None if v_out is None else _p(v_out), self.n_vert), "step_host",
+            allow=(ERR_CONTACT_OVERFLOW, ERR_STACK_OVERFLOW))
+
+    def set_profiling(self, on: bool):
+        self.check(lib().admm_b200_set_profiling(self.h, 1 if on else 0), "set_profiling")
+
+    def phase_times(self) -> Dict[str, Dict[str, float]]:
+        ms = (ctypes.c_double * len(PHASES))()
+        cnt = (ctypes.c_int64 * len(PHASES))()
+        self.check(lib().admm_b200_phase_times(self.h, ms, cnt, len(PHASES)), "phase_times")
+        return {p: {"ms": ms[i], "launches": cnt[i]} for i, p in enumerate(PHASES)}
+
+    def set_probe(self, kernel: str):
+        self.check(lib().admm_b200_set_probe(self.h, KERNELS[kernel]), "set_probe")
+
+    def probe_time(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        self.check(lib().admm_b200_probe_time(self.h, ctypes.byref(ms), ctypes.byref(n)), "probe_time")
+        return ms.value, n.value
+
+    def tuning(self) -> Dict[str, float]:
+        la, lr = ctypes.c_int32(), ctypes.c_int32()
+        ma, mr = ctypes.c_float(), ctypes.c_float()
+        self.check(lib().admm_b200_tuning(self.h, ctypes.byref(la), ctypes.byref(lr), ctypes.byref(ma),
+                                          ctypes.byref(mr)), "tuning")
+        return {"jacobi_lanes": la.value, "rhs_lanes": lr.value, "jacobi_ms": ma.value, "rhs_ms": mr.value}
 
     def max_slots(self) -> int:
         n = ctypes.c_int32()
@@ -480,6 +525,32 @@ class BVHB200:
         n = ctypes.c_int32()
         self._h.check(lib().admm_b200_contact_count(self._h.h, ctypes.byref(n)), "contact_count")
         return n.value
+
+    def step_host(self, x_in: np.ndarray, v_in: Optional[np.ndarray], x_out: np.ndarray,
+                  v_out: Optional[np.ndarray]) -> int:
+        """One substep from/to host arrays (pinned for full speed), copies inside the call."""
+        return self.check(lib().admm_b200_step_host(
+            self.h, _p(x_in), None if v_in is None else _p(v_in), _p(x_out),
+            None if v_out is None else _p(v_out), self.n_vert), "step_host",
+            allow=(ERR_CONTACT_OVERFLOW, ERR_STACK_OVERFLOW))
+
+    def set_profiling(self, on: bool):
+        self.check(lib().admm_b200_set_profiling(self.h, 1 if on else 0), "set_profiling")
+
+    def phase_times(self) -> Dict[str, Dict[str, float]]:
+        ms = (ctypes.c_double * len(PHASES))()
+        cnt = (ctypes.c_int64 * len(PHASES))()
+        self.check(lib().admm_b200_phase_times(self.h, ms, cnt, len(PHASES)), "phase_times")
+        return {p: {"ms": ms[i], "launches": cnt[i]} for i, p in enumerate(PHASES)}
+
+    def set_probe(self, kernel: str):
+        self.check(lib().admm_b200_set_probe(self.h, KERNELS[kernel]), "set_probe")
+
+    def probe_time(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        self.check(lib().admm_b200_probe_time(self.h, ctypes.byref(ms), ctypes.byref(n)), "probe_time")
+        return ms.value, n.value
 
     def max_slots(self) -> int:
         return self._h.max_slots()

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -51,6 +52,26 @@ struct AdmmB200 {
     float residual_tol = 0.f;
     int residual_every = 0;
     bool warmstart_ue = true, warmstart_uc = true;
+    bool bvh_refit = true;
+    // autotuner choices (lanes per row of the sliced-ELL matrices) and their times
+    int tune_lanes_a = 1, tune_lanes_r = 1;
+    float tune_ms_a = 0.f, tune_ms_r = 0.f;
+    // host-buffer stepping
+    float* stage = nullptr;    // [6n] row-major x then v
+    // profiling: eager launches with one event pair per launch, tagged by phase
+    bool profiling = false;
+    int phase = 0;
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<int> prof_phase;
+    int prof_used = 0;
+    double phase_ms[ADMM_NUM_PHASES] = {0};
+    int64_t phase_launches[ADMM_NUM_PHASES] = {0};
+    // probes: event pairs captured into the step graph around one kernel class
+    int probe_kernel = 0;
+    std::vector<cudaEvent_t> probe_ev;
+    int probe_used = 0;
+    double probe_ms = 0.0;
+    int64_t probe_n = 0;
 };
 
 namespace {
@@ -103,6 +124,16 @@ int dupload(AdmmB200* h, T** p, const T* src, size_t count) {
     return ADMM_OK;
 }
 
+template <class T>
+void dfree(AdmmB200* h, T* p) {
+    if (!p) return;
+    for (auto& a : h->allocs)
+        if (a == (void*)p) {
+            cudaFree(a);
+            a = nullptr;
+        }
+}
+
 #define TRY(x)                 \
     do {                       \
         int r_ = (x);          \
@@ -132,11 +163,52 @@ int alloc_bvh(AdmmB200* h, BvhDev& t, int n) {
 }
 
 // ------------------------------ enqueue helpers -----------------------------
-#define LAUNCH(kernel, grid, block, ...)                                   \
+constexpr int kMaxProfEvents = 1 << 14;
+constexpr int kMaxProbes = 64;
+
+// Event bookkeeping around one launch: profiling (eager) and graph probes.
+struct LaunchTimer {
+    AdmmB200* h;
+    int probe_id;
+    cudaEvent_t a = nullptr, b = nullptr;
+    bool prof = false, probe = false;
+    LaunchTimer(AdmmB200* hh, int pid) : h(hh), probe_id(pid) {
+        if (h->profiling && h->prof_used + 2 <= (int)h->prof_ev.size()) {
+            prof = true;
+            a = h->prof_ev[h->prof_used];
+            b = h->prof_ev[h->prof_used + 1];
+            h->prof_phase[h->prof_used / 2] = h->phase;
+            h->prof_used += 2;
+        } else if (!h->profiling && pid != 0 && pid == h->probe_kernel &&
+                   h->probe_used + 2 <= (int)h->probe_ev.size()) {
+            probe = true;
+            a = h->probe_ev[h->probe_used];
+            b = h->probe_ev[h->probe_used + 1];
+            h->probe_used += 2;
+        }
+        // inside stream capture only an external record becomes a timing node of the graph
+        if (a) cudaEventRecordWithFlags(a, h->stream, probe ? cudaEventRecordExternal : cudaEventRecordDefault);
+    }
+    ~LaunchTimer() {
+        if (b) cudaEventRecordWithFlags(b, h->stream, probe ? cudaEventRecordExternal : cudaEventRecordDefault);
+    }
+};
+
+#define LAUNCH_P(pid, kernel, grid, block, ...)                            \
     do {                                                                   \
+        LaunchTimer lt_(h, (pid));                                         \
         kernel<<<(grid), (block), 0, h->stream>>>(__VA_ARGS__);            \
         h->launch_counter++;                                               \
     } while (0)
+#define LAUNCH(kernel, grid, block, ...) LAUNCH_P(0, kernel, grid, block, __VA_ARGS__)
+
+void enqueue_refit(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tri) {
+    const int n = t.n;
+    if (n <= 0) return;
+    if (tri) LAUNCH(k_leaf_refresh<3>, blocks(n, 256), 256, h->s.x, elems, stride, t);
+    else LAUNCH(k_leaf_refresh<2>, blocks(n, 256), 256, h->s.x, elems, stride, t);
+    LAUNCH(k_refit, blocks(n, 256), 256, t);
+}
 
 void enqueue_build(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tri) {
     const int n = t.n;
@@ -145,6 +217,7 @@ void enqueue_build(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tr
     else LAUNCH(k_elem_boxes<2>, blocks(n, 256), 256, h->s.x, elems, stride, n, t);
     LAUNCH(k_morton, blocks(n, 256), 256, t);
     if (n > 1) {
+        LaunchTimer lt(h, 0);  // one timer around the 40 launches of the sort
         radix_sort(t.keys, t.vals, t.keys_alt, t.vals_alt, n, 64, h->hist, h->s.scan_tmp, h->stream);
         h->launch_counter += 8 * 5;
     }
@@ -153,28 +226,39 @@ void enqueue_build(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tr
 }
 
 // DCD + contact conversion + incidence lists + S_c / Gamma / K_c, all on device.
-void enqueue_dcd(AdmmB200* h) {
+// rebuild = false refits the trees of the previous build.
+void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
     DevScene& s = h->s;
-    LAUNCH(k_scene_init, 1, 32, s.bf, s.be);
-    enqueue_build(h, s.bf, (const int*)s.st, 4, true);
-    enqueue_build(h, s.be, (const int*)s.se, 2, false);
+    h->phase = ADMM_PHASE_DCD;
+    if (rebuild) {
+        LAUNCH(k_scene_init, 1, 32, s.bf, s.be);
+        enqueue_build(h, s.bf, (const int*)s.st, 4, true);
+        enqueue_build(h, s.be, (const int*)s.se, 2, false);
+    } else {
+        enqueue_refit(h, s.bf, (const int*)s.st, 4, true);
+        enqueue_refit(h, s.be, (const int*)s.se, 2, false);
+    }
     const int nq = s.nsv + s.nse;
     if (s.nsv > 0) LAUNCH(k_dcd_vf<false>, blocks(s.nsv, 128), 128, s);
     if (s.nse > 0) LAUNCH(k_dcd_ee<false>, blocks(s.nse, 128), 128, s);
     if (nq > 0) {
+        LaunchTimer lt(h, 0);
         exclusive_scan(s.qcount, s.qoff, nq, s.scan_tmp, s.nc_raw, h->stream);
         h->launch_counter += 3;
     } else {
         cudaMemsetAsync(s.nc_raw, 0, sizeof(int), h->stream);
     }
     LAUNCH(k_set_count, 1, 1, s);
-    if (s.nsv > 0) LAUNCH(k_dcd_vf<true>, blocks(s.nsv, 128), 128, s);
-    if (s.nse > 0) LAUNCH(k_dcd_ee<true>, blocks(s.nse, 128), 128, s);
+    if (s.nsv > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_dcd_vf<true>, blocks(s.nsv, 128), 128, s);
+    if (s.nse > 0) LAUNCH_P(ADMM_KERNEL_DCD_EE, k_dcd_ee<true>, blocks(s.nse, 128), 128, s);
     cudaMemsetAsync(s.vcnt, 0, sizeof(int) * s.n, h->stream);
     cudaMemsetAsync(s.vfill, 0, sizeof(int) * s.n, h->stream);
     LAUNCH(k_contact_count, h->contact_grid, kContactThreads, s);
-    exclusive_scan(s.vcnt, s.vstart, s.n, s.scan_tmp, s.vstart + s.n, h->stream);
-    h->launch_counter += 3;
+    {
+        LaunchTimer lt(h, 0);
+        exclusive_scan(s.vcnt, s.vstart, s.n, s.scan_tmp, s.vstart + s.n, h->stream);
+        h->launch_counter += 3;
+    }
     LAUNCH(k_contact_fill, h->contact_grid, kContactThreads, s);
     LAUNCH(k_contact_sort_lists, blocks(s.nd, kContactThreads), kContactThreads, s);
     LAUNCH(k_contact_scc, h->contact_grid, kContactThreads, s);
@@ -182,10 +266,12 @@ void enqueue_dcd(AdmmB200* h) {
 
 void enqueue_local(AdmmB200* h, int mode) {
     const int g = h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks;
+    h->phase = ADMM_PHASE_LOCAL;
     if (mode == LOCAL_PROX)
-        LAUNCH(k_local<LOCAL_PROX>, g, kLocalThreads, h->s, h->tet_blocks, h->tri_blocks, h->bend_blocks);
+        LAUNCH_P(ADMM_KERNEL_LOCAL, k_local<LOCAL_PROX>, g, kLocalThreads, h->s, h->tet_blocks, h->tri_blocks, h->bend_blocks);
     else if (mode == (LOCAL_PROX | LOCAL_DUAL))
-        LAUNCH(k_local<LOCAL_PROX | LOCAL_DUAL>, g, kLocalThreads, h->s, h->tet_blocks, h->tri_blocks, h->bend_blocks);
+        LAUNCH_P(ADMM_KERNEL_LOCAL, k_local<LOCAL_PROX | LOCAL_DUAL>, g, kLocalThreads, h->s, h->tet_blocks, h->tri_blocks,
+                 h->bend_blocks);
     else
         LAUNCH(k_local<LOCAL_DUAL>, g, kLocalThreads, h->s, h->tet_blocks, h->tri_blocks, h->bend_blocks);
 }
@@ -193,39 +279,164 @@ void enqueue_local(AdmmB200* h, int mode) {
 void enqueue_contact(AdmmB200* h, bool dual) {
     DevScene& s = h->s;
     const int vb = blocks(s.nd, kVertThreads);
+    h->phase = ADMM_PHASE_CONTACT;
     if (dual) LAUNCH((k_contact_p<true, true>), vb, kVertThreads, s);
     else LAUNCH((k_contact_p<false, true>), vb, kVertThreads, s);
     for (int g = 0; g < h->gs_iter; g++) {
-        LAUNCH(k_contact_du, h->contact_grid, kContactThreads, s);
-        LAUNCH(k_contact_gather, blocks(s.nd, kContactThreads), kContactThreads, s);
+        LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
+        LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, blocks(s.nd, kContactThreads), kContactThreads, s);
     }
+}
+
+// one Jacobi sweep with the tuned number of lanes per row
+void launch_jacobi(AdmmB200* h, const float4* src, float4* dst) {
+    DevScene& s = h->s;
+    const int g = blocks(s.A.nslices * 32, kVertThreads);
+    switch (s.A.lanes) {
+        case 1: LAUNCH_P(ADMM_KERNEL_JACOBI, k_jacobi<1>, g, kVertThreads, s, src, dst); break;
+        case 2: LAUNCH_P(ADMM_KERNEL_JACOBI, k_jacobi<2>, g, kVertThreads, s, src, dst); break;
+        case 4: LAUNCH_P(ADMM_KERNEL_JACOBI, k_jacobi<4>, g, kVertThreads, s, src, dst); break;
+        default: LAUNCH_P(ADMM_KERNEL_JACOBI, k_jacobi<8>, g, kVertThreads, s, src, dst); break;
+    }
+}
+
+void launch_rhs(AdmmB200* h, bool save_prev) {
+    DevScene& s = h->s;
+    const int g = blocks(s.R.nslices * 32, kVertThreads);
+#define RHS_CASE(T)                                                                          \
+    if (save_prev) LAUNCH_P(ADMM_KERNEL_RHS, (k_rhs<T, true>), g, kVertThreads, s);          \
+    else LAUNCH_P(ADMM_KERNEL_RHS, (k_rhs<T, false>), g, kVertThreads, s);
+    switch (s.R.lanes) {
+        case 1: RHS_CASE(1) break;
+        case 2: RHS_CASE(2) break;
+        case 4: RHS_CASE(4) break;
+        default: RHS_CASE(8) break;
+    }
+#undef RHS_CASE
 }
 
 void enqueue_jacobi(AdmmB200* h, int sweeps) {
     DevScene& s = h->s;
     const int vb = blocks(s.nd, kVertThreads);
+    h->phase = ADMM_PHASE_JACOBI;
     if (sweeps <= 0) return;
     if (sweeps == 1) {
-        LAUNCH(k_jacobi, vb, kVertThreads, s, s.x, s.jac[0]);
+        launch_jacobi(h, s.x, s.jac[0]);
         LAUNCH(k_copy_dyn, vb, kVertThreads, s, s.jac[0], s.x);
         return;
     }
     for (int k = 0; k < sweeps; k++) {
         const float4* src = k == 0 ? s.x : s.jac[(k - 1) & 1];
         float4* dst = k == sweeps - 1 ? s.x : s.jac[k & 1];
-        LAUNCH(k_jacobi, vb, kVertThreads, s, src, dst);
+        launch_jacobi(h, src, dst);
     }
 }
 
 void enqueue_global(AdmmB200* h, bool save_prev) {
-    const int vb = blocks(h->s.nd, kVertThreads);
-    if (save_prev) LAUNCH(k_rhs<true>, vb, kVertThreads, h->s);
-    else LAUNCH(k_rhs<false>, vb, kVertThreads, h->s);
+    h->phase = ADMM_PHASE_RHS;
+    launch_rhs(h, save_prev);
     enqueue_jacobi(h, h->jac_iter);
+}
+
+int upload_ell(AdmmB200* h, const HostCsr& c, int rows, int lanes, SlicedEll& out) {
+    HostEll e = csr_to_sliced_ell(c, rows, lanes);
+    int *p = nullptr, *cc = nullptr;
+    float* v = nullptr;
+    TRY(dupload(h, &p, e.ptr.data(), e.ptr.size()));
+    TRY(dupload(h, &cc, e.col.data(), e.col.size()));
+    TRY(dupload(h, &v, e.val.data(), e.val.size()));
+    out.rows = rows;
+    out.nslices = e.nslices;
+    out.lanes = lanes;
+    out.ptr = p;
+    out.col = cc;
+    out.val = v;
+    return ADMM_OK;
+}
+
+void free_ell(AdmmB200* h, SlicedEll& m) {
+    dfree(h, const_cast<int*>(m.ptr));
+    dfree(h, const_cast<int*>(m.col));
+    dfree(h, const_cast<float*>(m.val));
+    m = SlicedEll{};
+}
+
+// Autotuner: lanes per row (1, 2, 4, 8) of both sliced-ELL matrices, chosen by
+// timing 10 launches of each candidate on this device with this scene.  The
+// choice is cached per (device, matrix shape) for the life of the process so
+// that every handle of one scene sums in the same order; `fixed` > 0 skips the
+// search and uses that many lanes.
+struct TuneKey {
+    int device, which, rows;
+    int64_t nnz;
+    bool operator==(const TuneKey& o) const {
+        return device == o.device && which == o.which && rows == o.rows && nnz == o.nnz;
+    }
+};
+std::mutex g_tune_mu;
+std::vector<std::pair<TuneKey, std::pair<int, float>>> g_tune_cache;
+
+int time_ell(AdmmB200* h, int which, float* ms_per_launch) {
+    DevScene& s = h->s;
+    if (which == 0) launch_jacobi(h, s.x, s.jac[0]);
+    else launch_rhs(h, false);
+    CK(cudaEventRecord(h->ev0, h->stream));
+    for (int r = 0; r < 10; r++) {
+        if (which == 0) launch_jacobi(h, s.x, s.jac[0]);
+        else launch_rhs(h, false);
+    }
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    CK(cudaGetLastError());
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    *ms_per_launch = ms / 10.f;
+    return ADMM_OK;
+}
+
+int autotune_ell(AdmmB200* h, const Assembly& as, int fixed, int* chosen_a, int* chosen_r, float* ms_a, float* ms_r) {
+    DevScene& s = h->s;
+    const int cand[4] = {1, 2, 4, 8};
+    for (int which = 0; which < 2; which++) {
+        const HostCsr& c = which == 0 ? as.A : as.R;
+        SlicedEll& target = which == 0 ? s.A : s.R;
+        const TuneKey key{h->device, which, s.nd, (int64_t)c.col.size()};
+        int best_l = fixed;
+        float best = 0.f;
+        if (best_l == 0) {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            for (auto& e : g_tune_cache)
+                if (e.first == key) {
+                    best_l = e.second.first;
+                    best = e.second.second;
+                }
+        }
+        if (best_l == 0) {
+            best = 1e30f;
+            for (int k = 0; k < 4; k++) {
+                TRY(upload_ell(h, c, s.nd, cand[k], target));
+                float ms = 0.f;
+                TRY(time_ell(h, which, &ms));
+                free_ell(h, target);
+                if (ms < best) {
+                    best = ms;
+                    best_l = cand[k];
+                }
+            }
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune_cache.push_back({key, {best_l, best}});
+        }
+        TRY(upload_ell(h, c, s.nd, best_l, target));
+        if (best == 0.f) TRY(time_ell(h, which, &best));
+        if (which == 0) { *chosen_a = best_l; *ms_a = best; }
+        else { *chosen_r = best_l; *ms_r = best; }
+    }
+    return ADMM_OK;
 }
 
 void enqueue_residual(AdmmB200* h) {
     DevScene& s = h->s;
+    h->phase = ADMM_PHASE_RESIDUAL;
     cudaMemsetAsync(s.res, 0, sizeof(double) * 4, h->stream);
     const int vb = blocks(s.nd, kLocalThreads);
     const int g = h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks + vb;
@@ -235,23 +446,30 @@ void enqueue_residual(AdmmB200* h) {
 // One substep (ADMMImplGPU::step).  The residual of the last iteration is kept.
 void enqueue_step(AdmmB200* h) {
     DevScene& s = h->s;
+    h->phase = ADMM_PHASE_PRE;
     LAUNCH(k_pre_integration, blocks(s.n, kVertThreads), kVertThreads, s);
     if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->stream);
     if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->stream);
     for (int it = 0; it < h->admm_max_iter; it++) {
         const bool first = it == 0, last = it == h->admm_max_iter - 1;
-        if (s.contact && it % h->dcd_interval == 0) enqueue_dcd(h);
+        if (s.contact && it % h->dcd_interval == 0) enqueue_dcd(h, !h->bvh_refit || it == 0);
         enqueue_local(h, first ? LOCAL_PROX : (LOCAL_PROX | LOCAL_DUAL));
         if (s.contact) enqueue_contact(h, !first);
         enqueue_global(h, last);
         if (last) enqueue_residual(h);
     }
     if (h->admm_max_iter > 0) enqueue_local(h, LOCAL_DUAL);
+    h->phase = ADMM_PHASE_FINAL;
     LAUNCH(k_vertex_final, blocks(s.n, kVertThreads), kVertThreads, s);
 }
 
 int build_step_graph(AdmmB200* h) {
     if (h->step_exec) return ADMM_OK;
+    if (h->probe_kernel != 0 && h->probe_ev.empty()) {
+        h->probe_ev.resize(2 * kMaxProbes);
+        for (auto& e : h->probe_ev) CK(cudaEventCreate(&e));
+    }
+    h->probe_used = 0;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     h->launch_counter = 0;
@@ -335,6 +553,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     h->jac_iter = d->jacobi_iter;
     h->residual_tol = d->residual_tol;
     h->warmstart_ue = d->warmstart_ue != 0;
+    h->bvh_refit = d->bvh_refit != 0;
     h->warmstart_uc = d->warmstart_uc != 0;
     h->residual_every = d->residual_check_every;
     const int n = s.n, nd = s.nd, m = s.m;
@@ -432,18 +651,11 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.z, m));
     TRY(dalloc(h, &s.ue, m));
     TRY(dalloc(h, &s.y, m));
-    // matrices
+    // matrices (sliced-ELL layouts are chosen by the autotuner below)
     {
-        int *p, *c; float* v; float* dg;
-        TRY(dupload(h, &p, as.A.ptr.data(), as.A.ptr.size()));
-        TRY(dupload(h, &c, as.A.col.data(), as.A.col.size()));
-        TRY(dupload(h, &v, as.A.val.data(), as.A.val.size()));
+        float* dg;
         TRY(dupload(h, &dg, as.a_diag.data(), nd));
-        s.A.rows = nd; s.A.nslices = as.A.nslices; s.A.ptr = p; s.A.col = c; s.A.val = v; s.a_diag = dg;
-        TRY(dupload(h, &p, as.R.ptr.data(), as.R.ptr.size()));
-        TRY(dupload(h, &c, as.R.col.data(), as.R.col.size()));
-        TRY(dupload(h, &v, as.R.val.data(), as.R.val.size()));
-        s.R.rows = nd; s.R.nslices = as.R.nslices; s.R.ptr = p; s.R.col = c; s.R.val = v;
+        s.a_diag = dg;
     }
     // collision geometry and contacts
     s.nst = d->enable_contact ? d->n_surf_tri : 0;
@@ -496,7 +708,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.scan_tmp, scan_n));
     TRY(dalloc(h, &s.res, 4));
     TRY(dalloc(h, &s.done, 4));
-    h->contact_grid = std::max(1, std::min(blocks(s.cap, kContactThreads), 148 * 8));
+    h->contact_grid = std::max(1, std::min(blocks(s.cap, kContactThreads), 2 * 148));
 
     h->tet_blocks = s.ntet ? blocks(s.ntet, kLocalThreads) : 0;
     h->tri_blocks = s.ntri ? blocks(s.ntri, kLocalThreads) : 0;
@@ -508,6 +720,48 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
     TRY(upload_state(h, h->x_init, h->v_init));
+    if (d->ell_lanes != 0 && d->ell_lanes != 1 && d->ell_lanes != 2 && d->ell_lanes != 4 && d->ell_lanes != 8)
+        return fail(h, ADMM_ERR_INVALID, "ell_lanes must be 0, 1, 2, 4 or 8");
+    TRY(autotune_ell(h, as, d->ell_lanes, &h->tune_lanes_a, &h->tune_lanes_r, &h->tune_ms_a, &h->tune_ms_r));
+    TRY(upload_state(h, h->x_init, h->v_init));
+    return ADMM_OK;
+}
+
+__global__ void k_unpack_state(DevScene s, const float* __restrict__ stage, int has_v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    const float4 x = make_float4(stage[3 * i], stage[3 * i + 1], stage[3 * i + 2], 0.f);
+    s.x0[i] = x;
+    s.x[i] = x;
+    if (has_v) s.v[i] = make_float4(stage[3 * s.n + 3 * i], stage[3 * s.n + 3 * i + 1], stage[3 * s.n + 3 * i + 2], 0.f);
+}
+
+__global__ void k_pack_state(DevScene s, float* __restrict__ stage) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n) return;
+    const float4 x = s.x0[i], v = s.v[i];
+    stage[3 * i] = x.x; stage[3 * i + 1] = x.y; stage[3 * i + 2] = x.z;
+    stage[3 * s.n + 3 * i] = v.x; stage[3 * s.n + 3 * i + 1] = v.y; stage[3 * s.n + 3 * i + 2] = v.z;
+}
+
+int accumulate_timers(AdmmB200* h) {
+    if (h->profiling) {
+        for (int k = 0; k + 1 < h->prof_used; k += 2) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->prof_ev[k], h->prof_ev[k + 1]));
+            const int ph = h->prof_phase[k / 2];
+            h->phase_ms[ph] += ms;
+            h->phase_launches[ph] += 1;
+        }
+        h->prof_used = 0;
+    } else if (h->probe_kernel != 0) {
+        for (int k = 0; k + 1 < h->probe_used; k += 2) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->probe_ev[k], h->probe_ev[k + 1]));
+            h->probe_ms += ms;
+            h->probe_n += 1;
+        }
+    }
     return ADMM_OK;
 }
 
@@ -554,7 +808,10 @@ void admm_b200_destroy(AdmmB200* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
-    for (void* p : h->allocs) cudaFree(p);
+    for (void* p : h->allocs)
+        if (p) cudaFree(p);
+    for (auto e : h->prof_ev) cudaEventDestroy(e);
+    for (auto e : h->probe_ev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -565,6 +822,20 @@ int admm_b200_step_async(AdmmB200* h, int n_steps) {
     if (!h) return ADMM_ERR_INVALID;
     if (n_steps < 0) return fail(h, ADMM_ERR_INVALID, "n_steps");
     CK(cudaSetDevice(h->device));
+    if (h->profiling) {
+        // eager, one substep at a time so that every event pair can be read back
+        CK(cudaEventRecord(h->ev0, h->stream));
+        for (int k = 0; k < n_steps; k++) {
+            h->prof_used = 0;
+            enqueue_step(h);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(h->stream));
+            TRY(accumulate_timers(h));
+        }
+        CK(cudaEventRecord(h->ev1, h->stream));
+        h->frame += n_steps;
+        return ADMM_OK;
+    }
     TRY(build_step_graph(h));
     CK(cudaEventRecord(h->ev0, h->stream));
     for (int k = 0; k < n_steps; k++) CK(cudaGraphLaunch(h->step_exec, h->stream));
@@ -587,6 +858,7 @@ int admm_b200_step(AdmmB200* h, int n_steps, AdmmStepStats* stats) {
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->last_ms = n_steps > 0 ? ms / n_steps : 0.f;
+    if (!h->profiling) TRY(accumulate_timers(h));
     int status = ADMM_OK;
     TRY(read_err_flags(h, &status));
     int nc = 0;
@@ -846,7 +1118,79 @@ int admm_b200_last_step_device_ms(AdmmB200* h, float* ms) {
 
 int admm_b200_set_profiling(AdmmB200* h, int enabled) {
     if (!h) return ADMM_ERR_INVALID;
-    (void)enabled;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (enabled && h->prof_ev.empty()) {
+        h->prof_ev.resize(kMaxProfEvents);
+        h->prof_phase.assign(kMaxProfEvents / 2, 0);
+        for (auto& e : h->prof_ev) CK(cudaEventCreate(&e));
+    }
+    h->profiling = enabled != 0;
+    h->prof_used = 0;
+    return ADMM_OK;
+}
+
+int admm_b200_step_host(AdmmB200* h, const float* x_in, const float* v_in, float* x_out, float* v_out, int n) {
+    if (!h || !x_in) return ADMM_ERR_INVALID;
+    if (n != h->s.n) return fail(h, ADMM_ERR_INVALID, "n must equal n_vert");
+    CK(cudaSetDevice(h->device));
+    if (!h->stage) TRY(dalloc(h, &h->stage, (size_t)6 * n));
+    TRY(build_step_graph(h));
+    const size_t bytes = sizeof(float) * 3 * (size_t)n;
+    CK(cudaMemcpyAsync(h->stage, x_in, bytes, cudaMemcpyHostToDevice, h->stream));
+    if (v_in) CK(cudaMemcpyAsync(h->stage + 3 * (size_t)n, v_in, bytes, cudaMemcpyHostToDevice, h->stream));
+    k_unpack_state<<<blocks(n, 256), 256, 0, h->stream>>>(h->s, h->stage, v_in ? 1 : 0);
+    CK(cudaGraphLaunch(h->step_exec, h->stream));
+    k_pack_state<<<blocks(n, 256), 256, 0, h->stream>>>(h->s, h->stage);
+    if (x_out) CK(cudaMemcpyAsync(x_out, h->stage, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if (v_out) CK(cudaMemcpyAsync(v_out, h->stage + 3 * (size_t)n, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->frame += 1;
+    int status = ADMM_OK;
+    TRY(read_err_flags(h, &status));
+    return status;
+}
+
+int admm_b200_phase_times(AdmmB200* h, double* ms, int64_t* launches, int n_phases) {
+    if (!h) return ADMM_ERR_INVALID;
+    for (int k = 0; k < n_phases && k < ADMM_NUM_PHASES; k++) {
+        if (ms) ms[k] = h->phase_ms[k];
+        if (launches) launches[k] = h->phase_launches[k];
+        h->phase_ms[k] = 0.0;
+        h->phase_launches[k] = 0;
+    }
+    return ADMM_OK;
+}
+
+int admm_b200_set_probe(AdmmB200* h, int kernel_class) {
+    if (!h || kernel_class < 0 || kernel_class > ADMM_KERNEL_DCD_EE) return ADMM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->step_exec) {
+        cudaGraphExecDestroy(h->step_exec);
+        h->step_exec = nullptr;
+    }
+    h->probe_kernel = kernel_class;
+    h->probe_ms = 0.0;
+    h->probe_n = 0;
+    return ADMM_OK;
+}
+
+int admm_b200_probe_time(AdmmB200* h, double* mean_ms, int64_t* count) {
+    if (!h) return ADMM_ERR_INVALID;
+    if (mean_ms) *mean_ms = h->probe_n ? h->probe_ms / (double)h->probe_n : 0.0;
+    if (count) *count = h->probe_n;
+    h->probe_ms = 0.0;
+    h->probe_n = 0;
+    return ADMM_OK;
+}
+
+int admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float* ms_r) {
+    if (!h) return ADMM_ERR_INVALID;
+    if (lanes_a) *lanes_a = h->tune_lanes_a;
+    if (lanes_r) *lanes_r = h->tune_lanes_r;
+    if (ms_a) *ms_a = h->tune_ms_a;
+    if (ms_r) *ms_r = h->tune_ms_r;
     return ADMM_OK;
 }
 

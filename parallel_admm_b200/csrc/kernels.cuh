@@ -214,30 +214,49 @@ __global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
     s.p[i] = p;
 }
 
+// Gather of one sliced-ELL row: the warp `w` (a slice) accumulates sum val * v[col]
+// for its 32/T rows; lanes of one row are reduced with shuffles.  Returns the
+// row's sum in every lane of the row; `row` receives the lane's row index.
+template <int T>
+ADMM_DEV float4 ell_row_sum(const SlicedEll& M, const float4* __restrict__ v, int w, int lane, int& row) {
+    constexpr int S = 32 / T;
+    row = w * S + (lane % S);
+    const int b = M.ptr[w], e = M.ptr[w + 1];
+    float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll 4
+    for (int k = b + lane; k < e; k += 32) {
+        const int c = __ldg(&M.col[k]);
+        const float a = __ldg(&M.val[k]);
+        const float4 q = v[c];
+        ax = fmaf(a, q.x, ax);
+        ay = fmaf(a, q.y, ay);
+        az = fmaf(a, q.z, az);
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    return f4(ax, ay, az);
+}
+
 // ---------------------------------------------------------------------------
 // Right-hand side (admm_impl_gpu.cu:307-318):
 //   b = M x~ + h^2 D^T W^2 (z - Ue) [+ h^2 W_c (h p + x0 - Uc)]
-// as a gather over the sliced-ELL copy of h^2 D^T W^2.  SAVE_PREV also keeps
-// x before the solve (for the dual residual).
+// as a gather over the sliced-ELL copy of h^2 D^T W^2 (one warp per slice).
+// SAVE_PREV also keeps x before the solve (for the dual residual).
 // ---------------------------------------------------------------------------
-template <bool SAVE_PREV>
+template <int T, bool SAVE_PREV>
 __global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.nd) return;
-    const int sl = i / kSlice, lane = i % kSlice;
-    const int b = s.R.ptr[sl], e = s.R.ptr[sl + 1];
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    for (int k = b + lane; k < e; k += kSlice) {
-        const int c = s.R.col[k];
-        if (c < 0) break;
-        const float w = s.R.val[k];
-        const float4 yy = s.y[c];
-        ax += w * yy.x;
-        ay += w * yy.y;
-        az += w * yy.z;
-    }
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= s.R.nslices) return;
+    int i;
+    const float4 acc = ell_row_sum<T>(s.R, s.y, w, lane, i);
+    if (lane >= 32 / T || i >= s.nd) return;
     const float4 m = s.mxt[i];
-    float4 bi = f4(m.x + ax, m.y + ay, m.z + az);
+    float4 bi = f4(m.x + acc.x, m.y + acc.y, m.z + acc.z);
     if (s.contact) {
         const float4 p = s.p[i], x0 = s.x0[i], uc = s.uc[i];
         const float wc = s.dt2wc[i];
@@ -252,27 +271,20 @@ __global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
 // ---------------------------------------------------------------------------
 // One Jacobi sweep (JacobiFunctor, jacobi_solver.cu:52-98):
 //   dst_i = (b_i - sum_{j != i} a_ij src_j) / a_ii
-// over the sliced-ELL copy of the off-diagonal part of A.
+// over the sliced-ELL copy of the off-diagonal part of A (one warp per slice).
 // ---------------------------------------------------------------------------
+template <int T>
 __global__ void __launch_bounds__(kVertThreads) k_jacobi(DevScene s, const float4* __restrict__ src,
                                                          float4* __restrict__ dst) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.nd) return;
-    const int sl = i / kSlice, lane = i % kSlice;
-    const int b = s.A.ptr[sl], e = s.A.ptr[sl + 1];
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    for (int k = b + lane; k < e; k += kSlice) {
-        const int c = s.A.col[k];
-        if (c < 0) break;
-        const float w = s.A.val[k];
-        const float4 xx = src[c];
-        ax += xx.x * w;
-        ay += xx.y * w;
-        az += xx.z * w;
-    }
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= s.A.nslices) return;
+    int i;
+    const float4 acc = ell_row_sum<T>(s.A, src, w, lane, i);
+    if (lane >= 32 / T || i >= s.nd) return;
     const float4 bi = s.b[i];
     const float d = s.a_diag[i];
-    dst[i] = f4((bi.x - ax) / d, (bi.y - ay) / d, (bi.z - az) / d);
+    dst[i] = f4((bi.x - acc.x) / d, (bi.y - acc.y) / d, (bi.z - acc.z) / d);
 }
 
 __global__ void k_copy_dyn(DevScene s, const float4* __restrict__ src, float4* __restrict__ dst) {

@@ -148,6 +148,23 @@ __global__ void __launch_bounds__(256) k_karras(BvhDev t) {
     t.parent[right] = i;
 }
 
+// Refit of an existing tree: recompute the sorted leaves' boxes from the
+// current positions and clear the arrival counters (k_refit follows).
+template <int NV>
+__global__ void __launch_bounds__(256) k_leaf_refresh(const float4* __restrict__ x, const int* __restrict__ elems,
+                                                     int elem_stride, BvhDev t) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = t.n;
+    if (k >= n) return;
+    const int e = t.leaf_elem[k];
+    float4 lo = f4(1e32f, 1e32f, 1e32f), up = f4(-1e32f, -1e32f, -1e32f);
+#pragma unroll
+    for (int j = 0; j < NV; j++) box_add(lo, up, x[elems[e * elem_stride + j]]);
+    t.box_lo[n - 1 + k] = lo;
+    t.box_up[n - 1 + k] = up;
+    if (k < n - 1) t.flags[k] = 0u;
+}
+
 // Bottom-up refit: the second child to arrive at a node merges the boxes.
 __global__ void __launch_bounds__(256) k_refit(BvhDev t) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;

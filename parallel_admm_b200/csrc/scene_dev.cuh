@@ -4,14 +4,14 @@
 
 namespace admm {
 
-constexpr int kSlice = 32;          // sliced-ELL slice height (one warp)
 constexpr int kStackDepth = 64;     // BVH traversal stack (lbvh.cu:1698 uses 64)
 
-// Sliced ELL (Monakov et al. 2010): rows in slices of kSlice; slice s stores
-// width[s] columns column-major at ptr[s] (entry k of row r at ptr[s] + k*kSlice + r%kSlice).
+// Sliced ELL with `lanes` (T) threads per row: slices of 32/T rows, one warp per
+// slice; entry k of local row lr at ptr[s] + (k/T)*32 + (k%T)*(32/T) + lr.
 struct SlicedEll {
     int rows = 0;
     int nslices = 0;
+    int lanes = 1;
     const int* ptr = nullptr;    // [nslices+1] offsets (multiples of kSlice)
     const int* col = nullptr;
     const float* val = nullptr;

@@ -15,7 +15,7 @@
 namespace admm {
 
 struct HostEll {
-    int rows = 0, nslices = 0;
+    int rows = 0, nslices = 0, lanes = 1;
     std::vector<int> ptr, col;
     std::vector<float> val;
     int64_t nnz = 0;  // true entries (without padding)
@@ -26,35 +26,52 @@ struct HostCsr {
     std::vector<double> val;
 };
 
-inline HostEll csr_to_sliced_ell(const HostCsr& c, int rows, int slice) {
+// Sliced ELL with T lanes per row (T in {1, 2, 4, 8}): slices of S = 32/T rows,
+// each slice's width padded to a multiple of T.  Entry k of local row lr of
+// slice s sits at ptr[s] + (k / T) * 32 + (k % T) * S + lr, so one warp step
+// reads 32 consecutive entries.  Padding repeats the row's own column with a
+// zero value (branch-free in the kernel).  T = 1 is the classic sliced ELL of
+// Monakov et al. (2010) with slice height 32.
+inline HostEll csr_to_sliced_ell(const HostCsr& c, int rows, int T) {
     HostEll e;
+    const int S = 32 / T;
     e.rows = rows;
-    e.nslices = (rows + slice - 1) / slice;
+    e.lanes = T;
+    e.nslices = (rows + S - 1) / S;
     e.ptr.assign(e.nslices + 1, 0);
     for (int s = 0; s < e.nslices; s++) {
         int w = 0;
-        for (int r = s * slice; r < std::min(rows, (s + 1) * slice); r++) w = std::max(w, c.start[r + 1] - c.start[r]);
-        e.ptr[s + 1] = e.ptr[s] + w * slice;
+        for (int r = s * S; r < std::min(rows, (s + 1) * S); r++) w = std::max(w, c.start[r + 1] - c.start[r]);
+        w = (w + T - 1) / T * T;
+        e.ptr[s + 1] = e.ptr[s] + w * S;
     }
-    e.col.assign(e.ptr[e.nslices], -1);
+    e.col.assign(e.ptr[e.nslices], 0);
     e.val.assign(e.ptr[e.nslices], 0.f);
-    for (int s = 0; s < e.nslices; s++)
-        for (int r = s * slice; r < std::min(rows, (s + 1) * slice); r++) {
-            const int lane = r - s * slice;
-            for (int k = c.start[r]; k < c.start[r + 1]; k++) {
-                const int idx = e.ptr[s] + (k - c.start[r]) * slice + lane;
-                e.col[idx] = c.col[k];
-                e.val[idx] = (float)c.val[k];
+    for (int s = 0; s < e.nslices; s++) {
+        const int w = (e.ptr[s + 1] - e.ptr[s]) / S;
+        for (int lr = 0; lr < S; lr++) {
+            const int r = s * S + lr;
+            const int len = r < rows ? c.start[r + 1] - c.start[r] : 0;
+            for (int k = 0; k < w; k++) {
+                const int idx = e.ptr[s] + (k / T) * 32 + (k % T) * S + lr;
+                if (k < len) {
+                    e.col[idx] = c.col[c.start[r] + k];
+                    e.val[idx] = (float)c.val[c.start[r] + k];
+                } else {
+                    e.col[idx] = r < rows ? r : 0;
+                    e.val[idx] = 0.f;
+                }
             }
-            e.nnz += c.start[r + 1] - c.start[r];
+            e.nnz += len;
         }
+    }
     return e;
 }
 
 struct Assembly {
     std::vector<float> a_diag;      // [nd]
-    HostEll A;                      // off-diagonal part, nd x nd
-    HostEll R;                      // h^2 D^T W^2, nd x m
+    HostCsr A;                      // off-diagonal part, nd x nd (columns sorted)
+    HostCsr R;                      // h^2 D^T W^2, nd x m (columns sorted)
     std::vector<float> wrow;        // [m]
     std::vector<float> dt2wc;       // [nd]
     int64_t nnz_D = 0;
@@ -163,8 +180,8 @@ inline std::string assemble(const AdmmB200Desc& d, Assembly& out) {
         for (auto& kv : rt[i]) { rc.col.push_back(kv.first); rc.val.push_back(kv.second); }
         rc.start[i + 1] = (int)rc.col.size();
     }
-    out.A = csr_to_sliced_ell(ac, nd, 32);
-    out.R = csr_to_sliced_ell(rc, nd, 32);
+    out.A = std::move(ac);
+    out.R = std::move(rc);
     out.wrow.assign(m, 0.f);
     for (int r = 0; r < m; r++) out.wrow[r] = (float)w[r];
     return "";

@@ -57,6 +57,8 @@ class SolverParams:
     warmstart_ue: bool = True
     warmstart_uc: bool = True
     w_scale: float = 200.0
+    bvh_refit: bool = True
+    ell_lanes: int = 0
 
 
 @dataclasses.dataclass
@@ -194,43 +196,63 @@ def _co_linear(v1, v2, v3):
 
 
 def bending_constraints(verts: np.ndarray, faces: np.ndarray, vert_range: Tuple[int, int], k: float):
-    """Mean-value Laplacian bending rows (bending_constraint.h:24-78,127-171)."""
+    """Mean-value Laplacian bending rows (bending_constraint.h:24-78,127-171), vectorised.
+
+    For every vertex with a ring of >= 3 neighbours: radius = mean |ring - mid|,
+    varea = pi r^2 / 3, ring weight i = cot at mid towards ring[i+1] + cot towards
+    ring[i-1] (each skipped when the three points are co-linear,
+    |cross|^2 < 1e-7), scaled by 1/(2 varea)/100; the middle coefficient is the
+    sum of the ring weights and the ring weights are negated; w = sqrt(k varea).
+    """
     n = verts.shape[0]
-    rings = adjacency_lists(faces, n)
     v = verts.astype(np.float64)
-    offsets = [0]
-    inds: List[int] = []
-    coeffs: List[float] = []
-    ws: List[float] = []
-    for vi in range(vert_range[0], vert_range[1]):
-        ring = rings[vi]
-        if len(ring) < 3:
-            continue
-        mid = v[vi]
-        radius = np.mean(np.linalg.norm(v[ring] - mid, axis=1))
-        varea = PI_REF * radius * radius / 3.0
-        rn = len(ring)
-        c = []
-        for i in range(rn):
-            vert = v[ring[i]]
-            cw = v[ring[(i + 1) % rn]]
-            ccw = v[ring[(i + rn - 1) % rn]]
-            fv = 0.0
-            if not _co_linear(vert, mid, cw):
-                fv += _cot_at(vert, mid, cw)
-            if not _co_linear(vert, mid, ccw):
-                fv += _cot_at(vert, mid, ccw)
-            c.append(fv)
-        c = np.asarray(c) / (2.0 * varea) / 100.0
-        middle = c.sum()
-        inds.append(vi)
-        inds.extend(int(r) for r in ring)
-        coeffs.append(middle)
-        coeffs.extend((-c).tolist())
-        offsets.append(len(inds))
-        ws.append(math.sqrt(k * varea))
-    return (np.asarray(offsets, np.int32), np.asarray(inds, np.int32),
-            np.asarray(coeffs, np.float32), np.asarray(ws, np.float32))
+    e = np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]])
+    e = np.concatenate([e, e[:, ::-1]])
+    e = np.unique(e, axis=0)                       # sorted (vertex, neighbour) pairs
+    lo, hi = vert_range
+    e = e[(e[:, 0] >= lo) & (e[:, 0] < hi)]
+    starts = np.searchsorted(e[:, 0], np.arange(n + 1))
+    deg = np.diff(starts)
+    mids = np.nonzero(deg >= 3)[0]
+    mids = mids[(mids >= lo) & (mids < hi)]
+    if len(mids) == 0:
+        return (np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32), np.zeros(0, np.float32))
+    d = deg[mids]
+    seg = np.repeat(np.arange(len(mids)), d)
+    base = starts[mids]
+    pos = np.arange(d.sum()) - np.repeat(np.cumsum(d) - d, d)     # position within the ring
+    ring = e[np.repeat(base, d) + pos, 1]
+    nxt = e[np.repeat(base, d) + (pos + 1) % np.repeat(d, d), 1]
+    prv = e[np.repeat(base, d) + (pos + np.repeat(d, d) - 1) % np.repeat(d, d), 1]
+    mid = np.repeat(mids, d)
+    pm = v[mid]
+    dist = np.linalg.norm(v[ring] - pm, axis=1)
+    radius = np.bincount(seg, weights=dist) / d
+    varea = PI_REF * radius * radius / 3.0
+
+    def cot_term(a_idx, c_idx):
+        a = v[a_idx] - pm
+        b = v[c_idx] - pm
+        cr = np.cross(a, b)
+        c2 = np.sum(cr * cr, axis=1)
+        ok = c2 >= 1e-7
+        val = np.zeros(len(a))
+        val[ok] = np.sum(a * b, axis=1)[ok] / np.sqrt(c2[ok])
+        return val
+    c = cot_term(ring, nxt) + cot_term(ring, prv)
+    c = c / (2.0 * varea[seg]) / 100.0
+    middle = np.bincount(seg, weights=c, minlength=len(mids))
+    offsets = np.zeros(len(mids) + 1, np.int64)
+    offsets[1:] = np.cumsum(d + 1)
+    inds = np.empty(offsets[-1], np.int64)
+    coeffs = np.empty(offsets[-1], np.float64)
+    inds[offsets[:-1]] = mids
+    coeffs[offsets[:-1]] = middle
+    ring_slot = np.repeat(offsets[:-1] + 1, d) + pos
+    inds[ring_slot] = ring
+    coeffs[ring_slot] = -c
+    ws = np.sqrt(k * varea)
+    return (offsets.astype(np.int32), inds.astype(np.int32), coeffs.astype(np.float32), ws.astype(np.float32))
 
 
 def lumped_mass(n: int, verts: np.ndarray, faces: np.ndarray, face_density: np.ndarray,

@@ -122,8 +122,8 @@ def test_dcd_pairs_bitexact(case):
     assert n == len(ref_pairs)
     assert n > 0
     got = h.contacts()
-    assert _pairset(got["pairs"]) == _pairset(ref_pairs)
-    assert len(_pairset(got["pairs"])) == n  # no duplicates
+    # identical multisets (a point-triangle tuple can equal an edge-edge tuple)
+    assert sorted(map(tuple, got["pairs"].tolist())) == sorted(map(tuple, ref_pairs.tolist()))
 
 
 def test_contact_conversion_and_step_parity():
@@ -200,14 +200,32 @@ def test_long_run_cloth_1e3():
 
 
 def test_residuals_match_oracle():
+    """FP64 residual reductions agree with the oracle above the FP32 noise floor of the state.
+
+    D x - z is formed from FP32 x and z, so relative residuals below ~1e-6 are rounding
+    noise (2e-6 absolute allowance); with contact at impact they are far above it.
+    """
     sc = scene.cloth_on_box(16)
     h, o = _setup(sc)
     sg = h.step(2)
     so = o.step(2)
     for key in ("primal", "dual"):
-        a, b = sg[key], so[key]
-        assert np.isfinite(a)
-        assert abs(a - b) <= 0.05 * abs(b) + 1e-7, (key, a, b)
+        assert np.isfinite(sg[key])
+        assert abs(sg[key] - so[key]) <= 0.05 * abs(so[key]) + 2e-6, (key, sg[key], so[key])
+    sc = scene.cube_on_ground(8, drop=0.0)
+    v0 = np.zeros_like(sc.verts)
+    v0[:sc.n_dyn, 1] = -np.sqrt(2 * 9.8)
+    x0 = sc.verts.copy()
+    x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.02
+    h, o = _setup(sc)
+    h.set_state(x0, v0)
+    for b, a in ((B.BUF_X0, x0), (B.BUF_X, x0), (B.BUF_V, v0)):
+        o.write(b, a)
+    sg = h.step(1)
+    so = o.step(1)
+    assert so["primal"] > 1e-4 and so["n_contacts"] > 0
+    for key in ("primal", "dual"):
+        assert abs(sg[key] - so[key]) <= 0.05 * abs(so[key]) + 2e-6, (key, sg[key], so[key])
 
 
 def test_determinism_and_reset():
@@ -268,3 +286,35 @@ def test_backend_contract_call_order():
     assert det.points().shape == (det.max_slots(), 3)
     be.reset()
     assert np.allclose(be.getVertices(), sc.verts)
+
+
+def test_refit_and_rebuild_give_the_same_motion():
+    """Refitting the BVH between DCDs of a substep changes only traversal cost and the
+    order of contacts within a query (so the summation order): one impact substep agrees
+    to 1e-5 with the same contact count; three substeps at impact (where rounding can flip
+    borderline pairs) agree to the contact tolerance 1e-3."""
+    sc = scene.cube_on_ground(8, drop=0.0)
+    v0 = np.zeros_like(sc.verts)
+    v0[:sc.n_dyn, 1] = -np.sqrt(2 * 9.8)
+    x0 = sc.verts.copy()
+    x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.02
+    ext = np.ptp(x0[:sc.n_dyn], axis=0).max()
+    for nsteps, tol in ((1, TOL_STEP), (3, TOL_LONG)):
+        out = []
+        for refit in (0, 1):
+            sc.params.bvh_refit = bool(refit)
+            h = B.Handle(sc)
+            h.set_state(x0, v0)
+            st = h.step(nsteps)
+            out.append((h.get_state()[0], st["n_contacts"]))
+        assert out[0][1] > 0
+        if nsteps == 1:
+            assert out[0][1] == out[1][1]
+        assert np.abs(out[0][0] - out[1][0]).max() / ext <= tol
+
+
+def test_autotuner_choice_is_valid():
+    h = B.Handle(scene.cube_on_ground(12))
+    t = h.tuning()
+    assert t["jacobi_lanes"] in (1, 2, 4, 8) and t["rhs_lanes"] in (1, 2, 4, 8)
+    assert 0 < t["jacobi_ms"] < 10 and 0 < t["rhs_ms"] < 10
