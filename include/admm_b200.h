@@ -259,6 +259,22 @@ int  admm_b200_kernels_per_step(AdmmB200* h, int* n);
  * A (Jacobi) and h^2 D^T W^2 (right-hand side), and the measured ms per launch. */
 int  admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float* ms_r);
 
+/* --- allocation-free Jacobi solve (no counterpart in the reference) ---
+ * For callers that cannot allocate device memory themselves or through a handle
+ * (their memory is owned by their own pool allocator, or cudaMalloc's latency and
+ * implicit synchronisation are not acceptable in their loop).  Runs `sweeps`
+ * Jacobi sweeps x <- D^-1 (b - (A - D) x) on caller-owned device buffers:
+ * A's off-diagonal part in CSR (row_start[n+1], cols, vals), its diagonal diag[n],
+ * b, x_in and x_out row-major n x 3 floats (x_out may equal x_in), enqueued on
+ * `stream` (a cudaStream_t; NULL = the default stream).  Allocates nothing: the
+ * ping-pong buffers are a static device array of 2 x 262144 x 3 floats, so
+ * n <= 262144 (larger n returns ADMM_ERR_INVALID).  All calls in a process share
+ * that array: calls that overlap on the GPU race.  The first call on a device
+ * looks up the array's device address; make it before any stream capture. */
+int  admm_b200_jacobi_noalloc(int n, const int32_t* row_start, const int32_t* cols, const float* vals,
+                              const float* diag, const float* b, const float* x_in, float* x_out, int sweeps,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

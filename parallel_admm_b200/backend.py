@@ -185,6 +185,8 @@ def lib():
             "admm_b200_set_probe": (ctypes.c_int, [vp, ctypes.c_int]),
             "admm_b200_probe_time": (ctypes.c_int, [vp, _d, ctypes.POINTER(ctypes.c_int64)]),
             "admm_b200_tuning": (ctypes.c_int, [vp, _i, _i, _f, _f]),
+            "admm_b200_jacobi_noalloc": (ctypes.c_int, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int,
+                                                        vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -206,6 +208,7 @@ def exported_symbols():
         "admm_b200_clear_contacts", "admm_b200_residuals", "admm_b200_last_step_device_ms",
         "admm_b200_set_profiling", "admm_b200_kernels_per_step", "admm_b200_step_host",
         "admm_b200_phase_times", "admm_b200_set_probe", "admm_b200_probe_time", "admm_b200_tuning",
+        "admm_b200_jacobi_noalloc",
     ]
 
 
