@@ -53,6 +53,7 @@ struct AdmmB200 {
     int residual_every = 0;
     bool warmstart_ue = true, warmstart_uc = true;
     bool bvh_refit = true;
+    bool pdl = true;                // programmatic dependent launch between the kernels of a substep
     // autotuner choices (lanes per row of the sliced-ELL matrices) and their times
     int tune_lanes_a = 1, tune_lanes_r = 1;
     float tune_ms_a = 0.f, tune_ms_r = 0.f;
@@ -159,6 +160,7 @@ int alloc_bvh(AdmmB200* h, BvhDev& t, int n) {
     TRY(dalloc(h, &t.elem_lo, n));
     TRY(dalloc(h, &t.elem_up, n));
     TRY(dalloc(h, &t.scene, 8));
+    TRY(dalloc(h, &t.node4, n > 1 ? 4 * (size_t)(n - 1) : 4));
     return ADMM_OK;
 }
 
@@ -194,11 +196,11 @@ struct LaunchTimer {
     }
 };
 
-#define LAUNCH_P(pid, kernel, grid, block, ...)                            \
-    do {                                                                   \
-        LaunchTimer lt_(h, (pid));                                         \
-        kernel<<<(grid), (block), 0, h->stream>>>(__VA_ARGS__);            \
-        h->launch_counter++;                                               \
+#define LAUNCH_P(pid, kernel, grid, block, ...)                                      \
+    do {                                                                             \
+        LaunchTimer lt_(h, (pid));                                                   \
+        launch_k(kernel, dim3(grid), dim3(block), 0, h->stream, h->pdl, __VA_ARGS__); \
+        h->launch_counter++;                                                         \
     } while (0)
 #define LAUNCH(kernel, grid, block, ...) LAUNCH_P(0, kernel, grid, block, __VA_ARGS__)
 
@@ -218,7 +220,7 @@ void enqueue_build(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tr
     LAUNCH(k_morton, blocks(n, 256), 256, t);
     if (n > 1) {
         LaunchTimer lt(h, 0);  // one timer around the 40 launches of the sort
-        radix_sort(t.keys, t.vals, t.keys_alt, t.vals_alt, n, 64, h->hist, h->s.scan_tmp, h->stream);
+        radix_sort(t.keys, t.vals, t.keys_alt, t.vals_alt, n, 64, h->hist, h->s.scan_tmp, h->stream, h->pdl);
         h->launch_counter += 8 * 5;
     }
     LAUNCH(k_karras, blocks(n, 256), 256, t);
@@ -243,7 +245,7 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
     if (s.nse > 0) LAUNCH(k_dcd_ee<false>, blocks(s.nse, 128), 128, s);
     if (nq > 0) {
         LaunchTimer lt(h, 0);
-        exclusive_scan(s.qcount, s.qoff, nq, s.scan_tmp, s.nc_raw, h->stream);
+        exclusive_scan(s.qcount, s.qoff, nq, s.scan_tmp, s.nc_raw, h->stream, h->pdl);
         h->launch_counter += 3;
     } else {
         cudaMemsetAsync(s.nc_raw, 0, sizeof(int), h->stream);
@@ -256,7 +258,7 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
     LAUNCH(k_contact_count, h->contact_grid, kContactThreads, s);
     {
         LaunchTimer lt(h, 0);
-        exclusive_scan(s.vcnt, s.vstart, s.n, s.scan_tmp, s.vstart + s.n, h->stream);
+        exclusive_scan(s.vcnt, s.vstart, s.n, s.scan_tmp, s.vstart + s.n, h->stream, h->pdl);
         h->launch_counter += 3;
     }
     LAUNCH(k_contact_fill, h->contact_grid, kContactThreads, s);
@@ -338,7 +340,7 @@ void enqueue_global(AdmmB200* h, bool save_prev) {
     enqueue_jacobi(h, h->jac_iter);
 }
 
-int upload_ell(AdmmB200* h, const HostCsr& c, int rows, int lanes, SlicedEll& out) {
+int upload_ell(AdmmB200* h, const HostCsr& c, int rows, int lanes, SlicedEll& out, HostEll* keep = nullptr) {
     HostEll e = csr_to_sliced_ell(c, rows, lanes);
     int *p = nullptr, *cc = nullptr;
     float* v = nullptr;
@@ -351,6 +353,7 @@ int upload_ell(AdmmB200* h, const HostCsr& c, int rows, int lanes, SlicedEll& ou
     out.ptr = p;
     out.col = cc;
     out.val = v;
+    if (keep) *keep = std::move(e);
     return ADMM_OK;
 }
 

@@ -3,11 +3,42 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #define ADMM_DEV __device__ __forceinline__
+
+// Programmatic dependent launch: every kernel of a substep first lets the next
+// kernel of the stream begin its launch, then waits until all preceding kernels
+// have completed and their writes are visible.  Results are unchanged; the
+// launch latency of a kernel overlaps the execution of its predecessor.  Both
+// instructions are no-ops for a kernel launched without the PDL attribute.
+#define ADMM_PDL_PROLOGUE()                                          \
+    do {                                                             \
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); \
+        asm volatile("griddepcontrol.wait;" ::: "memory");           \
+    } while (0)
 
 namespace admm {
 
 constexpr int kWarp = 32;
+
+// Launches `k` on `st`; with pdl the launch carries the programmatic stream
+// serialization attribute (the kernel must start with ADMM_PDL_PROLOGUE).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                            Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
 
 ADMM_DEV float4 f4(float x, float y, float z, float w = 0.f) { return make_float4(x, y, z, w); }
 ADMM_DEV float4 add3(float4 a, float4 b) { return f4(a.x + b.x, a.y + b.y, a.z + b.z); }

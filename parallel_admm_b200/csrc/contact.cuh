@@ -16,6 +16,7 @@ ADMM_DEV float comp(float4 v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k ==
 // per-vertex contact counts over all four vertices (updateContactCounts,
 // contact_solver.cu:90-101)
 __global__ void __launch_bounds__(kContactThreads) k_contact_count(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int nc = ccount(s);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         const int4 q = s.pairs[c];
@@ -28,6 +29,7 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_count(DevScene s) {
 
 // incidence slots (compute_Scc_kernel's CSR fill, contact_solver.cu:210-223)
 __global__ void __launch_bounds__(kContactThreads) k_contact_fill(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int nc = ccount(s);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         const int4 q = s.pairs[c];
@@ -43,6 +45,7 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_fill(DevScene s) {
 // Sort each vertex's incidence list by (contact, slot) so the gather below
 // sums in a fixed order (the reference's order depends on atomics, F13).
 __global__ void __launch_bounds__(kContactThreads) k_contact_sort_lists(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.nd) return;
     const int b = s.vstart[i], e = s.vstart[i + 1];
@@ -60,6 +63,7 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_sort_lists(DevScene
 // S_c, Gamma_c, K_c, r_c = 0 (compute_Scc_kernel, contact_solver.cu:188-227;
 // the fills at 240-243).
 __global__ void __launch_bounds__(kContactThreads) k_contact_scc(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int nc = ccount(s);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         const int4 q = s.pairs[c];
@@ -80,6 +84,7 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_scc(DevScene s) {
 
 // Friction-cone projection per contact (get_delta_u_kernel, contact_solver.cu:337-379).
 __global__ void __launch_bounds__(kContactThreads) k_contact_du(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int nc = ccount(s);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         const int4 q = s.pairs[c];
@@ -116,6 +121,7 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_du(DevScene s) {
 
 // p_i += sum_c Gamma_c,i du_c over the incidence list (update_p, contact_solver.cu:381-399).
 __global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.nd) return;
     const int b = s.vstart[i], e = s.vstart[i + 1];

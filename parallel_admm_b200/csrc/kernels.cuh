@@ -94,6 +94,7 @@ ADMM_DEV void bend_dx(const float4* __restrict__ x, const DevScene& s, int c, fl
 
 template <int MODE>
 __global__ void __launch_bounds__(kLocalThreads) k_local(DevScene s, int tet_blocks, int tri_blocks, int bend_blocks) {
+    ADMM_PDL_PROLOGUE();
     int blk = blockIdx.x;
     if (blk < tet_blocks) {
         const int c = blk * kLocalThreads + threadIdx.x;
@@ -155,6 +156,7 @@ __global__ void __launch_bounds__(kLocalThreads) k_local(DevScene s, int tet_blo
 // p <- v copy of the static range (admm_impl_gpu.cu:282).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kVertThreads) k_pre_integration(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
     float4 x0 = s.x0[i], v = s.v[i], x;
@@ -185,6 +187,7 @@ __global__ void __launch_bounds__(kVertThreads) k_pre_integration(DevScene s) {
 // ---------------------------------------------------------------------------
 template <bool DUALC, bool WARM>
 __global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.nd) return;
     const float4 x = s.x[i], x0 = s.x0[i];
@@ -249,6 +252,7 @@ ADMM_DEV float4 ell_row_sum(const SlicedEll& M, const float4* __restrict__ v, in
 // ---------------------------------------------------------------------------
 template <int T, bool SAVE_PREV>
 __global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= s.R.nslices) return;
@@ -276,6 +280,7 @@ __global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
 template <int T>
 __global__ void __launch_bounds__(kVertThreads) k_jacobi(DevScene s, const float4* __restrict__ src,
                                                          float4* __restrict__ dst) {
+    ADMM_PDL_PROLOGUE();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= s.A.nslices) return;
@@ -288,6 +293,7 @@ __global__ void __launch_bounds__(kVertThreads) k_jacobi(DevScene s, const float
 }
 
 __global__ void k_copy_dyn(DevScene s, const float4* __restrict__ src, float4* __restrict__ dst) {
+    ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < s.nd) dst[i] = src[i];
 }
@@ -297,6 +303,7 @@ __global__ void k_copy_dyn(DevScene s, const float4* __restrict__ src, float4* _
 // (jacobi_solver.cu:236-252): v = (x - x0)/h on dynamic vertices, x0 = x.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kVertThreads) k_vertex_final(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
     const float4 x = s.x[i], x0 = s.x0[i];
@@ -341,6 +348,7 @@ ADMM_DEV void res_rows(const DevScene& s, int row, const float (&dx)[3 * NR], co
 
 __global__ void __launch_bounds__(kLocalThreads) k_residual(DevScene s, int tet_blocks, int tri_blocks,
                                                            int bend_blocks, int pin_blocks) {
+    ADMM_PDL_PROLOGUE();
     __shared__ double sh[kLocalThreads / 32];
     double pr = 0.0, du = 0.0, sc = 0.0;
     int blk = blockIdx.x;

@@ -31,6 +31,7 @@ ADMM_DEV void box_add(float4& lo, float4& up, float4 p) {
 template <int NV>
 __global__ void __launch_bounds__(256) k_elem_boxes(const float4* __restrict__ x, const int* __restrict__ elems,
                                                    int elem_stride, int n, BvhDev t) {
+    ADMM_PDL_PROLOGUE();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     float4 lo = f4(1e32f, 1e32f, 1e32f), up = f4(-1e32f, -1e32f, -1e32f);
     if (e < n) {
@@ -59,6 +60,7 @@ __global__ void __launch_bounds__(256) k_elem_boxes(const float4* __restrict__ x
 }
 
 __global__ void k_scene_init(BvhDev a, BvhDev b) {
+    ADMM_PDL_PROLOGUE();
     const int i = threadIdx.x;
     if (i < 3) {
         a.scene[i] = float_to_ordered(3e38f);
@@ -81,6 +83,7 @@ ADMM_DEV unsigned long long spread21(unsigned int v) {
 }
 
 __global__ void __launch_bounds__(256) k_morton(BvhDev t) {
+    ADMM_PDL_PROLOGUE();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= t.n) return;
     const float slo[3] = {ordered_to_float(t.scene[0]), ordered_to_float(t.scene[1]), ordered_to_float(t.scene[2])};
@@ -111,6 +114,7 @@ ADMM_DEV int karras_delta(const unsigned long long* __restrict__ k, int n, int i
 // Internal node i in [0, n-1); leaf k is node n-1+k.  Also writes the sorted
 // leaf records (element id and box) and clears the refit counters.
 __global__ void __launch_bounds__(256) k_karras(BvhDev t) {
+    ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = t.n;
     if (i < n) {
@@ -146,6 +150,19 @@ __global__ void __launch_bounds__(256) k_karras(BvhDev t) {
     t.right[i] = right;
     t.parent[left] = i;
     t.parent[right] = i;
+    t.node4[4 * i + 0].w = __int_as_float(left);
+    t.node4[4 * i + 2].w = __int_as_float(right);
+}
+
+// Writes node `c`'s box into its parent's record (left or right slot).
+ADMM_DEV void store_in_parent(const BvhDev& t, int c, float4 lo, float4 up) {
+    const int p = t.parent[c];
+    if (p < 0) return;
+    const int slot = (t.left[p] == c) ? 0 : 2;
+    float4* r = t.node4 + 4 * p + slot;
+    const float idx = __ldcg(&r[0].w);
+    __stcg(&r[0], make_float4(lo.x, lo.y, lo.z, idx));
+    __stcg(&r[1], make_float4(up.x, up.y, up.z, 0.f));
 }
 
 // Refit of an existing tree: recompute the sorted leaves' boxes from the
@@ -153,6 +170,7 @@ __global__ void __launch_bounds__(256) k_karras(BvhDev t) {
 template <int NV>
 __global__ void __launch_bounds__(256) k_leaf_refresh(const float4* __restrict__ x, const int* __restrict__ elems,
                                                      int elem_stride, BvhDev t) {
+    ADMM_PDL_PROLOGUE();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = t.n;
     if (k >= n) return;
@@ -167,10 +185,12 @@ __global__ void __launch_bounds__(256) k_leaf_refresh(const float4* __restrict__
 
 // Bottom-up refit: the second child to arrive at a node merges the boxes.
 __global__ void __launch_bounds__(256) k_refit(BvhDev t) {
+    ADMM_PDL_PROLOGUE();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = t.n;
     if (k >= n || n < 2) return;
     int node = n - 1 + k;
+    store_in_parent(t, node, t.box_lo[node], t.box_up[node]);
     int p = t.parent[node];
     for (int guard = 0; p >= 0; guard++) {
         if (guard >= n) {  // deeper than any valid tree: malformed, stop
@@ -181,11 +201,13 @@ __global__ void __launch_bounds__(256) k_refit(BvhDev t) {
         const unsigned old = atomicAdd(&t.flags[p], 1u);
         if (old == 0u) return;
         __threadfence();  // acquire: the sibling published its box before its atomic
-        const int l = t.left[p], r = t.right[p];
-        const float4 al = __ldcg(&t.box_lo[l]), bl = __ldcg(&t.box_lo[r]);
-        const float4 au = __ldcg(&t.box_up[l]), bu = __ldcg(&t.box_up[r]);
-        __stcg(&t.box_lo[p], f4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z)));
-        __stcg(&t.box_up[p], f4(fmaxf(au.x, bu.x), fmaxf(au.y, bu.y), fmaxf(au.z, bu.z)));
+        const float4 al = __ldcg(&t.node4[4 * p + 0]), au = __ldcg(&t.node4[4 * p + 1]);
+        const float4 bl = __ldcg(&t.node4[4 * p + 2]), bu = __ldcg(&t.node4[4 * p + 3]);
+        const float4 lo = f4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z));
+        const float4 up = f4(fmaxf(au.x, bu.x), fmaxf(au.y, bu.y), fmaxf(au.z, bu.z));
+        __stcg(&t.box_lo[p], lo);
+        __stcg(&t.box_up[p], up);
+        store_in_parent(t, p, lo, up);
         node = p;
         p = t.parent[p];
     }
@@ -303,6 +325,7 @@ ADMM_DEV void write_contact(const DevScene& s, int slot, int4 ids, const NpResul
 // VF: query q = surface vertex sv[q] against the face tree (lbvh.cu:1693-1748).
 template <bool WRITE>
 __global__ void __launch_bounds__(128) k_dcd_vf(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= s.nsv) return;
     const BvhDev& t = s.bf;
@@ -314,8 +337,8 @@ __global__ void __launch_bounds__(128) k_dcd_vf(DevScene s) {
     int stack[kStackDepth];
     int sp = 0;
     const int n = t.n;
-    auto visit = [&](int node) -> bool {  // returns true if node must be pushed
-        if (!box_overlap(P, P, t.box_lo[node], t.box_up[node], gap)) return false;
+    auto visit = [&](int node, float4 blo, float4 bup) -> bool {  // true: push the (internal) node
+        if (!box_overlap(P, P, blo, bup, gap)) return false;
         if (node < n - 1) return true;
         const int f = t.leaf_elem[node - (n - 1)];
         const int4 tri = s.st[f];
@@ -331,7 +354,7 @@ __global__ void __launch_bounds__(128) k_dcd_vf(DevScene s) {
         return false;
     };
     if (n == 1) {
-        visit(0);
+        visit(0, t.box_lo[0], t.box_up[0]);
     } else if (n > 1) {
         stack[sp++] = 0;
         for (int pops = 0; sp > 0; pops++) {
@@ -340,12 +363,14 @@ __global__ void __launch_bounds__(128) k_dcd_vf(DevScene s) {
                 break;
             }
             const int node = stack[--sp];
-            const int l = t.left[node], r = t.right[node];
-            if (visit(l)) {
+            const float4* rec = t.node4 + 4 * node;
+            const float4 ll = rec[0], lu = rec[1], rl = rec[2], ru = rec[3];
+            const int l = __float_as_int(ll.w), r = __float_as_int(rl.w);
+            if (visit(l, ll, lu)) {
                 if (sp < kStackDepth) stack[sp++] = l;
                 else s.err[1] = 1;
             }
-            if (visit(r)) {
+            if (visit(r, rl, ru)) {
                 if (sp < kStackDepth) stack[sp++] = r;
                 else s.err[1] = 1;
             }
@@ -358,6 +383,7 @@ __global__ void __launch_bounds__(128) k_dcd_vf(DevScene s) {
 // index that share no vertex (lbvh.cu:1750-1813).
 template <bool WRITE>
 __global__ void __launch_bounds__(128) k_dcd_ee(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= s.nse) return;
     const BvhDev& t = s.be;
@@ -372,8 +398,8 @@ __global__ void __launch_bounds__(128) k_dcd_ee(DevScene s) {
     int stack[kStackDepth];
     int sp = 0;
     const int n = t.n;
-    auto visit = [&](int node) -> bool {
-        if (!box_overlap(lo, up, t.box_lo[node], t.box_up[node], gap)) return false;
+    auto visit = [&](int node, float4 blo, float4 bup) -> bool {
+        if (!box_overlap(lo, up, blo, bup, gap)) return false;
         if (node < n - 1) return true;
         const int o = t.leaf_elem[node - (n - 1)];
         if (o <= e) return false;
@@ -390,7 +416,7 @@ __global__ void __launch_bounds__(128) k_dcd_ee(DevScene s) {
         return false;
     };
     if (n == 1) {
-        visit(0);
+        visit(0, t.box_lo[0], t.box_up[0]);
     } else if (n > 1) {
         stack[sp++] = 0;
         for (int pops = 0; sp > 0; pops++) {
@@ -399,12 +425,14 @@ __global__ void __launch_bounds__(128) k_dcd_ee(DevScene s) {
                 break;
             }
             const int node = stack[--sp];
-            const int l = t.left[node], r = t.right[node];
-            if (visit(l)) {
+            const float4* rec = t.node4 + 4 * node;
+            const float4 ll = rec[0], lu = rec[1], rl = rec[2], ru = rec[3];
+            const int l = __float_as_int(ll.w), r = __float_as_int(rl.w);
+            if (visit(l, ll, lu)) {
                 if (sp < kStackDepth) stack[sp++] = l;
                 else s.err[1] = 1;
             }
-            if (visit(r)) {
+            if (visit(r, rl, ru)) {
                 if (sp < kStackDepth) stack[sp++] = r;
                 else s.err[1] = 1;
             }
@@ -415,6 +443,7 @@ __global__ void __launch_bounds__(128) k_dcd_ee(DevScene s) {
 
 // nc = min(total, cap); overflow flag.
 __global__ void k_set_count(DevScene s) {
+    ADMM_PDL_PROLOGUE();
     const int raw = *s.nc_raw;
     *s.nc = raw < s.cap ? raw : s.cap;
     if (raw > s.cap) s.err[0] = 1;

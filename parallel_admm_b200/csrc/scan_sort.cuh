@@ -41,6 +41,7 @@ ADMM_DEV int block_exclusive_scan(int v, int* sh_warp) {
 // Phase 1: per-tile exclusive scan in place (out) and tile totals.
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int* __restrict__ in, int* __restrict__ out,
                                                             int n, int* __restrict__ tile_sums) {
+    ADMM_PDL_PROLOGUE();
     __shared__ int sh[32];
     const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     int v[kScanItems];
@@ -64,6 +65,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int* __restri
 // total written to *total (may be NULL) and tile_sums becomes exclusive.
 __global__ void __launch_bounds__(kScanThreads) k_scan_sums(int* __restrict__ tile_sums, int ntiles,
                                                            int* __restrict__ total) {
+    ADMM_PDL_PROLOGUE();
     __shared__ int sh[32];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
@@ -84,6 +86,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_sums(int* __restrict__ ti
 // Phase 3: add tile offsets.
 __global__ void __launch_bounds__(kScanThreads) k_scan_add(int* __restrict__ out, int n,
                                                           const int* __restrict__ tile_sums) {
+    ADMM_PDL_PROLOGUE();
     const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     const int add = tile_sums[blockIdx.x];
 #pragma unroll
@@ -95,12 +98,12 @@ inline int scan_tiles(int n) { return (n + kScanTile - 1) / kScanTile; }
 
 // exclusive scan of n ints: out[i] = sum_{j<i} in[j]; *total = sum (device).
 // tmp needs scan_tiles(n) ints.  in and out may alias.
-inline void exclusive_scan(const int* in, int* out, int n, int* tmp, int* total, cudaStream_t st) {
+inline void exclusive_scan(const int* in, int* out, int n, int* tmp, int* total, cudaStream_t st, bool pdl = false) {
     if (n <= 0) return;
     const int nt = scan_tiles(n);
-    k_scan_tiles<<<nt, kScanThreads, 0, st>>>(in, out, n, tmp);
-    k_scan_sums<<<1, kScanThreads, 0, st>>>(tmp, nt, total);
-    k_scan_add<<<nt, kScanThreads, 0, st>>>(out, n, tmp);
+    launch_k(k_scan_tiles, dim3(nt), dim3(kScanThreads), 0, st, pdl, in, out, n, tmp);
+    launch_k(k_scan_sums, dim3(1), dim3(kScanThreads), 0, st, pdl, tmp, nt, total);
+    launch_k(k_scan_add, dim3(nt), dim3(kScanThreads), 0, st, pdl, out, n, (const int*)tmp);
 }
 
 // ---------------------------------------------------------------------------
@@ -114,6 +117,7 @@ constexpr int kSortTile = 2048;
 
 __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const unsigned long long* __restrict__ keys, int n,
                                                             int shift, int* __restrict__ hist, int ntiles) {
+    ADMM_PDL_PROLOGUE();
     __shared__ int h[256];
     h[threadIdx.x] = 0;
     __syncthreads();
@@ -131,6 +135,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const unsigned l
                                                                unsigned long long* __restrict__ kout,
                                                                int* __restrict__ vout, int n, int shift,
                                                                const int* __restrict__ offs, int ntiles) {
+    ADMM_PDL_PROLOGUE();
     __shared__ int run[256];
     __shared__ int wcnt[kSortWarps][256];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -176,15 +181,17 @@ inline int sort_tiles(int n) { return (n + kSortTile - 1) / kSortTile; }
 // the number of passes is even, which holds for bits = 64.  hist needs
 // 256 * sort_tiles(n) ints, scan_tmp scan_tiles(256 * sort_tiles(n)) ints.
 inline void radix_sort(unsigned long long* keys, int* vals, unsigned long long* keys_alt, int* vals_alt, int n,
-                       int bits, int* hist, int* scan_tmp, cudaStream_t st) {
+                       int bits, int* hist, int* scan_tmp, cudaStream_t st, bool pdl = false) {
     if (n <= 1) return;
     const int nt = sort_tiles(n);
     unsigned long long *ki = keys, *ko = keys_alt;
     int *vi = vals, *vo = vals_alt;
     for (int shift = 0; shift < bits; shift += 8) {
-        k_radix_hist<<<nt, kSortThreads, 0, st>>>(ki, n, shift, hist, nt);
-        exclusive_scan(hist, hist, 256 * nt, scan_tmp, nullptr, st);
-        k_radix_scatter<<<nt, kSortThreads, 0, st>>>(ki, vi, ko, vo, n, shift, hist, nt);
+        launch_k(k_radix_hist, dim3(nt), dim3(kSortThreads), 0, st, pdl, (const unsigned long long*)ki, n, shift, hist,
+                 nt);
+        exclusive_scan(hist, hist, 256 * nt, scan_tmp, nullptr, st, pdl);
+        launch_k(k_radix_scatter, dim3(nt), dim3(kSortThreads), 0, st, pdl, (const unsigned long long*)ki,
+                 (const int*)vi, ko, vo, n, shift, (const int*)hist, nt);
         unsigned long long* tk = ki; ki = ko; ko = tk;
         int* tv = vi; vi = vo; vo = tv;
     }

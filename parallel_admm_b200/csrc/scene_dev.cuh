@@ -33,6 +33,10 @@ struct BvhDev {
     float4* elem_lo = nullptr;   // [n] unsorted element boxes
     float4* elem_up = nullptr;
     uint32_t* scene = nullptr;   // [6] ordered-float min xyz, max xyz
+    // Internal node i as one 64-byte record: node4[4i+0] = left child box lower
+    // (w = left index), [4i+1] = left upper, [4i+2] = right lower (w = right
+    // index), [4i+3] = right upper.  One load per traversal level.
+    float4* node4 = nullptr;     // [4(n-1)]
 };
 
 struct DevScene {
