@@ -253,7 +253,9 @@ int  admm_b200_phase_times(AdmmB200* h, double* ms, int64_t* launches, int n_pha
  * admm_b200_probe_time returns their mean (ms per launch) and count, then resets. */
 int  admm_b200_set_probe(AdmmB200* h, int kernel_class);
 int  admm_b200_probe_time(AdmmB200* h, double* mean_ms, int64_t* count);
-/* Number of kernels one substep launches (for launch accounting). */
+/* Number of kernels one substep launches (for launch accounting).  With
+ * residual_tol > 0 the count depends on the iterations run: it is the count of
+ * the most recent substep (before the first one, of a substep of one chunk). */
 int  admm_b200_kernels_per_step(AdmmB200* h, int* n);
 /* Autotuner choices made at create: lanes per row of the sliced-ELL copies of
  * A (Jacobi) and h^2 D^T W^2 (right-hand side), and the measured ms per launch. */

@@ -217,6 +217,8 @@ struct Oracle {
     float thickness;
     int admm_max_iter, dcd_interval, gs_max_iter, jacobi_iter;
     bool contact, ws_ue, ws_uc;
+    float residual_tol = 0.f;
+    int chunk = 0;
     // matrices
     Csr D;        // m x nd
     Csr A;        // nd x nd off-diagonal part
@@ -272,6 +274,11 @@ struct Oracle {
         admm_max_iter = d->admm_max_iter; dcd_interval = std::max(1, d->dcd_interval);
         gs_max_iter = d->gs_max_iter; jacobi_iter = d->jacobi_iter;
         contact = d->enable_contact != 0; ws_ue = d->warmstart_ue != 0; ws_uc = d->warmstart_uc != 0;
+        residual_tol = d->residual_tol;
+        {
+            const int every = d->residual_check_every > 0 ? d->residual_check_every : dcd_interval;
+            chunk = (every + dcd_interval - 1) / dcd_interval * dcd_interval;
+        }
         x0_init.assign(3 * n, R(0));
         v0_init.assign(3 * n, R(0));
         for (int i = 0; i < 3 * n; i++) x0_init[i] = d->x0[i];
@@ -654,6 +661,12 @@ struct Oracle {
                     for (int k = 0; k < 3; k++)
                         Uc[3 * i + k] = Uc[3 * i + k] + ((x[3 * i + k] - x0[3 * i + k]) - p[3 * i + k] * dt);
             iters++;
+            // residual_tol > 0: test after every chunk of iterations; stop when both
+            // relative residuals are within tol or another chunk would pass max_iter
+            if (residual_tol > 0.f && iters % chunk == 0) {
+                const bool conv = last_primal <= (double)residual_tol && last_dual <= (double)residual_tol;
+                if (conv || iters + chunk > admm_max_iter) break;
+            }
         }
         // do_post_process_kernel (jacobi_solver.cu:236-252)
         for (int i = 0; i < n; i++)

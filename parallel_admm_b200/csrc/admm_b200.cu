@@ -54,6 +54,12 @@ struct AdmmB200 {
     bool warmstart_ue = true, warmstart_uc = true;
     bool bvh_refit = true;
     bool pdl = true;                // programmatic dependent launch between the kernels of a substep
+    cudaStream_t cstream = nullptr; // stream the enqueue helpers launch on (capture target)
+    cudaStream_t body_stream = nullptr;
+    int chunk = 0;                  // ADMM iterations between residual checks (residual_tol > 0)
+    bool in_body = false;           // capturing the body of the conditional node (no event nodes allowed)
+    int kernels_body = 0;           // kernels of one conditional-body chunk
+    int last_iters = 0;             // ADMM iterations of the most recent substep
     // autotuner choices (lanes per row of the sliced-ELL matrices) and their times
     int tune_lanes_a = 1, tune_lanes_r = 1;
     float tune_ms_a = 0.f, tune_ms_r = 0.f;
@@ -181,7 +187,7 @@ struct LaunchTimer {
             b = h->prof_ev[h->prof_used + 1];
             h->prof_phase[h->prof_used / 2] = h->phase;
             h->prof_used += 2;
-        } else if (!h->profiling && pid != 0 && pid == h->probe_kernel &&
+        } else if (!h->profiling && !h->in_body && pid != 0 && pid == h->probe_kernel &&
                    h->probe_used + 2 <= (int)h->probe_ev.size()) {
             probe = true;
             a = h->probe_ev[h->probe_used];
@@ -189,17 +195,17 @@ struct LaunchTimer {
             h->probe_used += 2;
         }
         // inside stream capture only an external record becomes a timing node of the graph
-        if (a) cudaEventRecordWithFlags(a, h->stream, probe ? cudaEventRecordExternal : cudaEventRecordDefault);
+        if (a) cudaEventRecordWithFlags(a, h->cstream, probe ? cudaEventRecordExternal : cudaEventRecordDefault);
     }
     ~LaunchTimer() {
-        if (b) cudaEventRecordWithFlags(b, h->stream, probe ? cudaEventRecordExternal : cudaEventRecordDefault);
+        if (b) cudaEventRecordWithFlags(b, h->cstream, probe ? cudaEventRecordExternal : cudaEventRecordDefault);
     }
 };
 
 #define LAUNCH_P(pid, kernel, grid, block, ...)                                      \
     do {                                                                             \
         LaunchTimer lt_(h, (pid));                                                   \
-        launch_k(kernel, dim3(grid), dim3(block), 0, h->stream, h->pdl, __VA_ARGS__); \
+        launch_k(kernel, dim3(grid), dim3(block), 0, h->cstream, h->pdl, __VA_ARGS__); \
         h->launch_counter++;                                                         \
     } while (0)
 #define LAUNCH(kernel, grid, block, ...) LAUNCH_P(0, kernel, grid, block, __VA_ARGS__)
@@ -220,7 +226,7 @@ void enqueue_build(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tr
     LAUNCH(k_morton, blocks(n, 256), 256, t);
     if (n > 1) {
         LaunchTimer lt(h, 0);  // one timer around the 40 launches of the sort
-        radix_sort(t.keys, t.vals, t.keys_alt, t.vals_alt, n, 64, h->hist, h->s.scan_tmp, h->stream, h->pdl);
+        radix_sort(t.keys, t.vals, t.keys_alt, t.vals_alt, n, 64, h->hist, h->s.scan_tmp, h->cstream, h->pdl);
         h->launch_counter += 8 * 5;
     }
     LAUNCH(k_karras, blocks(n, 256), 256, t);
@@ -245,20 +251,20 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
     if (s.nse > 0) LAUNCH(k_dcd_ee<false>, blocks(s.nse, 128), 128, s);
     if (nq > 0) {
         LaunchTimer lt(h, 0);
-        exclusive_scan(s.qcount, s.qoff, nq, s.scan_tmp, s.nc_raw, h->stream, h->pdl);
+        exclusive_scan(s.qcount, s.qoff, nq, s.scan_tmp, s.nc_raw, h->cstream, h->pdl);
         h->launch_counter += 3;
     } else {
-        cudaMemsetAsync(s.nc_raw, 0, sizeof(int), h->stream);
+        cudaMemsetAsync(s.nc_raw, 0, sizeof(int), h->cstream);
     }
     LAUNCH(k_set_count, 1, 1, s);
     if (s.nsv > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_dcd_vf<true>, blocks(s.nsv, 128), 128, s);
     if (s.nse > 0) LAUNCH_P(ADMM_KERNEL_DCD_EE, k_dcd_ee<true>, blocks(s.nse, 128), 128, s);
-    cudaMemsetAsync(s.vcnt, 0, sizeof(int) * s.n, h->stream);
-    cudaMemsetAsync(s.vfill, 0, sizeof(int) * s.n, h->stream);
+    cudaMemsetAsync(s.vcnt, 0, sizeof(int) * s.n, h->cstream);
+    cudaMemsetAsync(s.vfill, 0, sizeof(int) * s.n, h->cstream);
     LAUNCH(k_contact_count, h->contact_grid, kContactThreads, s);
     {
         LaunchTimer lt(h, 0);
-        exclusive_scan(s.vcnt, s.vstart, s.n, s.scan_tmp, s.vstart + s.n, h->stream, h->pdl);
+        exclusive_scan(s.vcnt, s.vstart, s.n, s.scan_tmp, s.vstart + s.n, h->cstream, h->pdl);
         h->launch_counter += 3;
     }
     LAUNCH(k_contact_fill, h->contact_grid, kContactThreads, s);
@@ -440,10 +446,102 @@ int autotune_ell(AdmmB200* h, const Assembly& as, int fixed, int* chosen_a, int*
 void enqueue_residual(AdmmB200* h) {
     DevScene& s = h->s;
     h->phase = ADMM_PHASE_RESIDUAL;
-    cudaMemsetAsync(s.res, 0, sizeof(double) * 4, h->stream);
+    cudaMemsetAsync(s.res, 0, sizeof(double) * 4, h->cstream);
     const int vb = blocks(s.nd, kLocalThreads);
     const int g = h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks + vb;
     LAUNCH(k_residual, g, kLocalThreads, s, h->tet_blocks, h->tri_blocks, h->bend_blocks, h->pin_blocks);
+}
+
+// One ADMM iteration `it` of a substep (first: no dual update before it).  The
+// BVH is built by the first detection of a substep (it == 0 of the first chunk)
+// and refitted by the later ones unless bvh_refit is off.
+void enqueue_iteration(AdmmB200* h, int it, bool first, bool residual) {
+    DevScene& s = h->s;
+    if (s.contact && it % h->dcd_interval == 0) enqueue_dcd(h, !h->bvh_refit || first);
+    enqueue_local(h, first ? LOCAL_PROX : (LOCAL_PROX | LOCAL_DUAL));
+    if (s.contact) enqueue_contact(h, !first);
+    enqueue_global(h, residual);
+    if (residual) enqueue_residual(h);
+}
+
+void enqueue_step_begin(AdmmB200* h) {
+    DevScene& s = h->s;
+    h->phase = ADMM_PHASE_PRE;
+    LAUNCH(k_pre_integration, blocks(s.n, kVertThreads), kVertThreads, s);
+    if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->cstream);
+    if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->cstream);
+}
+
+void enqueue_step_end(AdmmB200* h) {
+    DevScene& s = h->s;
+    enqueue_local(h, LOCAL_DUAL);
+    h->phase = ADMM_PHASE_FINAL;
+    LAUNCH(k_vertex_final, blocks(s.n, kVertThreads), kVertThreads, s);
+}
+
+// Eager substep with the convergence test (profiling): the host reads the
+// decision of k_check_converged after every chunk.
+int run_step_tol_eager(AdmmB200* h, float tol) {
+    DevScene& s = h->s;
+    enqueue_step_begin(h);
+    cudaMemsetAsync(s.done, 0, sizeof(int) * 4, h->cstream);
+    const int k = h->chunk;
+    for (int c = 0;; c++) {
+        for (int it = 0; it < k; it++) enqueue_iteration(h, it, c == 0 && it == 0, it == k - 1);
+        LAUNCH(k_check_converged, 1, 32, s, cudaGraphConditionalHandle(0), tol, k, h->admm_max_iter, 0);
+        int more = 0;
+        CK(cudaMemcpyAsync(&more, s.done + 1, sizeof(int), cudaMemcpyDeviceToHost, h->cstream));
+        CK(cudaStreamSynchronize(h->cstream));
+        if (!more) break;
+    }
+    enqueue_step_end(h);
+    return ADMM_OK;
+}
+
+// Substep with a convergence test (residual_tol > 0): the first chunk of
+// h->chunk iterations, then a WHILE node of the graph whose body runs further
+// chunks while k_check_converged keeps its condition set.
+int enqueue_step_tol(AdmmB200* h, float tol) {
+    DevScene& s = h->s;
+    enqueue_step_begin(h);
+    cudaMemsetAsync(s.done, 0, sizeof(int) * 4, h->cstream);
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamGetCaptureInfo(h->cstream, &cst, nullptr, &g, nullptr, nullptr));
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    const int k = h->chunk;
+    for (int it = 0; it < k; it++) enqueue_iteration(h, it, it == 0, it == k - 1);
+    LAUNCH(k_check_converged, 1, 32, s, cond, tol, k, h->admm_max_iter, 1);
+    // WHILE node after everything captured so far
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(h->cstream, &cst, nullptr, &g, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CK(cudaGraphAddNode(&wnode, g, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    // the body: one more chunk, captured from a second stream into the body graph
+    cudaStream_t parent = h->cstream;
+    h->cstream = h->body_stream;
+    h->in_body = true;
+    const int before = h->launch_counter;
+    CK(cudaStreamBeginCaptureToGraph(h->cstream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < k; it++) enqueue_iteration(h, it, false, it == k - 1);
+    LAUNCH(k_check_converged, 1, 32, s, cond, tol, k, h->admm_max_iter, 1);
+    h->kernels_body = h->launch_counter - before;
+    h->launch_counter = before;
+    h->in_body = false;
+    cudaGraph_t bg = nullptr;
+    CK(cudaStreamEndCapture(h->cstream, &bg));
+    h->cstream = parent;
+    CK(cudaStreamUpdateCaptureDependencies(h->cstream, &wnode, 1, cudaStreamSetCaptureDependencies));
+    enqueue_step_end(h);
+    return ADMM_OK;
 }
 
 // One substep (ADMMImplGPU::step).  The residual of the last iteration is kept.
@@ -451,16 +549,9 @@ void enqueue_step(AdmmB200* h) {
     DevScene& s = h->s;
     h->phase = ADMM_PHASE_PRE;
     LAUNCH(k_pre_integration, blocks(s.n, kVertThreads), kVertThreads, s);
-    if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->stream);
-    if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->stream);
-    for (int it = 0; it < h->admm_max_iter; it++) {
-        const bool first = it == 0, last = it == h->admm_max_iter - 1;
-        if (s.contact && it % h->dcd_interval == 0) enqueue_dcd(h, !h->bvh_refit || it == 0);
-        enqueue_local(h, first ? LOCAL_PROX : (LOCAL_PROX | LOCAL_DUAL));
-        if (s.contact) enqueue_contact(h, !first);
-        enqueue_global(h, last);
-        if (last) enqueue_residual(h);
-    }
+    if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->cstream);
+    if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->cstream);
+    for (int it = 0; it < h->admm_max_iter; it++) enqueue_iteration(h, it, it == 0, it == h->admm_max_iter - 1);
     if (h->admm_max_iter > 0) enqueue_local(h, LOCAL_DUAL);
     h->phase = ADMM_PHASE_FINAL;
     LAUNCH(k_vertex_final, blocks(s.n, kVertThreads), kVertThreads, s);
@@ -474,11 +565,19 @@ int build_step_graph(AdmmB200* h) {
     }
     h->probe_used = 0;
     cudaGraph_t g = nullptr;
+    h->cstream = h->stream;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     h->launch_counter = 0;
-    enqueue_step(h);
+    int rc = ADMM_OK;
+    if (h->residual_tol > 0.f) rc = enqueue_step_tol(h, h->residual_tol);
+    else enqueue_step(h);
     h->kernels_per_step = h->launch_counter;
-    CK(cudaStreamEndCapture(h->stream, &g));
+    cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
+    if (rc != ADMM_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    CK(ee);
     cudaError_t e = cudaGraphInstantiate(&h->step_exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(h, ADMM_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
@@ -720,6 +819,14 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     if (h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks == 0) return fail(h, ADMM_ERR_INVALID, "no constraints");
 
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking));
+    h->cstream = h->stream;
+    {
+        const int every = d->residual_check_every > 0 ? d->residual_check_every : h->dcd_interval;
+        h->chunk = (every + h->dcd_interval - 1) / h->dcd_interval * h->dcd_interval;
+        if (h->residual_tol > 0.f && h->chunk > h->admm_max_iter)
+            return fail(h, ADMM_ERR_INVALID, "residual_check_every/dcd_interval exceed admm_max_iter");
+    }
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
     TRY(upload_state(h, h->x_init, h->v_init));
@@ -818,6 +925,7 @@ void admm_b200_destroy(AdmmB200* h) {
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->body_stream) cudaStreamDestroy(h->body_stream);
     delete h;
 }
 
@@ -830,7 +938,9 @@ int admm_b200_step_async(AdmmB200* h, int n_steps) {
         CK(cudaEventRecord(h->ev0, h->stream));
         for (int k = 0; k < n_steps; k++) {
             h->prof_used = 0;
-            enqueue_step(h);
+            h->cstream = h->stream;
+            if (h->residual_tol > 0.f) TRY(run_step_tol_eager(h, h->residual_tol));
+            else enqueue_step(h);
             CK(cudaGetLastError());
             CK(cudaStreamSynchronize(h->stream));
             TRY(accumulate_timers(h));
@@ -867,6 +977,8 @@ int admm_b200_step(AdmmB200* h, int n_steps, AdmmStepStats* stats) {
     int nc = 0;
     CK(cudaMemcpy(&nc, h->s.nc, sizeof(int), cudaMemcpyDeviceToHost));
     h->peak = std::max(h->peak, nc);
+    h->last_iters = h->admm_max_iter;
+    if (h->residual_tol > 0.f) CK(cudaMemcpy(&h->last_iters, h->s.done, sizeof(int), cudaMemcpyDeviceToHost));
     if (stats) {
         double r[4];
         CK(cudaMemcpy(r, h->s.res, sizeof(r), cudaMemcpyDeviceToHost));
@@ -874,7 +986,7 @@ int admm_b200_step(AdmmB200* h, int n_steps, AdmmStepStats* stats) {
         stats->step_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() /
                          (n_steps > 0 ? n_steps : 1);
         stats->n_contacts = nc;
-        stats->admm_iters = h->admm_max_iter;
+        stats->admm_iters = h->last_iters;
         const double sc = r[2] > 0.0 ? std::sqrt(r[2]) : 1.0;
         stats->primal_residual = std::sqrt(r[0]) / sc;
         stats->dual_residual = std::sqrt(r[1]) / sc;
@@ -1201,6 +1313,11 @@ int admm_b200_kernels_per_step(AdmmB200* h, int* n) {
     if (!h || !n) return ADMM_ERR_INVALID;
     TRY(build_step_graph(h));
     *n = h->kernels_per_step;
+    // residual-tolerance mode: the first chunk runs outside the conditional node
+    if (h->residual_tol > 0.f && h->chunk > 0) {
+        const int it = h->last_iters > 0 ? h->last_iters : h->chunk;
+        *n += h->kernels_body * (it / h->chunk - 1);
+    }
     return ADMM_OK;
 }
 

@@ -410,4 +410,25 @@ __global__ void __launch_bounds__(kLocalThreads) k_residual(DevScene s, int tet_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Convergence test after a chunk of ADMM iterations (residual_tol > 0): counts
+// the chunk's iterations into iters[0] and keeps the WHILE node of the substep
+// graph looping while the relative primal or dual residual is above `tol` and
+// another chunk still fits in `max_iter` iterations.  One thread.
+// ---------------------------------------------------------------------------
+// The decision is also stored in done[1] (1 = another chunk), which the eager
+// (profiling) path reads on the host; in_graph = 0 skips the graph condition.
+__global__ void k_check_converged(DevScene s, cudaGraphConditionalHandle cond, float tol, int chunk, int max_iter,
+                                  int in_graph) {
+    ADMM_PDL_PROLOGUE();
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int iters = s.done[0] + chunk;
+    s.done[0] = iters;
+    const double sc = s.res[2] > 0.0 ? sqrt(s.res[2]) : 1.0;
+    const double pr = sqrt(s.res[0]) / sc, du = sqrt(s.res[1]) / sc;
+    const bool more = (pr > (double)tol || du > (double)tol) && iters + chunk <= max_iter;
+    s.done[1] = more ? 1 : 0;
+    if (in_graph) cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
 }  // namespace admm

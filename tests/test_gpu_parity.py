@@ -318,3 +318,57 @@ def test_autotuner_choice_is_valid():
     t = h.tuning()
     assert t["jacobi_lanes"] in (1, 2, 4, 8) and t["rhs_lanes"] in (1, 2, 4, 8)
     assert 0 < t["jacobi_ms"] < 10 and 0 < t["rhs_ms"] < 10
+
+
+@pytest.mark.parametrize("name,tol", [("cloth", 1e-4), ("cube_impact", 1e-4)])
+def test_tolerance_mode_matches_oracle(name, tol):
+    """residual_tol > 0: chunks of dcd_interval iterations until both relative residuals are
+    <= tol (device-side WHILE node); same iteration counts and positions as the oracle."""
+    if name == "cloth":
+        sc = scene.cloth_on_box(16)
+        x0 = v0 = None
+    else:
+        sc = scene.cube_on_ground(8, drop=0.0)
+        v0 = np.zeros_like(sc.verts)
+        v0[:sc.n_dyn, 1] = -np.sqrt(2 * 9.8)
+        x0 = sc.verts.copy()
+        x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.02
+    sc.params.admm_max_iter = 60
+    h, o = _setup(sc, residual_tol=tol)
+    if x0 is not None:
+        h.set_state(x0, v0)
+        for b, a in ((B.BUF_X0, x0), (B.BUF_X, x0), (B.BUF_V, v0)):
+            o.write(b, a)
+    ext = np.ptp(sc.verts[:sc.n_dyn], axis=0).max()
+    for k in range(2):
+        sg = h.step(1)
+        so = o.step(1)
+        assert sg["iters"] % sc.params.dcd_interval == 0 and 0 < sg["iters"] <= 60
+        assert sg["iters"] == so["iters"], (k, sg, so)
+        if sg["iters"] < 60:
+            assert sg["primal"] <= tol and sg["dual"] <= tol
+        xg, _ = h.get_state()
+        assert np.abs(xg - o.read(B.BUF_X0)).max() / ext <= TOL_LONG
+
+
+def test_tolerance_mode_eager_matches_graph():
+    """The eager (profiling) path of residual_tol mode takes the same decisions on the host as
+    the conditional graph node on the device, and the launch count follows the chunks run."""
+    sc = scene.cloth_on_box(16)
+    sc.params.admm_max_iter = 40
+    hg = B.Handle(sc, residual_tol=1e-4)
+    he = B.Handle(sc, residual_tol=1e-4)
+    he.set_profiling(True)
+    k_min = hg.kernels_per_step()
+    for _ in range(3):
+        sg = hg.step(1)
+        se = he.step(1)
+        assert sg["iters"] == se["iters"]
+        xg, _ = hg.get_state()
+        xe, _ = he.get_state()
+        np.testing.assert_array_equal(xg, xe)
+        chunks = sg["iters"] // sc.params.dcd_interval
+        k = hg.kernels_per_step()
+        assert (k > k_min) == (chunks > 1)
+    hg.close()
+    he.close()
