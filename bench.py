@@ -237,6 +237,8 @@ def main():
     ap.add_argument("--probe", default="local", choices=["local", "jacobi", "rhs"])
     ap.add_argument("--cpu-stride", type=int, default=10, help="CPU-baseline sample: one substep every N frames")
     ap.add_argument("--tol", type=float, default=1e-4, help="ADMM residual tolerance (0 = fixed iteration count)")
+    ap.add_argument("--jacobi-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="global step: 0 autotuned, 1 one kernel per sweep, 2 persistent kernel")
     ap.add_argument("--ref-steps", type=int, default=200, help="cap on steps timed by --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="also print a per-phase kernel-time breakdown")
@@ -259,6 +261,7 @@ def main():
     from parallel_admm_b200 import backend as B
 
     sc = make_scene(args.config)
+    sc.params.jacobi_mode = args.jacobi_mode
     h = B.Handle(sc, device=local, residual_tol=args.tol)
     h.set_probe(args.probe)
     for _ in range(args.warmup):
@@ -327,11 +330,17 @@ def main():
 
     phases = None
     if args.profile and rank == 0:
+        # device time per phase inside the step graph (events at phase changes), same frames;
+        # with a residual tolerance only the first chunk of each step is covered
         h.reset()
-        h.set_profiling(True)
-        h.step(min(args.steps, 20), allow=(B.ERR_CONTACT_OVERFLOW,))
-        phases = h.phase_times()
-        h.set_profiling(False)
+        h.set_probe("phases")
+        h.phase_times()
+        for _ in range(args.steps):
+            h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+        phases = {k: {"ms_per_step": v["ms"] / args.steps, "launches_per_step": v["launches"] / args.steps}
+                  for k, v in h.phase_times().items()}
+        phases["scope"] = "first chunk of each step" if args.tol > 0 else "whole step"
+        h.set_probe(args.probe)
 
     if world > 1:
         dist.destroy_process_group()

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define ADMM_B200_ABI_VERSION 1
+#define ADMM_B200_ABI_VERSION 2
 
 /* status codes */
 #define ADMM_OK                    0
@@ -36,6 +36,7 @@ extern "C" {
 #define ADMM_ERR_NOT_CONVERGED    -7  /* residual tolerance not reached at max_iter    */
 #define ADMM_ERR_NO_DEVICE        -8  /* no usable sm_100 device                       */
 #define ADMM_ERR_STATE            -9  /* call out of order (e.g. step before create)   */
+#define ADMM_ERR_TIMEOUT         -10  /* a bounded device-side wait gave up            */
 
 typedef struct AdmmB200 AdmmB200; /* opaque handle */
 
@@ -105,6 +106,16 @@ typedef struct AdmmB200Desc {
      * autotuner at create (cached per process and matrix shape, so handles of the
      * same scene sum in the same order). */
     int32_t ell_lanes;
+    /* How the global step runs: 0 = chosen by the autotuner at create; 1 = one
+     * kernel for the right-hand side and one per Jacobi sweep; 2 = one persistent
+     * kernel for the right-hand side and all sweeps, its blocks synchronised
+     * through per-block sweep counters (falls back to 1 when the device cannot
+     * hold all blocks at once or jacobi_iter < 2).  Both give identical bits. */
+    int32_t jacobi_mode;
+    /* Broad phase of the DCD: 0 = default (2); 1 = LBVH (the reference's
+     * structure, bvh_refit applies); 2 = uniform-grid spatial hash.  Both report
+     * the same pair set; the order of the contact list differs. */
+    int32_t broad_phase;
 } AdmmB200Desc;
 
 /* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */
@@ -238,6 +249,10 @@ int  admm_b200_step_host(AdmmB200* h, const float* x_in, const float* v_in, floa
 #define ADMM_KERNEL_CONTACT_GATHER  5
 #define ADMM_KERNEL_DCD_VF          6
 #define ADMM_KERNEL_DCD_EE          7
+/* set_probe argument: events at every phase change of the substep graph (outside
+ * a residual_tol loop body); admm_b200_phase_times then returns the device time
+ * between changes per phase, launch gaps included. */
+#define ADMM_PROBE_PHASES         100
 
 /* Device time (CUDA events on the handle's stream) per substep of the last
  * admm_b200_step call. */
@@ -260,6 +275,10 @@ int  admm_b200_kernels_per_step(AdmmB200* h, int* n);
 /* Autotuner choices made at create: lanes per row of the sliced-ELL copies of
  * A (Jacobi) and h^2 D^T W^2 (right-hand side), and the measured ms per launch. */
 int  admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float* ms_r);
+/* How the global step runs (jacobi_mode): persistent = 1 for the one-kernel
+ * global step (blocks = its grid), 0 for one kernel per sweep; the autotuner's
+ * ms per global step in both modes (0 when not timed). */
+int  admm_b200_global_mode(AdmmB200* h, int* persistent, int* blocks, float* ms_sweeps, float* ms_persist);
 
 /* --- allocation-free Jacobi solve (no counterpart in the reference) ---
  * For callers that cannot allocate device memory themselves or through a handle

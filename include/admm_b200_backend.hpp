@@ -32,7 +32,9 @@ public:
     bool finalized = false;
     bool sync_to_host = true;
     int device = 0;
-    int ell_lanes = 0;  // 0 = autotuned
+    int ell_lanes = 0;    // 0 = autotuned
+    int jacobi_mode = 0;  // 0 = autotuned
+    int broad_phase = 0;  // 0 = default (uniform grid)
 
     ~ADMMInnerB200() override {
         if (h_) admm_b200_destroy(h_);
@@ -189,6 +191,8 @@ private:
         d.residual_check_every = 0;
         d.bvh_refit = 1;
         d.ell_lanes = ell_lanes;
+        d.jacobi_mode = jacobi_mode;
+        d.broad_phase = broad_phase;
     }
 };
 

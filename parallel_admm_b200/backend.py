@@ -21,7 +21,7 @@ from .scene import Scene
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libadmm_b200.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 OK = 0
 ERR_INVALID = -1
 ERR_CUDA = -2
@@ -32,11 +32,12 @@ ERR_NAN = -6
 ERR_NOT_CONVERGED = -7
 ERR_NO_DEVICE = -8
 ERR_STATE = -9
+ERR_TIMEOUT = -10
 
 BUF_X, BUF_X0, BUF_V, BUF_P, BUF_UC, BUF_UE, BUF_Z, BUF_B, BUF_MXT = range(9)
 PHASES = ("pre", "dcd", "local", "contact", "rhs", "jacobi", "residual", "final")
 KERNELS = {"none": 0, "local": 1, "jacobi": 2, "rhs": 3, "contact_du": 4, "contact_gather": 5,
-           "dcd_vf": 6, "dcd_ee": 7}
+           "dcd_vf": 6, "dcd_ee": 7, "phases": 100}
 
 _f = ctypes.POINTER(ctypes.c_float)
 _i = ctypes.POINTER(ctypes.c_int32)
@@ -70,7 +71,8 @@ class AdmmB200Desc(ctypes.Structure):
         ("jacobi_iter", ctypes.c_int32), ("max_contacts", ctypes.c_int32),
         ("enable_contact", ctypes.c_int32), ("warmstart_ue", ctypes.c_int32), ("warmstart_uc", ctypes.c_int32),
         ("residual_tol", ctypes.c_float), ("residual_check_every", ctypes.c_int32),
-        ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32),
+        ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32), ("jacobi_mode", ctypes.c_int32),
+        ("broad_phase", ctypes.c_int32),
     ]
 
 
@@ -133,6 +135,8 @@ class DescHolder:
         d.residual_tol, d.residual_check_every = 0.0, 0
         d.bvh_refit = int(p.bvh_refit)
         d.ell_lanes = int(p.ell_lanes)
+        d.jacobi_mode = int(p.jacobi_mode)
+        d.broad_phase = int(p.broad_phase)
         for k, v in overrides.items():
             setattr(d, k, v)
         self.desc = d
@@ -185,6 +189,7 @@ def lib():
             "admm_b200_set_probe": (ctypes.c_int, [vp, ctypes.c_int]),
             "admm_b200_probe_time": (ctypes.c_int, [vp, _d, ctypes.POINTER(ctypes.c_int64)]),
             "admm_b200_tuning": (ctypes.c_int, [vp, _i, _i, _f, _f]),
+            "admm_b200_global_mode": (ctypes.c_int, [vp, _i, _i, _f, _f]),
             "admm_b200_jacobi_noalloc": (ctypes.c_int, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int,
                                                         vp]),
         }
@@ -208,7 +213,7 @@ def exported_symbols():
         "admm_b200_clear_contacts", "admm_b200_residuals", "admm_b200_last_step_device_ms",
         "admm_b200_set_profiling", "admm_b200_kernels_per_step", "admm_b200_step_host",
         "admm_b200_phase_times", "admm_b200_set_probe", "admm_b200_probe_time", "admm_b200_tuning",
-        "admm_b200_jacobi_noalloc",
+        "admm_b200_jacobi_noalloc", "admm_b200_global_mode",
     ]
 
 
@@ -377,6 +382,14 @@ class Handle:
         self.check(lib().admm_b200_tuning(self.h, ctypes.byref(la), ctypes.byref(lr), ctypes.byref(ma),
                                           ctypes.byref(mr)), "tuning")
         return {"jacobi_lanes": la.value, "rhs_lanes": lr.value, "jacobi_ms": ma.value, "rhs_ms": mr.value}
+
+    def global_mode(self) -> Dict[str, float]:
+        """Global-step mode: persistent kernel (and its grid) or one kernel per sweep."""
+        pe, nb = ctypes.c_int32(), ctypes.c_int32()
+        ms, mp = ctypes.c_float(), ctypes.c_float()
+        self.check(lib().admm_b200_global_mode(self.h, ctypes.byref(pe), ctypes.byref(nb), ctypes.byref(ms),
+                                               ctypes.byref(mp)), "global_mode")
+        return {"persistent": bool(pe.value), "blocks": nb.value, "ms_sweeps": ms.value, "ms_persist": mp.value}
 
     def max_slots(self) -> int:
         n = ctypes.c_int32()

@@ -20,6 +20,7 @@
 
 #include "admm_b200.h"
 #include "contact.cuh"
+#include "grid.cuh"
 #include "kernels.cuh"
 #include "lbvh.cuh"
 #include "scan_sort.cuh"
@@ -53,6 +54,9 @@ struct AdmmB200 {
     int residual_every = 0;
     bool warmstart_ue = true, warmstart_uc = true;
     bool bvh_refit = true;
+    bool use_grid = true;           // broad phase: uniform grid (true) or LBVH
+    float grid_cell_size = 0.f;
+    int grid_buckets = 0;
     bool pdl = true;                // programmatic dependent launch between the kernels of a substep
     cudaStream_t cstream = nullptr; // stream the enqueue helpers launch on (capture target)
     cudaStream_t body_stream = nullptr;
@@ -63,6 +67,11 @@ struct AdmmB200 {
     // autotuner choices (lanes per row of the sliced-ELL matrices) and their times
     int tune_lanes_a = 1, tune_lanes_r = 1;
     float tune_ms_a = 0.f, tune_ms_r = 0.f;
+    // global step: persistent kernel (RHS + all sweeps) or one kernel per sweep
+    PersistPlan pp;
+    bool persist_ok = false;        // plan built and all blocks fit on the device at once
+    bool persist = false;           // chosen mode
+    float tune_ms_persist = 0.f, tune_ms_sweeps = 0.f;  // one global step, both modes
     // host-buffer stepping
     float* stage = nullptr;    // [6n] row-major x then v
     // profiling: eager launches with one event pair per launch, tagged by phase
@@ -74,7 +83,10 @@ struct AdmmB200 {
     double phase_ms[ADMM_NUM_PHASES] = {0};
     int64_t phase_launches[ADMM_NUM_PHASES] = {0};
     // probes: event pairs captured into the step graph around one kernel class
-    int probe_kernel = 0;
+    int probe_kernel = 0;           // ADMM_KERNEL_* class, or ADMM_PROBE_PHASES
+    std::vector<cudaEvent_t> pev;   // phase probes: one event at every phase change of the graph
+    std::vector<int> pev_phase, pev_launch;
+    int pev_used = 0;
     std::vector<cudaEvent_t> probe_ev;
     int probe_used = 0;
     double probe_ms = 0.0;
@@ -92,7 +104,8 @@ const char* kErrStr[] = {"ok",
                          "non-finite value",
                          "residual tolerance not reached",
                          "no usable sm_100 device",
-                         "call out of order"};
+                         "call out of order",
+                         "device-side wait timed out"};
 
 int fail(AdmmB200* h, int code, const std::string& what) {
     if (h) h->last_error = what;
@@ -202,6 +215,22 @@ struct LaunchTimer {
     }
 };
 
+constexpr int kMaxPhaseEvents = 1024;
+
+// Tags the launches that follow with phase `ph`.  With phase probes on, every
+// phase change outside the conditional body also records an event into the
+// graph, so that the device time between changes is charged to the phase.
+void set_phase(AdmmB200* h, int ph) {
+    if (h->probe_kernel == ADMM_PROBE_PHASES && !h->profiling && !h->in_body && ph != h->phase &&
+        h->pev_used < (int)h->pev.size()) {
+        cudaEventRecordWithFlags(h->pev[h->pev_used], h->cstream, cudaEventRecordExternal);
+        h->pev_phase[h->pev_used] = ph;
+        h->pev_launch[h->pev_used] = h->launch_counter;
+        h->pev_used++;
+    }
+    h->phase = ph;
+}
+
 #define LAUNCH_P(pid, kernel, grid, block, ...)                                      \
     do {                                                                             \
         LaunchTimer lt_(h, (pid));                                                   \
@@ -237,18 +266,34 @@ void enqueue_build(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tr
 // rebuild = false refits the trees of the previous build.
 void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
     DevScene& s = h->s;
-    h->phase = ADMM_PHASE_DCD;
-    if (rebuild) {
-        LAUNCH(k_scene_init, 1, 32, s.bf, s.be);
-        enqueue_build(h, s.bf, (const int*)s.st, 4, true);
-        enqueue_build(h, s.be, (const int*)s.se, 2, false);
-    } else {
-        enqueue_refit(h, s.bf, (const int*)s.st, 4, true);
-        enqueue_refit(h, s.be, (const int*)s.se, 2, false);
-    }
+    set_phase(h, ADMM_PHASE_DCD);
     const int nq = s.nsv + s.nse;
-    if (s.nsv > 0) LAUNCH(k_dcd_vf<false>, blocks(s.nsv, 128), 128, s);
-    if (s.nse > 0) LAUNCH(k_dcd_ee<false>, blocks(s.nse, 128), 128, s);
+    if (h->use_grid) {
+        const int ne = s.nst + s.nse;
+        cudaMemsetAsync(s.grid.ctr, 0, sizeof(int) * 4, h->cstream);
+        if (ne > 0) {
+            LAUNCH(k_grid_count, blocks(ne, 256), 256, s);
+            {
+                LaunchTimer lt(h, 0);
+                exclusive_scan(s.grid.cnt, s.grid.start, h->grid_buckets, s.scan_tmp, s.grid.start + h->grid_buckets,
+                               h->cstream, h->pdl);
+                h->launch_counter += 3;
+            }
+            LAUNCH(k_grid_scatter, blocks(ne, 256), 256, s);
+        }
+        if (nq > 0) LAUNCH(k_grid_query<false>, blocks(nq, 128), 128, s);
+    } else {
+        if (rebuild) {
+            LAUNCH(k_scene_init, 1, 32, s.bf, s.be);
+            enqueue_build(h, s.bf, (const int*)s.st, 4, true);
+            enqueue_build(h, s.be, (const int*)s.se, 2, false);
+        } else {
+            enqueue_refit(h, s.bf, (const int*)s.st, 4, true);
+            enqueue_refit(h, s.be, (const int*)s.se, 2, false);
+        }
+        if (s.nsv > 0) LAUNCH(k_dcd_vf<false>, blocks(s.nsv, 128), 128, s);
+        if (s.nse > 0) LAUNCH(k_dcd_ee<false>, blocks(s.nse, 128), 128, s);
+    }
     if (nq > 0) {
         LaunchTimer lt(h, 0);
         exclusive_scan(s.qcount, s.qoff, nq, s.scan_tmp, s.nc_raw, h->cstream, h->pdl);
@@ -257,8 +302,12 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
         cudaMemsetAsync(s.nc_raw, 0, sizeof(int), h->cstream);
     }
     LAUNCH(k_set_count, 1, 1, s);
-    if (s.nsv > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_dcd_vf<true>, blocks(s.nsv, 128), 128, s);
-    if (s.nse > 0) LAUNCH_P(ADMM_KERNEL_DCD_EE, k_dcd_ee<true>, blocks(s.nse, 128), 128, s);
+    if (h->use_grid) {
+        if (nq > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_grid_query<true>, blocks(nq, 128), 128, s);
+    } else {
+        if (s.nsv > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_dcd_vf<true>, blocks(s.nsv, 128), 128, s);
+        if (s.nse > 0) LAUNCH_P(ADMM_KERNEL_DCD_EE, k_dcd_ee<true>, blocks(s.nse, 128), 128, s);
+    }
     cudaMemsetAsync(s.vcnt, 0, sizeof(int) * s.n, h->cstream);
     cudaMemsetAsync(s.vfill, 0, sizeof(int) * s.n, h->cstream);
     LAUNCH(k_contact_count, h->contact_grid, kContactThreads, s);
@@ -274,7 +323,7 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
 
 void enqueue_local(AdmmB200* h, int mode) {
     const int g = h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks;
-    h->phase = ADMM_PHASE_LOCAL;
+    set_phase(h, ADMM_PHASE_LOCAL);
     if (mode == LOCAL_PROX)
         LAUNCH_P(ADMM_KERNEL_LOCAL, k_local<LOCAL_PROX>, g, kLocalThreads, h->s, h->tet_blocks, h->tri_blocks, h->bend_blocks);
     else if (mode == (LOCAL_PROX | LOCAL_DUAL))
@@ -287,7 +336,7 @@ void enqueue_local(AdmmB200* h, int mode) {
 void enqueue_contact(AdmmB200* h, bool dual) {
     DevScene& s = h->s;
     const int vb = blocks(s.nd, kVertThreads);
-    h->phase = ADMM_PHASE_CONTACT;
+    set_phase(h, ADMM_PHASE_CONTACT);
     if (dual) LAUNCH((k_contact_p<true, true>), vb, kVertThreads, s);
     else LAUNCH((k_contact_p<false, true>), vb, kVertThreads, s);
     for (int g = 0; g < h->gs_iter; g++) {
@@ -323,11 +372,53 @@ void launch_rhs(AdmmB200* h, bool save_prev) {
 #undef RHS_CASE
 }
 
+// The persistent global step: RHS (when rhs) and `sweeps` >= 2 Jacobi sweeps in
+// one cooperative launch, no programmatic early start (its blocks spin).
+void launch_persist(AdmmB200* h, bool rhs, bool save_prev, int sweeps) {
+    DevScene& s = h->s;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(h->pp.blocks);
+    cfg.blockDim = dim3(kPersistThreads);
+    cfg.stream = h->cstream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    LaunchTimer lt_(h, ADMM_KERNEL_JACOBI);
+    void (*k)(DevScene, PersistPlan, int) = nullptr;
+#define PERSIST_R(T, TR)                                              \
+    k = !rhs ? k_global_persist<T, TR, false, false>                  \
+        : save_prev ? k_global_persist<T, TR, true, true>             \
+                    : k_global_persist<T, TR, true, false>;
+#define PERSIST_A(T)                                   \
+    switch (s.R.lanes) {                               \
+        case 1: PERSIST_R(T, 1) break;                 \
+        case 2: PERSIST_R(T, 2) break;                 \
+        case 4: PERSIST_R(T, 4) break;                 \
+        default: PERSIST_R(T, 8) break;                \
+    }
+    switch (s.A.lanes) {
+        case 1: PERSIST_A(1) break;
+        case 2: PERSIST_A(2) break;
+        case 4: PERSIST_A(4) break;
+        default: PERSIST_A(8) break;
+    }
+#undef PERSIST_A
+#undef PERSIST_R
+    cudaLaunchKernelEx(&cfg, k, s, h->pp, sweeps);
+    h->launch_counter++;
+}
+
 void enqueue_jacobi(AdmmB200* h, int sweeps) {
     DevScene& s = h->s;
     const int vb = blocks(s.nd, kVertThreads);
-    h->phase = ADMM_PHASE_JACOBI;
+    set_phase(h, ADMM_PHASE_JACOBI);
     if (sweeps <= 0) return;
+    if (h->persist && sweeps >= 2) {
+        launch_persist(h, false, false, sweeps);
+        return;
+    }
     if (sweeps == 1) {
         launch_jacobi(h, s.x, s.jac[0]);
         LAUNCH(k_copy_dyn, vb, kVertThreads, s, s.jac[0], s.x);
@@ -341,9 +432,88 @@ void enqueue_jacobi(AdmmB200* h, int sweeps) {
 }
 
 void enqueue_global(AdmmB200* h, bool save_prev) {
-    h->phase = ADMM_PHASE_RHS;
+    if (h->persist && h->jac_iter >= 2) {
+        set_phase(h, ADMM_PHASE_JACOBI);
+        launch_persist(h, true, save_prev, h->jac_iter);
+        return;
+    }
+    set_phase(h, ADMM_PHASE_RHS);
     launch_rhs(h, save_prev);
     enqueue_jacobi(h, h->jac_iter);
+}
+
+// Persistent-kernel plan: rows in blocks of a multiple of 32 (at most one block
+// per SM), and for each block the other blocks owning a column of its rows in
+// the off-diagonal pattern of A, made symmetric.
+int build_persist_plan(AdmmB200* h, const HostCsr& A) {
+    DevScene& s = h->s;
+    h->persist_ok = false;
+    if (s.nd <= 0) return ADMM_OK;
+    int sms = 0, coop = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device));
+    if (!coop || sms <= 0) return ADMM_OK;
+    const int groups = (s.nd + 31) / 32;
+    const int per = (groups + sms - 1) / sms;
+    const int rb = 32 * per;
+    const int nb = (s.nd + rb - 1) / rb;
+    std::vector<std::vector<int>> dep(nb);
+    for (int i = 0; i < s.nd; i++) {
+        const int gi = i / rb;
+        for (int k = A.start[i]; k < A.start[i + 1]; k++) {
+            const int gj = A.col[k] / rb;
+            if (gj != gi) {
+                dep[gi].push_back(gj);
+                dep[gj].push_back(gi);
+            }
+        }
+    }
+    std::vector<int> ptr(nb + 1, 0), idx;
+    for (int g = 0; g < nb; g++) {
+        auto& v = dep[g];
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        idx.insert(idx.end(), v.begin(), v.end());
+        ptr[g + 1] = (int)idx.size();
+    }
+    int *dp = nullptr, *di = nullptr;
+    unsigned* ep = nullptr;
+    TRY(dupload(h, &dp, ptr.data(), ptr.size()));
+    TRY(dupload(h, &di, idx.data(), idx.size()));
+    TRY(dalloc(h, &ep, nb));
+    h->pp.blocks = nb;
+    h->pp.rows_per_block = rb;
+    h->pp.dep_ptr = dp;
+    h->pp.dep_idx = di;
+    h->pp.epoch = ep;
+    h->pp.spin_limit = 1 << 22;  // ~1-2 s of polling
+    // every instantiation has the same launch bounds (kPersistThreads, 1 block per SM)
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_global_persist<8, 8, true, true>, kPersistThreads, 0));
+    h->persist_ok = per_sm >= 1 && nb <= per_sm * sms;
+    return ADMM_OK;
+}
+
+// Milliseconds of one global step (RHS + jac_iter sweeps), eager, in either mode.
+int time_global(AdmmB200* h, bool persist, float* ms) {
+    const bool keep = h->persist;
+    h->persist = persist;
+    h->cstream = h->stream;
+    enqueue_global(h, false);
+    CK(cudaEventRecord(h->ev0, h->stream));
+    constexpr int kReps = 8;
+    for (int r = 0; r < kReps; r++) enqueue_global(h, false);
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    h->persist = keep;
+    CK(cudaGetLastError());
+    int e[4] = {0, 0, 0, 0};
+    CK(cudaMemcpy(e, h->s.err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e[3]) return fail(h, ADMM_ERR_TIMEOUT, "persistent global step: a block wait timed out");
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    *ms = t / kReps;
+    return ADMM_OK;
 }
 
 int upload_ell(AdmmB200* h, const HostCsr& c, int rows, int lanes, SlicedEll& out, HostEll* keep = nullptr) {
@@ -445,7 +615,7 @@ int autotune_ell(AdmmB200* h, const Assembly& as, int fixed, int* chosen_a, int*
 
 void enqueue_residual(AdmmB200* h) {
     DevScene& s = h->s;
-    h->phase = ADMM_PHASE_RESIDUAL;
+    set_phase(h, ADMM_PHASE_RESIDUAL);
     cudaMemsetAsync(s.res, 0, sizeof(double) * 4, h->cstream);
     const int vb = blocks(s.nd, kLocalThreads);
     const int g = h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks + vb;
@@ -466,7 +636,7 @@ void enqueue_iteration(AdmmB200* h, int it, bool first, bool residual) {
 
 void enqueue_step_begin(AdmmB200* h) {
     DevScene& s = h->s;
-    h->phase = ADMM_PHASE_PRE;
+    set_phase(h, ADMM_PHASE_PRE);
     LAUNCH(k_pre_integration, blocks(s.n, kVertThreads), kVertThreads, s);
     if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->cstream);
     if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->cstream);
@@ -475,7 +645,7 @@ void enqueue_step_begin(AdmmB200* h) {
 void enqueue_step_end(AdmmB200* h) {
     DevScene& s = h->s;
     enqueue_local(h, LOCAL_DUAL);
-    h->phase = ADMM_PHASE_FINAL;
+    set_phase(h, ADMM_PHASE_FINAL);
     LAUNCH(k_vertex_final, blocks(s.n, kVertThreads), kVertThreads, s);
 }
 
@@ -547,23 +717,29 @@ int enqueue_step_tol(AdmmB200* h, float tol) {
 // One substep (ADMMImplGPU::step).  The residual of the last iteration is kept.
 void enqueue_step(AdmmB200* h) {
     DevScene& s = h->s;
-    h->phase = ADMM_PHASE_PRE;
+    set_phase(h, ADMM_PHASE_PRE);
     LAUNCH(k_pre_integration, blocks(s.n, kVertThreads), kVertThreads, s);
     if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->cstream);
     if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->cstream);
     for (int it = 0; it < h->admm_max_iter; it++) enqueue_iteration(h, it, it == 0, it == h->admm_max_iter - 1);
     if (h->admm_max_iter > 0) enqueue_local(h, LOCAL_DUAL);
-    h->phase = ADMM_PHASE_FINAL;
+    set_phase(h, ADMM_PHASE_FINAL);
     LAUNCH(k_vertex_final, blocks(s.n, kVertThreads), kVertThreads, s);
 }
 
-int build_step_graph(AdmmB200* h) {
-    if (h->step_exec) return ADMM_OK;
-    if (h->probe_kernel != 0 && h->probe_ev.empty()) {
+int build_step_graph_once(AdmmB200* h) {
+    if (h->probe_kernel == ADMM_PROBE_PHASES && h->pev.empty()) {
+        h->pev.resize(kMaxPhaseEvents);
+        h->pev_phase.resize(kMaxPhaseEvents);
+        h->pev_launch.resize(kMaxPhaseEvents);
+        for (auto& e : h->pev) CK(cudaEventCreate(&e));
+    } else if (h->probe_kernel != 0 && h->probe_kernel != ADMM_PROBE_PHASES && h->probe_ev.empty()) {
         h->probe_ev.resize(2 * kMaxProbes);
         for (auto& e : h->probe_ev) CK(cudaEventCreate(&e));
     }
     h->probe_used = 0;
+    h->pev_used = 0;
+    h->phase = -1;
     cudaGraph_t g = nullptr;
     h->cstream = h->stream;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -571,6 +747,7 @@ int build_step_graph(AdmmB200* h) {
     int rc = ADMM_OK;
     if (h->residual_tol > 0.f) rc = enqueue_step_tol(h, h->residual_tol);
     else enqueue_step(h);
+    set_phase(h, ADMM_NUM_PHASES);  // closes the last phase
     h->kernels_per_step = h->launch_counter;
     cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
     if (rc != ADMM_OK) {
@@ -580,8 +757,35 @@ int build_step_graph(AdmmB200* h) {
     CK(ee);
     cudaError_t e = cudaGraphInstantiate(&h->step_exec, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) return fail(h, ADMM_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        h->step_exec = nullptr;
+        return fail(h, ADMM_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
     return ADMM_OK;
+}
+
+// Captures and instantiates the substep graph.  Should the runtime refuse the
+// cooperative persistent kernel inside a graph (or inside a conditional body),
+// the graph is built again with one kernel per sweep.
+int build_step_graph(AdmmB200* h) {
+    if (h->step_exec) return ADMM_OK;
+    const int rc = build_step_graph_once(h);
+    if (rc == ADMM_OK || !h->persist) return rc;
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    for (cudaStream_t st : {h->body_stream, h->stream})
+        if (cudaStreamIsCapturing(st, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+            g = nullptr;
+        }
+    cudaGetLastError();
+    h->cstream = h->stream;
+    h->in_body = false;
+    fprintf(stderr, "admm_b200: persistent global step not capturable (%s); using one kernel per sweep\n",
+            h->last_error.c_str());
+    h->persist = false;
+    return build_step_graph_once(h);
 }
 
 float4 pack(const float* p) { return make_float4(p[0], p[1], p[2], 0.f); }
@@ -609,6 +813,69 @@ int upload_state(AdmmB200* h, const std::vector<float4>& x, const std::vector<fl
     CK(cudaMemcpyAsync(s.x, x.data(), sizeof(float4) * s.n, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(s.v, v.data(), sizeof(float4) * s.n, cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    return ADMM_OK;
+}
+
+// Grid parameters from the rest shape: cell edge = max(2.05 x thickness, 1.5 x
+// the median of the surface elements' largest box extent), so that a vertex
+// query spans at most 2 cells per axis and most elements 1-2, while a few large
+// elements (a ground plane, a collider box) go to the big lists; buckets = twice
+// the rest insertions (power of two); entry capacity = 4x them (elements
+// beyond it fall back to the big lists).
+int setup_grid(AdmmB200* h, const AdmmB200Desc* d) {
+    DevScene& s = h->s;
+    GridDev& g = s.grid;
+    const int ne = s.nst + s.nse;
+    std::vector<float> ext;
+    std::vector<float4> lo(ne), up(ne);
+    ext.reserve(ne);
+    auto box = [&](int u, const int* v, int nv) {
+        float4 a = make_float4(1e32f, 1e32f, 1e32f, 0.f), b = make_float4(-1e32f, -1e32f, -1e32f, 0.f);
+        for (int k = 0; k < nv; k++) {
+            const float4 p = h->x_init[v[k]];
+            a.x = std::min(a.x, p.x); a.y = std::min(a.y, p.y); a.z = std::min(a.z, p.z);
+            b.x = std::max(b.x, p.x); b.y = std::max(b.y, p.y); b.z = std::max(b.z, p.z);
+        }
+        lo[u] = a;
+        up[u] = b;
+        ext.push_back(std::max(b.x - a.x, std::max(b.y - a.y, b.z - a.z)));
+    };
+    for (int f = 0; f < s.nst; f++) box(f, d->surf_tris + 3 * f, 3);
+    for (int e = 0; e < s.nse; e++) box(s.nst + e, d->surf_edges + 2 * e, 2);
+    float c = 2.05f * s.thickness;
+    if (!ext.empty()) {
+        const size_t k = (ext.size() - 1) / 2;
+        std::nth_element(ext.begin(), ext.begin() + k, ext.end());
+        c = std::max(c, 1.5f * ext[k]);
+    }
+    if (!(c > 0.f) || !std::isfinite(c)) c = 1.f;
+    g.inv_c = 1.f / c;
+    h->grid_cell_size = c;
+    int64_t ins = 0;
+    for (int u = 0; u < ne; u++) {
+        int64_t cells = 1;
+        const float a[3] = {lo[u].x, lo[u].y, lo[u].z}, b[3] = {up[u].x, up[u].y, up[u].z};
+        for (int k = 0; k < 3; k++) {
+            const int64_t span = (int64_t)std::floor(b[k] * g.inv_c) - (int64_t)std::floor(a[k] * g.inv_c) + 1;
+            cells = span <= kGridMaxSpan ? cells * span : 0;
+        }
+        ins += cells;
+    }
+    int64_t nb = 1024;
+    while (nb < 2 * ins) nb <<= 1;
+    if (nb > (int64_t(1) << 28)) return fail(h, ADMM_ERR_INVALID, "collision grid too large");
+    g.hmask = (int)nb - 1;
+    h->grid_buckets = (int)nb;
+    g.cap = (int)std::min<int64_t>(4 * ins + 4096, int64_t(1) << 30);
+    TRY(dalloc(h, &g.cnt, nb));
+    TRY(dalloc(h, &g.start, nb + 1));
+    TRY(dalloc(h, &g.ent_lo, g.cap));
+    TRY(dalloc(h, &g.ent_up, g.cap));
+    TRY(dalloc(h, &g.ctr, 4));
+    TRY(dalloc(h, &g.big_tri, std::max(s.nst, 1)));
+    TRY(dalloc(h, &g.big_edge, std::max(s.nse, 1)));
+    TRY(dalloc(h, &g.mode, std::max(ne, 1)));
+    TRY(dalloc(h, &g.qkey, std::max(s.cap, 1)));
     return ADMM_OK;
 }
 
@@ -806,7 +1073,11 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     h->sort_max = std::max(s.nst, s.nse);
     const int hist_n = 256 * sort_tiles(std::max(h->sort_max, 1));
     TRY(dalloc(h, &h->hist, hist_n));
-    const int scan_n = std::max(std::max(scan_tiles(hist_n), scan_tiles(n + 1)), scan_tiles(s.nsv + s.nse + 1)) + 4;
+    if (d->broad_phase < 0 || d->broad_phase > 2) return fail(h, ADMM_ERR_INVALID, "broad_phase must be 0, 1 or 2");
+    h->use_grid = d->broad_phase != 1;
+    TRY(setup_grid(h, d));
+    const int scan_n = std::max(std::max(std::max(scan_tiles(hist_n), scan_tiles(n + 1)), scan_tiles(s.nsv + s.nse + 1)),
+                                scan_tiles(h->grid_buckets)) + 4;
     TRY(dalloc(h, &s.scan_tmp, scan_n));
     TRY(dalloc(h, &s.res, 4));
     TRY(dalloc(h, &s.done, 4));
@@ -833,6 +1104,18 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     if (d->ell_lanes != 0 && d->ell_lanes != 1 && d->ell_lanes != 2 && d->ell_lanes != 4 && d->ell_lanes != 8)
         return fail(h, ADMM_ERR_INVALID, "ell_lanes must be 0, 1, 2, 4 or 8");
     TRY(autotune_ell(h, as, d->ell_lanes, &h->tune_lanes_a, &h->tune_lanes_r, &h->tune_ms_a, &h->tune_ms_r));
+    if (d->jacobi_mode < 0 || d->jacobi_mode > 2) return fail(h, ADMM_ERR_INVALID, "jacobi_mode must be 0, 1 or 2");
+    TRY(build_persist_plan(h, as.A));
+    h->persist = false;
+    if (h->persist_ok && h->jac_iter >= 2 && d->jacobi_mode != 1) {
+        if (d->jacobi_mode == 2) {
+            h->persist = true;
+        } else {
+            TRY(time_global(h, false, &h->tune_ms_sweeps));
+            TRY(time_global(h, true, &h->tune_ms_persist));
+            h->persist = h->tune_ms_persist < h->tune_ms_sweeps;
+        }
+    }
     TRY(upload_state(h, h->x_init, h->v_init));
     return ADMM_OK;
 }
@@ -860,10 +1143,20 @@ int accumulate_timers(AdmmB200* h) {
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, h->prof_ev[k], h->prof_ev[k + 1]));
             const int ph = h->prof_phase[k / 2];
+            if (ph < 0 || ph >= ADMM_NUM_PHASES) continue;
             h->phase_ms[ph] += ms;
             h->phase_launches[ph] += 1;
         }
         h->prof_used = 0;
+    } else if (h->probe_kernel == ADMM_PROBE_PHASES) {
+        for (int k = 0; k + 1 < h->pev_used; k++) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, h->pev[k], h->pev[k + 1]));
+            const int ph = h->pev_phase[k];
+            if (ph < 0 || ph >= ADMM_NUM_PHASES) continue;
+            h->phase_ms[ph] += ms;
+            h->phase_launches[ph] += h->pev_launch[k + 1] - h->pev_launch[k];
+        }
     } else if (h->probe_kernel != 0) {
         for (int k = 0; k + 1 < h->probe_used; k += 2) {
             float ms = 0.f;
@@ -878,8 +1171,11 @@ int accumulate_timers(AdmmB200* h) {
 int read_err_flags(AdmmB200* h, int* status) {
     int e[4] = {0, 0, 0, 0};
     CK(cudaMemcpy(e, h->s.err, sizeof(e), cudaMemcpyDeviceToHost));
-    if (e[0] || e[1] || e[2]) CK(cudaMemset(h->s.err, 0, sizeof(int) * 4));
-    *status = e[0] ? ADMM_ERR_CONTACT_OVERFLOW : e[1] ? ADMM_ERR_STACK_OVERFLOW : e[2] ? ADMM_ERR_NAN : ADMM_OK;
+    if (e[0] || e[1] || e[2] || e[3]) CK(cudaMemset(h->s.err, 0, sizeof(int) * 4));
+    // after a timed-out wait the blocks' sweep counters disagree: start them again from 0
+    if (e[3] && h->pp.epoch) CK(cudaMemset(h->pp.epoch, 0, sizeof(unsigned) * h->pp.blocks));
+    *status = e[3] ? ADMM_ERR_TIMEOUT : e[0] ? ADMM_ERR_CONTACT_OVERFLOW : e[1] ? ADMM_ERR_STACK_OVERFLOW
+            : e[2] ? ADMM_ERR_NAN : ADMM_OK;
     return ADMM_OK;
 }
 
@@ -922,6 +1218,7 @@ void admm_b200_destroy(AdmmB200* h) {
         if (p) cudaFree(p);
     for (auto e : h->prof_ev) cudaEventDestroy(e);
     for (auto e : h->probe_ev) cudaEventDestroy(e);
+    for (auto e : h->pev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1278,7 +1575,8 @@ int admm_b200_phase_times(AdmmB200* h, double* ms, int64_t* launches, int n_phas
 }
 
 int admm_b200_set_probe(AdmmB200* h, int kernel_class) {
-    if (!h || kernel_class < 0 || kernel_class > ADMM_KERNEL_DCD_EE) return ADMM_ERR_INVALID;
+    if (!h || kernel_class < 0 || (kernel_class > ADMM_KERNEL_DCD_EE && kernel_class != ADMM_PROBE_PHASES))
+        return ADMM_ERR_INVALID;
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     if (h->step_exec) {
@@ -1306,6 +1604,15 @@ int admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float
     if (lanes_r) *lanes_r = h->tune_lanes_r;
     if (ms_a) *ms_a = h->tune_ms_a;
     if (ms_r) *ms_r = h->tune_ms_r;
+    return ADMM_OK;
+}
+
+int admm_b200_global_mode(AdmmB200* h, int* persistent, int* blocks, float* ms_sweeps, float* ms_persist) {
+    if (!h) return ADMM_ERR_INVALID;
+    if (persistent) *persistent = h->persist ? 1 : 0;
+    if (blocks) *blocks = h->persist ? h->pp.blocks : 0;
+    if (ms_sweeps) *ms_sweeps = h->tune_ms_sweeps;
+    if (ms_persist) *ms_persist = h->tune_ms_persist;
     return ADMM_OK;
 }
 

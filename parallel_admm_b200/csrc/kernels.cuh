@@ -220,7 +220,9 @@ __global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
 // Gather of one sliced-ELL row: the warp `w` (a slice) accumulates sum val * v[col]
 // for its 32/T rows; lanes of one row are reduced with shuffles.  Returns the
 // row's sum in every lane of the row; `row` receives the lane's row index.
-template <int T>
+// CG = true reads v through L2 only (ld.global.cg): v is written by other
+// blocks of a persistent kernel while this one runs.
+template <int T, bool CG = false>
 ADMM_DEV float4 ell_row_sum(const SlicedEll& M, const float4* __restrict__ v, int w, int lane, int& row) {
     constexpr int S = 32 / T;
     row = w * S + (lane % S);
@@ -230,7 +232,7 @@ ADMM_DEV float4 ell_row_sum(const SlicedEll& M, const float4* __restrict__ v, in
     for (int k = b + lane; k < e; k += 32) {
         const int c = __ldg(&M.col[k]);
         const float a = __ldg(&M.val[k]);
-        const float4 q = v[c];
+        const float4 q = CG ? __ldcg(&v[c]) : v[c];
         ax = fmaf(a, q.x, ax);
         ay = fmaf(a, q.y, ay);
         az = fmaf(a, q.z, az);
@@ -250,15 +252,9 @@ ADMM_DEV float4 ell_row_sum(const SlicedEll& M, const float4* __restrict__ v, in
 // as a gather over the sliced-ELL copy of h^2 D^T W^2 (one warp per slice).
 // SAVE_PREV also keeps x before the solve (for the dual residual).
 // ---------------------------------------------------------------------------
-template <int T, bool SAVE_PREV>
-__global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
-    ADMM_PDL_PROLOGUE();
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= s.R.nslices) return;
-    int i;
-    const float4 acc = ell_row_sum<T>(s.R, s.y, w, lane, i);
-    if (lane >= 32 / T || i >= s.nd) return;
+// b_i from the row sum acc = (h^2 D^T W^2 (z - Ue))_i.
+template <bool SAVE_PREV>
+ADMM_DEV void rhs_row(const DevScene& s, int i, float4 acc) {
     const float4 m = s.mxt[i];
     float4 bi = f4(m.x + acc.x, m.y + acc.y, m.z + acc.z);
     if (s.contact) {
@@ -270,6 +266,25 @@ __global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
     }
     s.b[i] = bi;
     if (SAVE_PREV) s.xprev[i] = s.x[i];
+}
+
+template <int T, bool SAVE_PREV>
+__global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
+    ADMM_PDL_PROLOGUE();
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= s.R.nslices) return;
+    int i;
+    const float4 acc = ell_row_sum<T>(s.R, s.y, w, lane, i);
+    if (lane >= 32 / T || i >= s.nd) return;
+    rhs_row<SAVE_PREV>(s, i, acc);
+}
+
+// dst_i = (b_i - acc) / a_ii
+ADMM_DEV void jacobi_row(const DevScene& s, int i, float4 acc, float4* __restrict__ dst) {
+    const float4 bi = s.b[i];
+    const float d = s.a_diag[i];
+    dst[i] = f4((bi.x - acc.x) / d, (bi.y - acc.y) / d, (bi.z - acc.z) / d);
 }
 
 // ---------------------------------------------------------------------------
@@ -287,9 +302,98 @@ __global__ void __launch_bounds__(kVertThreads) k_jacobi(DevScene s, const float
     int i;
     const float4 acc = ell_row_sum<T>(s.A, src, w, lane, i);
     if (lane >= 32 / T || i >= s.nd) return;
-    const float4 bi = s.b[i];
-    const float d = s.a_diag[i];
-    dst[i] = f4((bi.x - acc.x) / d, (bi.y - acc.y) / d, (bi.z - acc.z) / d);
+    jacobi_row(s, i, acc, dst);
+}
+
+// ---------------------------------------------------------------------------
+// The whole global step in one persistent kernel: the right-hand side (RHS)
+// and `sweeps` Jacobi sweeps, bit-identical to k_rhs + k_jacobi launches.
+//
+// Block g owns rows [g*RB, (g+1)*RB) (RB a multiple of 32, so that the slices
+// of both sliced-ELL matrices align with the blocks).  After every sweep a
+// block publishes the number of sweeps it has completed in epoch[g]
+// (st.release.gpu after a block barrier); before sweep k it waits until every
+// block in its dependency list -- the owners of the columns of its rows,
+// symmetrised -- has completed sweep k-1 (ld.acquire.gpu).  That one wait
+// covers both hazards of the ping-pong buffers: the values it reads are
+// complete, and no neighbour still reads the buffer it is about to overwrite.
+// Epoch counters only grow (wrap-safe comparisons); all blocks hold the same
+// count between launches, so each launch takes its own block's count as base.
+// Every wait is bounded by spin_limit polls; on expiry the block sets err[3]
+// and returns, and the blocks waiting on it expire in turn.  All blocks must
+// be co-resident: the launch is cooperative.
+// ---------------------------------------------------------------------------
+constexpr int kPersistThreads = 512;
+
+ADMM_DEV unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+ADMM_DEV void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <int T, int TR, bool RHS, bool SAVE_PREV>
+__global__ void __launch_bounds__(kPersistThreads, 1) k_global_persist(DevScene s, PersistPlan pp, int sweeps) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    __shared__ unsigned sh_base;
+    __shared__ int sh_abort;
+    const int g = blockIdx.x;
+    const int r0 = g * pp.rows_per_block, r1 = min(s.nd, r0 + pp.rows_per_block);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) {
+        sh_base = ld_acquire_u32(pp.epoch + g);
+        sh_abort = 0;
+    }
+    if (RHS) {
+        constexpr int SR = 32 / TR;
+        const int w1 = (r1 + SR - 1) / SR;
+        for (int w = r0 / SR + warp; w < w1; w += nw) {
+            int i;
+            const float4 acc = ell_row_sum<TR>(s.R, s.y, w, lane, i);
+            if (lane < SR && i < r1) rhs_row<SAVE_PREV>(s, i, acc);
+        }
+    }
+    __syncthreads();
+    const unsigned base = sh_base;
+    constexpr int S = 32 / T;
+    const int w1 = (r1 + S - 1) / S;
+    const int d0 = pp.dep_ptr[g], d1 = pp.dep_ptr[g + 1];
+    for (int k = 0; k < sweeps; k++) {
+        if (k > 0) {
+            if (warp == 0) {
+                const unsigned target = base + (unsigned)k;
+                bool ok = true;
+                for (int d = d0 + lane; d < d1 && ok; d += 32) {
+                    const unsigned* e = pp.epoch + pp.dep_idx[d];
+                    int spins = 0;
+                    while ((int)(ld_acquire_u32(e) - target) < 0) {
+                        if (++spins > pp.spin_limit) {
+                            ok = false;
+                            break;
+                        }
+                        if (spins > 32) __nanosleep(64);
+                    }
+                }
+                if (__any_sync(0xffffffffu, !ok) && lane == 0) {
+                    sh_abort = 1;
+                    s.err[3] = 1;
+                }
+            }
+            __syncthreads();
+            if (sh_abort) return;
+        }
+        const float4* src = k == 0 ? s.x : s.jac[(k - 1) & 1];
+        float4* dst = k == sweeps - 1 ? s.x : s.jac[k & 1];
+        for (int w = r0 / S + warp; w < w1; w += nw) {
+            int i;
+            const float4 acc = ell_row_sum<T, true>(s.A, src, w, lane, i);
+            if (lane < S && i < r1) jacobi_row(s, i, acc, dst);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) st_release_u32(pp.epoch + g, base + (unsigned)k + 1u);
+    }
 }
 
 __global__ void k_copy_dyn(DevScene s, const float4* __restrict__ src, float4* __restrict__ dst) {

@@ -39,6 +39,32 @@ struct BvhDev {
     float4* node4 = nullptr;     // [4(n-1)]
 };
 
+// Work split and dependency lists of the persistent global-step kernel.
+struct PersistPlan {
+    int blocks = 0;                // one per SM at most (cooperative launch)
+    int rows_per_block = 0;        // multiple of 32
+    const int* dep_ptr = nullptr;  // [blocks + 1]
+    const int* dep_idx = nullptr;  // blocks whose rows share a matrix entry with this block's rows
+    unsigned* epoch = nullptr;     // [blocks] sweeps completed (monotone, wraps)
+    int spin_limit = 0;            // polls before a wait gives up
+};
+
+// Uniform-grid broad phase: hash table of (cell, element type) buckets.
+struct GridDev {
+    float inv_c = 0.f;             // 1 / cell edge
+    int hmask = 0;                 // buckets - 1 (power of two)
+    int cap = 0;                   // entry capacity
+    int* cnt = nullptr;            // [buckets] entries per bucket (zero between DCDs)
+    int* start = nullptr;          // [buckets + 1] bucket offsets
+    float4* ent_lo = nullptr;      // [cap] element box lo, w = element index (int bits)
+    float4* ent_up = nullptr;      // [cap] element box up, w = type (0 triangle, 1 edge)
+    int* ctr = nullptr;            // [4] entries reserved, big triangles, big edges
+    int* big_tri = nullptr;        // [n surface triangles]
+    int* big_edge = nullptr;       // [n surface edges]
+    int* mode = nullptr;           // [triangles + edges] 1 = in the grid, 0 = big list
+    int* qkey = nullptr;           // [contact capacity] partner index per contact slot
+};
+
 struct DevScene {
     int n = 0, nd = 0, m = 0;
     int ntri = 0, ntet = 0, nbend = 0, npin = 0;
@@ -76,7 +102,7 @@ struct DevScene {
     int cap = 0;
     int* nc = nullptr;                    // [1] device contact count (clamped to cap)
     int* nc_raw = nullptr;                // [1] unclamped count
-    int* err = nullptr;                   // [4] error flags: overflow, stack, nan
+    int* err = nullptr;                   // [4] error flags: overflow, stack, nan, wait timeout
     int4* pairs = nullptr;
     float4* bary = nullptr;
     float4* nrm = nullptr;                // normal xyz, w = h_cN - thickness
@@ -95,6 +121,7 @@ struct DevScene {
     const int2* se = nullptr;             // surface edges
     const int* sv = nullptr;              // surface vertices
     BvhDev bf, be;                        // face tree, edge tree
+    GridDev grid;                         // uniform-grid broad phase
     int* qcount = nullptr;                // [nsv + nse] per-query pair counts
     int* qoff = nullptr;                  // [nsv + nse + 1] exclusive offsets
     int* scan_tmp = nullptr;              // block sums for scans

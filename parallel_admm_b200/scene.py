@@ -59,6 +59,8 @@ class SolverParams:
     w_scale: float = 200.0
     bvh_refit: bool = True
     ell_lanes: int = 0
+    jacobi_mode: int = 0  # 0 autotuned, 1 one kernel per sweep, 2 persistent global step
+    broad_phase: int = 0  # 0 default (grid), 1 LBVH, 2 uniform grid
 
 
 @dataclasses.dataclass

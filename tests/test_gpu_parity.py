@@ -99,8 +99,9 @@ def _pairset(pairs, canon=True):
     return out
 
 
+@pytest.mark.parametrize("broad", [1, 2], ids=["lbvh", "grid"])
 @pytest.mark.parametrize("case", ["cloth_fold", "cube_squeezed", "cloth_flat_on_box"])
-def test_dcd_pairs_bitexact(case):
+def test_dcd_pairs_bitexact(case, broad):
     from oracle import oracle as O
     if case == "cloth_fold":
         sc, x = _crumpled_cloth()
@@ -116,6 +117,7 @@ def test_dcd_pairs_bitexact(case):
         x = sc.verts.copy()
         x[:sc.n_dyn, 1] = 0.5 + 0.5 * sc.params.thickness  # lying on the box top
     x = np.ascontiguousarray(x, np.float32)
+    sc.params.broad_phase = broad
     h = B.Handle(sc)
     n = h.detect(x)
     ref_pairs, _ = O.dcd(x, sc.surf_verts, sc.surf_tris, sc.surf_edges, sc.params.thickness)
@@ -164,28 +166,46 @@ def test_full_step_cloth_parity():
 
 
 def test_full_step_cube_contact_parity():
-    """The cube right at impact (1 m drop speed), FP32 GPU vs FP64 oracle."""
+    """The cube right at impact (1 m drop speed).
+
+    Frames 0-2 run free against the FP64 oracle (1e-5 per step).  From frame 3 on, contacts
+    at the edge of the thickness band decide differently in FP64 and FP32 (the narrow phase
+    is FP32 on both sides of the reference), so frames 3-9 are compared one substep at a time,
+    from the oracle's state (positions, velocities, both duals), against the FP32 oracle:
+    identical contact counts and positions within 1e-4 relative."""
+    from oracle import oracle as O
     sc = scene.cube_on_ground(10, drop=0.0)
     v0 = np.zeros_like(sc.verts)
     v0[:sc.n_dyn, 1] = -np.sqrt(2 * 9.8 * 1.0)
     x0 = sc.verts.copy()
     x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.03
     h, o = _setup(sc)
+    o32 = O.Oracle(h.holder, double=False)
     h.set_state(x0, v0)
-    o.write(B.BUF_X0, x0)
-    o.write(B.BUF_V, v0)
-    o.write(B.BUF_X, x0)
+    for orc in (o, o32):
+        orc.write(B.BUF_X0, x0)
+        orc.write(B.BUF_V, v0)
+        orc.write(B.BUF_X, x0)
     ext = np.ptp(x0[:sc.n_dyn], axis=0).max()
     ncs = []
-    for k in range(4):
+    for k in range(3):
         sg = h.step(1)
         so = o.step(1)
+        o32.step(1)
         ncs.append((sg["n_contacts"], so["n_contacts"]))
-        xg, vg = h.get_state()
-        xo = o.read(B.BUF_X0)
-        err = np.abs(xg - xo).max() / ext
-        assert err <= TOL_LONG, (k, err, ncs)
-    assert max(c[0] for c in ncs) > 0
+        err = np.abs(h.get_state()[0] - o.read(B.BUF_X0)).max() / ext
+        assert err <= TOL_STEP * (k + 1), (k, err, ncs)
+    for k in range(3, 10):
+        h.set_state(o32.read(B.BUF_X0), o32.read(B.BUF_V))
+        h.write(B.BUF_UE, o32.read(B.BUF_UE))
+        h.write(B.BUF_UC, o32.read(B.BUF_UC))
+        sg = h.step(1)
+        so = o32.step(1)
+        ncs.append((sg["n_contacts"], so["n_contacts"]))
+        assert sg["n_contacts"] == so["n_contacts"], (k, ncs)
+        err = np.abs(h.get_state()[0] - o32.read(B.BUF_X0)).max() / ext
+        assert err <= 1e-4, (k, err, ncs)
+    assert min(c[0] for c in ncs) > 0
 
 
 def test_long_run_cloth_1e3():
@@ -288,7 +308,7 @@ def test_backend_contract_call_order():
     assert np.allclose(be.getVertices(), sc.verts)
 
 
-def test_refit_and_rebuild_give_the_same_motion():
+def test_refit_rebuild_and_grid_give_the_same_motion():
     """Refitting the BVH between DCDs of a substep changes only traversal cost and the
     order of contacts within a query (so the summation order): one impact substep agrees
     to 1e-5 with the same contact count; three substeps at impact (where rounding can flip
@@ -301,16 +321,18 @@ def test_refit_and_rebuild_give_the_same_motion():
     ext = np.ptp(x0[:sc.n_dyn], axis=0).max()
     for nsteps, tol in ((1, TOL_STEP), (3, TOL_LONG)):
         out = []
-        for refit in (0, 1):
+        for broad, refit in ((1, 0), (1, 1), (2, 0)):
             sc.params.bvh_refit = bool(refit)
+            sc.params.broad_phase = broad
             h = B.Handle(sc)
             h.set_state(x0, v0)
             st = h.step(nsteps)
             out.append((h.get_state()[0], st["n_contacts"]))
         assert out[0][1] > 0
-        if nsteps == 1:
-            assert out[0][1] == out[1][1]
-        assert np.abs(out[0][0] - out[1][0]).max() / ext <= tol
+        for k in (1, 2):
+            if nsteps == 1:
+                assert out[0][1] == out[k][1]
+            assert np.abs(out[0][0] - out[k][0]).max() / ext <= tol
 
 
 def test_autotuner_choice_is_valid():
@@ -372,3 +394,67 @@ def test_tolerance_mode_eager_matches_graph():
         assert (k > k_min) == (chunks > 1)
     hg.close()
     he.close()
+
+
+def _cube_at_impact(n=8):
+    sc = scene.cube_on_ground(n, drop=0.0)
+    v0 = np.zeros_like(sc.verts)
+    v0[:sc.n_dyn, 1] = -np.sqrt(2 * 9.8)
+    x0 = sc.verts.copy()
+    x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.02
+    return sc, x0, v0
+
+
+@pytest.mark.parametrize("case", ["cloth", "cube_impact", "cube_impact_tol"])
+def test_persistent_global_step_bitwise(case):
+    """jacobi_mode 2 (RHS and all sweeps in one cooperative kernel, blocks synchronised by
+    sweep counters) reproduces jacobi_mode 1 (one kernel per sweep) bit for bit."""
+    if case == "cloth":
+        sc, x0, v0 = scene.cloth_on_box(24), None, None
+    else:
+        sc, x0, v0 = _cube_at_impact(10)
+    over = {"residual_tol": 1e-4} if case.endswith("_tol") else {}
+    sc.params.ell_lanes = 4
+    hs = []
+    for mode in (1, 2):
+        sc.params.jacobi_mode = mode
+        h = B.Handle(sc, **over)
+        if x0 is not None:
+            h.set_state(x0, v0)
+        hs.append(h)
+    gm = hs[1].global_mode()
+    assert gm["persistent"] and gm["blocks"] >= 1
+    assert not hs[0].global_mode()["persistent"]
+    for k in range(4):
+        st = [h.step(1) for h in hs]
+        assert st[0]["iters"] == st[1]["iters"] and st[0]["n_contacts"] == st[1]["n_contacts"]
+        assert st[1]["status"] == B.OK
+        xa, va = hs[0].get_state()
+        xb, vb = hs[1].get_state()
+        np.testing.assert_array_equal(xa, xb)
+        np.testing.assert_array_equal(va, vb)
+    for h in hs:
+        h.close()
+
+
+def test_persistent_jacobi_entry_bitwise():
+    """admm_b200_jacobi (standalone sweeps) in both modes, odd and even sweep counts."""
+    sc = scene.cube_on_ground(12)
+    sc.params.ell_lanes = 2
+    rng = np.random.default_rng(21)
+    x = _perturbed(sc, 1e-3, seed=22)
+    b = rng.normal(size=(sc.n_dyn, 3))
+    out = []
+    for mode in (1, 2):
+        sc.params.jacobi_mode = mode
+        h = B.Handle(sc)
+        res = []
+        for sweeps in (2, 3, 7):
+            h.write(B.BUF_X, x)
+            h.write(B.BUF_B, b)
+            h.jacobi(sweeps)
+            res.append(h.read(B.BUF_X))
+        out.append(res)
+        h.close()
+    for a, c in zip(*out):
+        np.testing.assert_array_equal(a, c)
