@@ -241,6 +241,9 @@ def main():
                     help="global step: 0 autotuned, 1 one kernel per sweep, 2 persistent kernel")
     ap.add_argument("--ref-steps", type=int, default=200, help="cap on steps timed by --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="open a CUDA profiler range (cudaProfilerStart/Stop) around the first N timed steps, "
+                         "for ncu --profile-from-start off")
     ap.add_argument("--profile", action="store_true", help="also print a per-phase kernel-time breakdown")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -285,10 +288,14 @@ def main():
 
     with ClockSampler(local) as clk:
         barrier()
-        for _ in range(args.steps):
+        for k in range(args.steps):
             flush.fill_(1.0)
             torch.cuda.synchronize()
+            if args.profile_steps and k == 0:
+                torch.cuda.cudart().cudaProfilerStart()
             st = h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+            if args.profile_steps and k + 1 == args.profile_steps:
+                torch.cuda.cudart().cudaProfilerStop()
             dev_ms.append(h.last_step_device_ms())
             contacts.append(st["n_contacts"])
             iters.append(st["iters"])

@@ -281,7 +281,7 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
             }
             LAUNCH(k_grid_scatter, blocks(ne, 256), 256, s);
         }
-        if (nq > 0) LAUNCH(k_grid_query<false>, blocks(nq, 128), 128, s);
+        if (nq > 0) LAUNCH(k_grid_query<false>, blocks(nq * kQueryLanes, 128), 128, s);
     } else {
         if (rebuild) {
             LAUNCH(k_scene_init, 1, 32, s.bf, s.be);
@@ -303,7 +303,7 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
     }
     LAUNCH(k_set_count, 1, 1, s);
     if (h->use_grid) {
-        if (nq > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_grid_query<true>, blocks(nq, 128), 128, s);
+        if (nq > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_grid_query<true>, blocks(nq * kQueryLanes, 128), 128, s);
     } else {
         if (s.nsv > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_dcd_vf<true>, blocks(s.nsv, 128), 128, s);
         if (s.nse > 0) LAUNCH_P(ADMM_KERNEL_DCD_EE, k_dcd_ee<true>, blocks(s.nse, 128), 128, s);

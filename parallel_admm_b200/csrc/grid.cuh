@@ -160,20 +160,7 @@ __global__ void __launch_bounds__(256) k_grid_scatter(DevScene s) {
     });
 }
 
-// One accepted pair: count it, or (WRITE) store it at slot base + count.
-template <bool WRITE>
-ADMM_DEV void grid_emit(const DevScene& s, int base, int& count, int partner, int4 ids, const NpResult& r, bool ee) {
-    if (WRITE) {
-        const int slot = base + count;
-        if (slot < s.cap) {
-            write_contact(s, slot, ids, r, ee);
-            s.grid.qkey[slot] = partner;
-        }
-    }
-    count++;
-}
-
-// Insertion sort of the slots [b, e) by partner index (all contact arrays).
+// Insertion sort of the contact slots [b, e) by partner index.
 ADMM_DEV void grid_sort_segment(const DevScene& s, int b, int e) {
     int* key = s.grid.qkey;
     for (int k = b + 1; k < e; k++) {
@@ -197,143 +184,212 @@ ADMM_DEV void grid_sort_segment(const DevScene& s, int b, int e) {
     }
 }
 
-// Vertex-face query of surface vertex q (lbvh.cu:1693-1748 semantics).
-template <bool WRITE>
-ADMM_DEV int grid_query_vf(const DevScene& s, int q, int base) {
+// ---------------------------------------------------------------------------
+// Queries.  kQueryLanes consecutive threads serve one query: they split its
+// cells (and the big lists) between them, so that the loads of different
+// cells are in flight at the same time.  Each walk calls f(partner) for every
+// element that passes the box test and the once-per-pair cell rule; f applies
+// the index rules and the narrow phase.
+// ---------------------------------------------------------------------------
+constexpr int kQueryLanes = 8;
+constexpr int kQueryHits = 8;  // hits a lane keeps in registers between counting and writing
+
+ADMM_DEV int3 grid_cell_at(int3 a, int3 b, int ci) {
+    const int dx = b.x - a.x + 1, dy = b.y - a.y + 1;
+    return make_int3(a.x + ci % dx, a.y + (ci / dx) % dy, a.z + ci / (dx * dy));
+}
+
+ADMM_DEV int grid_cells(int3 a, int3 b) { return (b.x - a.x + 1) * (b.y - a.y + 1) * (b.z - a.z + 1); }
+
+ADMM_DEV float4 tri_box_lo(const DevScene& s, int f, float4& up) {
+    const int4 t = s.st[f];
+    float4 lo = f4(1e32f, 1e32f, 1e32f);
+    up = f4(-1e32f, -1e32f, -1e32f);
+    box_add(lo, up, s.x[t.x]);
+    box_add(lo, up, s.x[t.y]);
+    box_add(lo, up, s.x[t.z]);
+    return lo;
+}
+
+ADMM_DEV float4 edge_box_lo(const DevScene& s, int o, float4& up) {
+    const int2 e = s.se[o];
+    float4 lo = f4(1e32f, 1e32f, 1e32f);
+    up = f4(-1e32f, -1e32f, -1e32f);
+    box_add(lo, up, s.x[e.x]);
+    box_add(lo, up, s.x[e.y]);
+    return lo;
+}
+
+// Candidate triangles of surface vertex position P (lane `sub` of the group).
+template <class F>
+ADMM_DEV void grid_walk_vf(const DevScene& s, float4 P, int sub, F f) {
     const GridDev& g = s.grid;
-    const int v = s.sv[q];
-    const float4 P = s.x[v];
     const float gap = s.thickness;
-    int count = 0;
-    auto test = [&](int f) {
-        const int4 tri = s.st[f];
-        if (v == tri.x || v == tri.y || v == tri.z) return;
-        NpResult r;
-        if (narrow_pt(P, s.x[tri.x], s.x[tri.y], s.x[tri.z], r) && r.dist < gap && r.dist >= 0.f)
-            grid_emit<WRITE>(s, base, count, f, make_int4(v, tri.x, tri.y, tri.z), r, false);
-    };
     int3 a, b;
     grid_query_range(P, P, gap, g.inv_c, a, b);
     if (grid_range_small(a, b)) {
-        for (int iz = a.z; iz <= b.z; iz++)
-            for (int iy = a.y; iy <= b.y; iy++)
-                for (int ix = a.x; ix <= b.x; ix++) {
-                    const int bk = grid_bucket(ix, iy, iz, 0, g.hmask);
-                    const int k1 = g.start[bk + 1];
-                    for (int k = g.start[bk]; k < k1; k++) {
-                        const float4 lo = g.ent_lo[k], up = g.ent_up[k];
-                        if (__float_as_int(up.w) != 0 || !box_overlap(P, P, lo, up, gap)) continue;
-                        int3 ea, eb;
-                        grid_range(lo, up, g.inv_c, ea, eb);
-                        if (max(a.x, ea.x) != ix || max(a.y, ea.y) != iy || max(a.z, ea.z) != iz) continue;
-                        test(__float_as_int(lo.w));
-                    }
-                }
+        const int nc = grid_cells(a, b);
+        for (int ci = sub; ci < nc; ci += kQueryLanes) {
+            const int3 c = grid_cell_at(a, b, ci);
+            const int bk = grid_bucket(c.x, c.y, c.z, 0, g.hmask);
+            const int k1 = g.start[bk + 1];
+            for (int k = g.start[bk]; k < k1; k++) {
+                const float4 lo = g.ent_lo[k], up = g.ent_up[k];
+                if (__float_as_int(up.w) != 0 || !box_overlap(P, P, lo, up, gap)) continue;
+                int3 ea, eb;
+                grid_range(lo, up, g.inv_c, ea, eb);
+                if (max(a.x, ea.x) != c.x || max(a.y, ea.y) != c.y || max(a.z, ea.z) != c.z) continue;
+                f(__float_as_int(lo.w));
+            }
+        }
     } else {
-        for (int f = 0; f < s.nst; f++) {
-            if (!g.mode[f]) continue;
-            const int4 tri = s.st[f];
-            float4 lo = f4(1e32f, 1e32f, 1e32f), up = f4(-1e32f, -1e32f, -1e32f);
-            box_add(lo, up, s.x[tri.x]);
-            box_add(lo, up, s.x[tri.y]);
-            box_add(lo, up, s.x[tri.z]);
-            if (box_overlap(P, P, lo, up, gap)) test(f);
+        for (int t = sub; t < s.nst; t += kQueryLanes) {
+            if (!g.mode[t]) continue;
+            float4 up;
+            const float4 lo = tri_box_lo(s, t, up);
+            if (box_overlap(P, P, lo, up, gap)) f(t);
         }
     }
     const int nb = g.ctr[1];
-    for (int j = 0; j < nb; j++) {
-        const int f = g.big_tri[j];
-        const int4 tri = s.st[f];
-        float4 lo = f4(1e32f, 1e32f, 1e32f), up = f4(-1e32f, -1e32f, -1e32f);
-        box_add(lo, up, s.x[tri.x]);
-        box_add(lo, up, s.x[tri.y]);
-        box_add(lo, up, s.x[tri.z]);
-        if (box_overlap(P, P, lo, up, gap)) test(f);
+    for (int j = sub; j < nb; j += kQueryLanes) {
+        const int t = g.big_tri[j];
+        float4 up;
+        const float4 lo = tri_box_lo(s, t, up);
+        if (box_overlap(P, P, lo, up, gap)) f(t);
     }
-    return count;
 }
 
-// Edge-edge query of surface edge e (lbvh.cu:1750-1813 semantics: pairs of
-// edges that share no vertex, lower index first).
-template <bool WRITE>
-ADMM_DEV int grid_query_ee(const DevScene& s, int e, int base) {
+// Candidate partner edges of surface edge e with box [lo, up]: grid edges with a
+// larger index (grid edge e), every big edge (grid edge e) or big edges with a
+// larger index (big edge e).
+template <class F>
+ADMM_DEV void grid_walk_ee(const DevScene& s, int e, float4 lo, float4 up, int sub, F f) {
     const GridDev& g = s.grid;
-    const int2 ed = s.se[e];
-    const float4 A0 = s.x[ed.x], A1 = s.x[ed.y];
-    float4 lo = f4(1e32f, 1e32f, 1e32f), up = f4(-1e32f, -1e32f, -1e32f);
-    box_add(lo, up, A0);
-    box_add(lo, up, A1);
     const float gap = s.thickness;
     const bool small = g.mode[s.nst + e] != 0;
-    int count = 0;
-    auto test = [&](int o) {
-        const int2 od = s.se[o];
-        if (ed.x == od.x || ed.x == od.y || ed.y == od.x || ed.y == od.y) return;
-        NpResult r;
-        if (o > e) {
-            if (narrow_ee(A0, A1, s.x[od.x], s.x[od.y], r) && r.dist < gap && r.dist >= 0.f)
-                grid_emit<WRITE>(s, base, count, o, make_int4(ed.x, ed.y, od.x, od.y), r, true);
-        } else {
-            if (narrow_ee(s.x[od.x], s.x[od.y], A0, A1, r) && r.dist < gap && r.dist >= 0.f)
-                grid_emit<WRITE>(s, base, count, o, make_int4(od.x, od.y, ed.x, ed.y), r, true);
-        }
-    };
-    int3 a, b;
-    grid_query_range(lo, up, gap, g.inv_c, a, b);
-    if (small && !grid_range_small(a, b)) {
-        for (int o = e + 1; o < s.nse; o++) {
-            if (!g.mode[s.nst + o]) continue;
-            const int2 od = s.se[o];
-            float4 olo = f4(1e32f, 1e32f, 1e32f), oup = f4(-1e32f, -1e32f, -1e32f);
-            box_add(olo, oup, s.x[od.x]);
-            box_add(olo, oup, s.x[od.y]);
-            if (box_overlap(lo, up, olo, oup, gap)) test(o);
-        }
-    } else if (small) {
-        for (int iz = a.z; iz <= b.z; iz++)
-            for (int iy = a.y; iy <= b.y; iy++)
-                for (int ix = a.x; ix <= b.x; ix++) {
-                    const int bk = grid_bucket(ix, iy, iz, 1, g.hmask);
-                    const int k1 = g.start[bk + 1];
-                    for (int k = g.start[bk]; k < k1; k++) {
-                        const float4 elo = g.ent_lo[k], eup = g.ent_up[k];
-                        const int o = __float_as_int(elo.w);
-                        if (__float_as_int(eup.w) != 1 || o <= e || !box_overlap(lo, up, elo, eup, gap)) continue;
-                        int3 ea, eb;
-                        grid_range(elo, eup, g.inv_c, ea, eb);
-                        if (max(a.x, ea.x) != ix || max(a.y, ea.y) != iy || max(a.z, ea.z) != iz) continue;
-                        test(o);
-                    }
+    if (small) {
+        int3 a, b;
+        grid_query_range(lo, up, gap, g.inv_c, a, b);
+        if (grid_range_small(a, b)) {
+            const int nc = grid_cells(a, b);
+            for (int ci = sub; ci < nc; ci += kQueryLanes) {
+                const int3 c = grid_cell_at(a, b, ci);
+                const int bk = grid_bucket(c.x, c.y, c.z, 1, g.hmask);
+                const int k1 = g.start[bk + 1];
+                for (int k = g.start[bk]; k < k1; k++) {
+                    const float4 elo = g.ent_lo[k], eup = g.ent_up[k];
+                    const int o = __float_as_int(elo.w);
+                    if (__float_as_int(eup.w) != 1 || o <= e || !box_overlap(lo, up, elo, eup, gap)) continue;
+                    int3 ea, eb;
+                    grid_range(elo, eup, g.inv_c, ea, eb);
+                    if (max(a.x, ea.x) != c.x || max(a.y, ea.y) != c.y || max(a.z, ea.z) != c.z) continue;
+                    f(o);
                 }
+            }
+        } else {
+            for (int o = e + 1 + sub; o < s.nse; o += kQueryLanes) {
+                if (!g.mode[s.nst + o]) continue;
+                float4 oup;
+                const float4 olo = edge_box_lo(s, o, oup);
+                if (box_overlap(lo, up, olo, oup, gap)) f(o);
+            }
+        }
     }
     const int nb = g.ctr[2];
-    for (int j = 0; j < nb; j++) {
+    for (int j = sub; j < nb; j += kQueryLanes) {
         const int o = g.big_edge[j];
-        // a grid edge owns its pairs with every big edge; two big edges: the lower index
         if (o == e || (!small && o < e)) continue;
-        const int2 od = s.se[o];
-        float4 olo = f4(1e32f, 1e32f, 1e32f), oup = f4(-1e32f, -1e32f, -1e32f);
-        box_add(olo, oup, s.x[od.x]);
-        box_add(olo, oup, s.x[od.y]);
-        if (box_overlap(lo, up, olo, oup, gap)) test(o);  // the overlap rule is symmetric
+        float4 oup;
+        const float4 olo = edge_box_lo(s, o, oup);
+        if (box_overlap(lo, up, olo, oup, gap)) f(o);  // the overlap rule is symmetric
     }
-    return count;
 }
 
-// Count (WRITE = false: qcount) or write (WRITE = true, at qoff) the pairs of
-// every query: surface vertices first, then surface edges.
+// Narrow phase of vertex v against triangle f (region 0, 0 <= d < thickness).
+ADMM_DEV bool grid_hit_vf(const DevScene& s, int v, float4 P, int f, int4& ids, NpResult& r) {
+    const int4 tri = s.st[f];
+    if (v == tri.x || v == tri.y || v == tri.z) return false;
+    ids = make_int4(v, tri.x, tri.y, tri.z);
+    return narrow_pt(P, s.x[tri.x], s.x[tri.y], s.x[tri.z], r) && r.dist < s.thickness && r.dist >= 0.f;
+}
+
+// Narrow phase of edges e and o (no shared vertex), lower index first.
+ADMM_DEV bool grid_hit_ee(const DevScene& s, int e, int o, int4& ids, NpResult& r) {
+    const int2 ed = s.se[e], od = s.se[o];
+    if (ed.x == od.x || ed.x == od.y || ed.y == od.x || ed.y == od.y) return false;
+    const int2 lo = o > e ? ed : od, hi = o > e ? od : ed;
+    ids = make_int4(lo.x, lo.y, hi.x, hi.y);
+    return narrow_ee(s.x[lo.x], s.x[lo.y], s.x[hi.x], s.x[hi.y], r) && r.dist < s.thickness && r.dist >= 0.f;
+}
+
+// Count (WRITE = false: qcount) or write (WRITE = true: at qoff, then sorted by
+// partner) the pairs of every query: surface vertices first, then edges.
 template <bool WRITE>
 __global__ void __launch_bounds__(128) k_grid_query(DevScene s) {
     ADMM_PDL_PROLOGUE();
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= s.nsv + s.nse) return;
-    const int base = WRITE ? s.qoff[q] : 0;
-    const int n = q < s.nsv ? grid_query_vf<WRITE>(s, q, base) : grid_query_ee<WRITE>(s, q - s.nsv, base);
-    if (!WRITE) {
-        s.qcount[q] = n;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = t / kQueryLanes, sub = t % kQueryLanes;
+    if (q >= s.nsv + s.nse) return;  // whole groups leave together
+    const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kQueryLanes - 1));
+    const bool vf = q < s.nsv;
+    const int e = q - s.nsv;
+    int v = 0;
+    float4 P = f4(0.f, 0.f, 0.f), lo = P, up = P;
+    if (vf) {
+        v = s.sv[q];
+        P = s.x[v];
     } else {
-        const int e = min(base + n, s.cap);
-        if (e - base > 1) grid_sort_segment(s, base, e);
+        lo = edge_box_lo(s, e, up);
+    }
+    int hits[kQueryHits];
+    int n = 0;
+    auto consider = [&](int partner) {
+        int4 ids;
+        NpResult r;
+        if (vf ? grid_hit_vf(s, v, P, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r)) {
+            if (n < kQueryHits) hits[n] = partner;
+            n++;
+        }
+    };
+    if (vf) grid_walk_vf(s, P, sub, consider);
+    else grid_walk_ee(s, e, lo, up, sub, consider);
+    // group sum / exclusive prefix of the lane counts
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < kQueryLanes; o <<= 1) {
+        const int y = __shfl_up_sync(gmask, incl, o, kQueryLanes);
+        if (sub >= o) incl += y;
+    }
+    const int total = __shfl_sync(gmask, incl, kQueryLanes - 1, kQueryLanes);
+    if (!WRITE) {
+        if (sub == 0) s.qcount[q] = total;
+        return;
+    }
+    const int base = s.qoff[q];
+    int slot = base + incl - n;
+    auto emit = [&](int partner) {
+        int4 ids;
+        NpResult r;
+        const bool hit = vf ? grid_hit_vf(s, v, P, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r);
+        if (hit) {
+            if (slot < s.cap) {
+                write_contact(s, slot, ids, r, !vf);
+                s.grid.qkey[slot] = partner;
+            }
+            slot++;
+        }
+    };
+    if (n <= kQueryHits) {
+        for (int k = 0; k < n; k++) emit(hits[k]);
+    } else if (vf) {
+        grid_walk_vf(s, P, sub, emit);
+    } else {
+        grid_walk_ee(s, e, lo, up, sub, emit);
+    }
+    __syncwarp(gmask);
+    if (sub == 0) {
+        const int end = min(base + total, s.cap);
+        if (end - base > 1) grid_sort_segment(s, base, end);
     }
 }
 
