@@ -55,6 +55,8 @@ struct AdmmB200 {
     bool warmstart_ue = true, warmstart_uc = true;
     bool bvh_refit = true;
     bool use_grid = true;           // broad phase: uniform grid (true) or LBVH
+    bool contact_fused = false;     // one kernel per contact pass (true) or the two of the reference
+    int enqueue_rc = ADMM_OK;       // first error while enqueueing or capturing a substep
     float grid_cell_size = 0.f;
     int grid_buckets = 0;
     bool pdl = true;                // programmatic dependent launch between the kernels of a substep
@@ -333,16 +335,30 @@ void enqueue_local(AdmmB200* h, int mode) {
         LAUNCH(k_local<LOCAL_DUAL>, g, kLocalThreads, h->s, h->tet_blocks, h->tri_blocks, h->bend_blocks);
 }
 
-void enqueue_contact(AdmmB200* h, bool dual) {
+// Contact step of one ADMM iteration: p for every dynamic vertex, then gs_iter
+// Jacobi passes of the friction-cone projection -- one fused kernel per pass
+// (ping-pong between p/p2 and r/r2), or the reference's two kernels per pass.
+int enqueue_contact(AdmmB200* h, bool dual) {
     DevScene& s = h->s;
     const int vb = blocks(s.nd, kVertThreads);
     set_phase(h, ADMM_PHASE_CONTACT);
     if (dual) LAUNCH((k_contact_p<true, true>), vb, kVertThreads, s);
     else LAUNCH((k_contact_p<false, true>), vb, kVertThreads, s);
-    for (int g = 0; g < h->gs_iter; g++) {
-        LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
-        LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, blocks(s.nd, kContactThreads), kContactThreads, s);
+    const int cb = blocks(s.nd, kContactThreads);
+    if (!h->contact_fused) {
+        for (int g = 0; g < h->gs_iter; g++) {
+            LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
+            LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, cb, kContactThreads, s);
+        }
+        return ADMM_OK;
     }
+    for (int g = 0; g < h->gs_iter; g++) {
+        const bool even = (g & 1) == 0;
+        LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_pass, cb, kContactThreads, s, even ? s.p : s.p2,
+                 even ? s.p2 : s.p, even ? s.rc : s.rc2, even ? s.rc2 : s.rc);
+    }
+    if (h->gs_iter & 1) LAUNCH(k_contact_pass_copy, cb, kContactThreads, s, s.p2, s.rc2);
+    return ADMM_OK;
 }
 
 // one Jacobi sweep with the tuned number of lanes per row
@@ -629,7 +645,10 @@ void enqueue_iteration(AdmmB200* h, int it, bool first, bool residual) {
     DevScene& s = h->s;
     if (s.contact && it % h->dcd_interval == 0) enqueue_dcd(h, !h->bvh_refit || first);
     enqueue_local(h, first ? LOCAL_PROX : (LOCAL_PROX | LOCAL_DUAL));
-    if (s.contact) enqueue_contact(h, !first);
+    if (s.contact) {
+        const int rc = enqueue_contact(h, !first);
+        if (rc != ADMM_OK && h->enqueue_rc == ADMM_OK) h->enqueue_rc = rc;
+    }
     enqueue_global(h, residual);
     if (residual) enqueue_residual(h);
 }
@@ -744,9 +763,11 @@ int build_step_graph_once(AdmmB200* h) {
     h->cstream = h->stream;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     h->launch_counter = 0;
+    h->enqueue_rc = ADMM_OK;
     int rc = ADMM_OK;
     if (h->residual_tol > 0.f) rc = enqueue_step_tol(h, h->residual_tol);
     else enqueue_step(h);
+    if (rc == ADMM_OK) rc = h->enqueue_rc;
     set_phase(h, ADMM_NUM_PHASES);  // closes the last phase
     h->kernels_per_step = h->launch_counter;
     cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
@@ -1061,6 +1082,8 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.gamma, s.cap));
     TRY(dalloc(h, &s.kc, s.cap));
     TRY(dalloc(h, &s.rc, s.cap));
+    TRY(dalloc(h, &s.rc2, s.cap));
+    TRY(dalloc(h, &s.p2, n));
     TRY(dalloc(h, &s.du, s.cap));
     TRY(dalloc(h, &s.vcnt, n));
     TRY(dalloc(h, &s.vfill, n));
@@ -1075,6 +1098,8 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &h->hist, hist_n));
     if (d->broad_phase < 0 || d->broad_phase > 2) return fail(h, ADMM_ERR_INVALID, "broad_phase must be 0, 1 or 2");
     h->use_grid = d->broad_phase != 1;
+    if (d->contact_mode < 0 || d->contact_mode > 2) return fail(h, ADMM_ERR_INVALID, "contact_mode must be 0, 1 or 2");
+    h->contact_fused = d->contact_mode == 2;
     TRY(setup_grid(h, d));
     const int scan_n = std::max(std::max(std::max(scan_tiles(hist_n), scan_tiles(n + 1)), scan_tiles(s.nsv + s.nse + 1)),
                                 scan_tiles(h->grid_buckets)) + 4;
@@ -1091,6 +1116,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
 
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking));
+
     h->cstream = h->stream;
     {
         const int every = d->residual_check_every > 0 ? d->residual_check_every : h->dcd_interval;
@@ -1223,6 +1249,7 @@ void admm_b200_destroy(AdmmB200* h) {
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->body_stream) cudaStreamDestroy(h->body_stream);
+
     delete h;
 }
 
@@ -1451,7 +1478,8 @@ int admm_b200_contact_step(AdmmB200* h) {
     if (!h) return ADMM_ERR_INVALID;
     if (!h->s.contact || !h->detected) return fail(h, ADMM_ERR_STATE, "contact_step needs a detection first");
     CK(cudaSetDevice(h->device));
-    enqueue_contact(h, false);
+    h->cstream = h->stream;
+    TRY(enqueue_contact(h, false));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
     return ADMM_OK;

@@ -1,6 +1,7 @@
 // kernels.cuh -- per-iteration ADMM kernels (local step, dual updates, RHS,
 // Jacobi sweeps, integration, residuals).
 #pragma once
+#include "contact.cuh"
 #include "prox.cuh"
 #include "scene_dev.cuh"
 
@@ -186,10 +187,7 @@ __global__ void __launch_bounds__(kVertThreads) k_pre_integration(DevScene s) {
 //   WARM  : p += sum_c Gamma_c,i r_c        (update_p_kernel, contact_solver.cu:316-335)
 // ---------------------------------------------------------------------------
 template <bool DUALC, bool WARM>
-__global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
-    ADMM_PDL_PROLOGUE();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.nd) return;
+ADMM_DEV void contact_p_one(const DevScene& s, int i) {
     const float4 x = s.x[i], x0 = s.x0[i];
     float4 uc = s.uc[i];
     if (DUALC) {
@@ -215,6 +213,14 @@ __global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
         }
     }
     s.p[i] = p;
+}
+
+template <bool DUALC, bool WARM>
+__global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
+    ADMM_PDL_PROLOGUE();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.nd) return;
+    contact_p_one<DUALC, WARM>(s, i);
 }
 
 // Gather of one sliced-ELL row: the warp `w` (a slice) accumulates sum val * v[col]

@@ -110,6 +110,8 @@ struct DevScene {
     float4* gamma = nullptr;              // Gamma_c per contact slot
     float4* kc = nullptr;
     float4* rc = nullptr;
+    float4* rc2 = nullptr;                // second r_c buffer of the fused contact passes
+    float4* p2 = nullptr;                 // [n] second p buffer of the fused contact passes
     float4* du = nullptr;
     int* vcnt = nullptr;                  // [n] contacts per vertex
     int* vfill = nullptr;                 // [n]
