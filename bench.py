@@ -234,13 +234,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cube", choices=sorted(CONFIGS))
-    ap.add_argument("--probe", default="local", choices=["local", "jacobi", "rhs"])
+    ap.add_argument("--probe", default="jacobi", choices=["local", "jacobi", "rhs"])
     ap.add_argument("--cpu-stride", type=int, default=10, help="CPU-baseline sample: one substep every N frames")
     ap.add_argument("--tol", type=float, default=1e-4, help="ADMM residual tolerance (0 = fixed iteration count)")
+    ap.add_argument("--ell-lanes", type=int, default=0, choices=[0, 1, 2, 4, 8],
+                    help="pin the lanes per row of both sliced-ELL matrices (0 = autotuned; pin it under a profiler, "
+                         "whose serialised launches mislead the autotuner)")
     ap.add_argument("--jacobi-mode", type=int, default=0, choices=[0, 1, 2],
                     help="global step: 0 autotuned, 1 one kernel per sweep, 2 persistent kernel")
     ap.add_argument("--ref-steps", type=int, default=200, help="cap on steps timed by --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--start-frame", type=int, default=0,
+                    help="advance this many substeps (untimed) before the timed region, e.g. to time contact frames")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="open a CUDA profiler range (cudaProfilerStart/Stop) around the first N timed steps, "
                          "for ncu --profile-from-start off")
@@ -265,6 +270,7 @@ def main():
 
     sc = make_scene(args.config)
     sc.params.jacobi_mode = args.jacobi_mode
+    sc.params.ell_lanes = args.ell_lanes
     h = B.Handle(sc, device=local, residual_tol=args.tol)
     h.set_probe(args.probe)
     for _ in range(args.warmup):
@@ -272,6 +278,9 @@ def main():
     h.probe_time()
     h.reset()
 
+    for _ in range(args.start_frame):
+        h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+    h.probe_time()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     dev_ms = []
     contacts = []

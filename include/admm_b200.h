@@ -116,13 +116,6 @@ typedef struct AdmmB200Desc {
      * structure, bvh_refit applies); 2 = uniform-grid spatial hash.  Both report
      * the same pair set; the order of the contact list differs. */
     int32_t broad_phase;
-    /* Contact step of an ADMM iteration: 0 = default (1); 1 = two kernels per
-     * Jacobi pass, friction-cone projection then gather (the reference's
-     * get_delta_u_kernel / update_p); 2 = one fused kernel per pass, in which
-     * every vertex recomputes the projections of its own contacts (half the
-     * launches, but a longer dependent-load chain per thread: slower on the
-     * 20^3 cube).  Both give identical bits. */
-    int32_t contact_mode;
 } AdmmB200Desc;
 
 /* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */

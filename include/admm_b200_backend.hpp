@@ -35,7 +35,6 @@ public:
     int ell_lanes = 0;    // 0 = autotuned
     int jacobi_mode = 0;  // 0 = autotuned
     int broad_phase = 0;  // 0 = default (uniform grid)
-    int contact_mode = 0; // 0 = default (two kernels per contact pass)
 
     ~ADMMInnerB200() override {
         if (h_) admm_b200_destroy(h_);
@@ -194,7 +193,6 @@ private:
         d.ell_lanes = ell_lanes;
         d.jacobi_mode = jacobi_mode;
         d.broad_phase = broad_phase;
-        d.contact_mode = contact_mode;
     }
 };
 

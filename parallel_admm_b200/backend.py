@@ -72,7 +72,7 @@ class AdmmB200Desc(ctypes.Structure):
         ("enable_contact", ctypes.c_int32), ("warmstart_ue", ctypes.c_int32), ("warmstart_uc", ctypes.c_int32),
         ("residual_tol", ctypes.c_float), ("residual_check_every", ctypes.c_int32),
         ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32), ("jacobi_mode", ctypes.c_int32),
-        ("broad_phase", ctypes.c_int32), ("contact_mode", ctypes.c_int32),
+        ("broad_phase", ctypes.c_int32),
     ]
 
 
@@ -137,7 +137,6 @@ class DescHolder:
         d.ell_lanes = int(p.ell_lanes)
         d.jacobi_mode = int(p.jacobi_mode)
         d.broad_phase = int(p.broad_phase)
-        d.contact_mode = int(p.contact_mode)
         for k, v in overrides.items():
             setattr(d, k, v)
         self.desc = d

@@ -55,7 +55,6 @@ struct AdmmB200 {
     bool warmstart_ue = true, warmstart_uc = true;
     bool bvh_refit = true;
     bool use_grid = true;           // broad phase: uniform grid (true) or LBVH
-    bool contact_fused = false;     // one kernel per contact pass (true) or the two of the reference
     int enqueue_rc = ADMM_OK;       // first error while enqueueing or capturing a substep
     float grid_cell_size = 0.f;
     int grid_buckets = 0;
@@ -319,8 +318,9 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
         h->launch_counter += 3;
     }
     LAUNCH(k_contact_fill, h->contact_grid, kContactThreads, s);
-    LAUNCH(k_contact_sort_lists, blocks(s.nd, kContactThreads), kContactThreads, s);
+    LAUNCH(k_contact_sort_lists, blocks(s.nd * 32, kContactThreads), kContactThreads, s);
     LAUNCH(k_contact_scc, h->contact_grid, kContactThreads, s);
+    LAUNCH(k_contact_incidence, h->contact_grid, kContactThreads, s);
 }
 
 void enqueue_local(AdmmB200* h, int mode) {
@@ -335,29 +335,19 @@ void enqueue_local(AdmmB200* h, int mode) {
         LAUNCH(k_local<LOCAL_DUAL>, g, kLocalThreads, h->s, h->tet_blocks, h->tri_blocks, h->bend_blocks);
 }
 
-// Contact step of one ADMM iteration: p for every dynamic vertex, then gs_iter
-// Jacobi passes of the friction-cone projection -- one fused kernel per pass
-// (ping-pong between p/p2 and r/r2), or the reference's two kernels per pass.
+// Contact step of one ADMM iteration (project_impl, contact_solver.cu:316-431):
+// p with the warm start, then gs_iter passes of friction-cone projection and
+// gather.
 int enqueue_contact(AdmmB200* h, bool dual) {
     DevScene& s = h->s;
-    const int vb = blocks(s.nd, kVertThreads);
+    const int gb = blocks(s.nd * kGatherLanes, kContactThreads);
     set_phase(h, ADMM_PHASE_CONTACT);
-    if (dual) LAUNCH((k_contact_p<true, true>), vb, kVertThreads, s);
-    else LAUNCH((k_contact_p<false, true>), vb, kVertThreads, s);
-    const int cb = blocks(s.nd, kContactThreads);
-    if (!h->contact_fused) {
-        for (int g = 0; g < h->gs_iter; g++) {
-            LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
-            LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, cb, kContactThreads, s);
-        }
-        return ADMM_OK;
-    }
+    if (dual) LAUNCH((k_contact_p<true, true>), blocks(s.nd * kGatherLanes, kVertThreads), kVertThreads, s);
+    else LAUNCH((k_contact_p<false, true>), blocks(s.nd * kGatherLanes, kVertThreads), kVertThreads, s);
     for (int g = 0; g < h->gs_iter; g++) {
-        const bool even = (g & 1) == 0;
-        LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_pass, cb, kContactThreads, s, even ? s.p : s.p2,
-                 even ? s.p2 : s.p, even ? s.rc : s.rc2, even ? s.rc2 : s.rc);
+        LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
+        LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, gb, kContactThreads, s);
     }
-    if (h->gs_iter & 1) LAUNCH(k_contact_pass_copy, cb, kContactThreads, s, s.p2, s.rc2);
     return ADMM_OK;
 }
 
@@ -1082,8 +1072,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.gamma, s.cap));
     TRY(dalloc(h, &s.kc, s.cap));
     TRY(dalloc(h, &s.rc, s.cap));
-    TRY(dalloc(h, &s.rc2, s.cap));
-    TRY(dalloc(h, &s.p2, n));
+    TRY(dalloc(h, &s.ginc, 4 * (size_t)s.cap));
     TRY(dalloc(h, &s.du, s.cap));
     TRY(dalloc(h, &s.vcnt, n));
     TRY(dalloc(h, &s.vfill, n));
@@ -1098,8 +1087,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &h->hist, hist_n));
     if (d->broad_phase < 0 || d->broad_phase > 2) return fail(h, ADMM_ERR_INVALID, "broad_phase must be 0, 1 or 2");
     h->use_grid = d->broad_phase != 1;
-    if (d->contact_mode < 0 || d->contact_mode > 2) return fail(h, ADMM_ERR_INVALID, "contact_mode must be 0, 1 or 2");
-    h->contact_fused = d->contact_mode == 2;
+
     TRY(setup_grid(h, d));
     const int scan_n = std::max(std::max(std::max(scan_tiles(hist_n), scan_tiles(n + 1)), scan_tiles(s.nsv + s.nse + 1)),
                                 scan_tiles(h->grid_buckets)) + 4;

@@ -42,13 +42,35 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_fill(DevScene s) {
     }
 }
 
-// Sort each vertex's incidence list by (contact, slot) so the gather below
-// sums in a fixed order (the reference's order depends on atomics, F13).
+// Sort each vertex's incidence list by (contact, slot) so the gathers below
+// sum in a fixed order (the reference's order depends on atomics, F13).  One
+// warp per vertex: the keys are distinct, so each key's position is its rank,
+// counted over the list held in two registers per lane (lists up to 64); a
+// longer list is sorted by one lane.
+constexpr int kRankSortMax = 64;
+
 __global__ void __launch_bounds__(kContactThreads) k_contact_sort_lists(DevScene s) {
     ADMM_PDL_PROLOGUE();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.nd) return;
-    const int b = s.vstart[i], e = s.vstart[i + 1];
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= s.nd) return;  // whole warps
+    const int b = s.vstart[i], e = s.vstart[i + 1], L = e - b;
+    if (L <= 1) return;
+    if (L <= kRankSortMax) {
+        const int k0 = lane < L ? s.vlist[b + lane] : 0x7fffffff;
+        const int k1 = lane + 32 < L ? s.vlist[b + 32 + lane] : 0x7fffffff;
+        int r0 = 0, r1 = 0;
+        for (int j = 0; j < L; j++) {
+            const int kj = __shfl_sync(0xffffffffu, j < 32 ? k0 : k1, j & 31);
+            r0 += kj < k0;
+            r1 += kj < k1;
+        }
+        __syncwarp();
+        if (lane < L) s.vlist[b + r0] = k0;
+        if (lane + 32 < L) s.vlist[b + r1] = k1;
+        return;
+    }
+    if (lane != 0) return;
     for (int k = b + 1; k < e; k++) {
         const int key = s.vlist[k];
         int j = k - 1;
@@ -83,6 +105,42 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_scc(DevScene s) {
 }
 
 // Friction-cone projection of contact c (get_delta_u_kernel, contact_solver.cu:337-379).
+// Incidence entries in list order: (contact, Gamma_c,i) for every position of
+// the sorted lists, so that a gather needs no further indirection.
+__global__ void __launch_bounds__(kContactThreads) k_contact_incidence(DevScene s) {
+    ADMM_PDL_PROLOGUE();
+    const int n4 = 4 * ccount(s);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n4; k += gridDim.x * blockDim.x) {
+        const int slot = s.vlist[k];
+        const int c = slot >> 2;
+        s.ginc[k] = make_float2(__int_as_float(c), comp(s.gamma[c], slot & 3));
+    }
+}
+
+// Sum of Gamma_c,i v_c over the incidence entries [b, e) of one vertex by the
+// kGatherLanes lanes of a group: lane l takes entries b+l, b+l+G, ...; the
+// partial sums are combined by xor shuffles (a fixed order), every lane gets
+// the total.
+constexpr int kGatherLanes = 8;
+
+ADMM_DEV float4 gather_group(const DevScene& s, const float4* __restrict__ v, int b, int e, int sub, unsigned gmask) {
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int k = b + sub; k < e; k += kGatherLanes) {
+        const float2 gi = s.ginc[k];
+        const float4 d = v[__float_as_int(gi.x)];
+        ax = fmaf(d.x, gi.y, ax);
+        ay = fmaf(d.y, gi.y, ay);
+        az = fmaf(d.z, gi.y, az);
+    }
+#pragma unroll
+    for (int o = kGatherLanes / 2; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(gmask, ax, o, kGatherLanes);
+        ay += __shfl_xor_sync(gmask, ay, o, kGatherLanes);
+        az += __shfl_xor_sync(gmask, az, o, kGatherLanes);
+    }
+    return f4(ax, ay, az);
+}
+
 // Projection of u = sum_k bary_k p_k + K_c onto the friction cone for contact c
 // with accumulated correction r: returns du (the caller sets r_c = r + du).
 ADMM_DEV float4 friction_cone_du(const DevScene& s, int c, float ux, float uy, float uz, float4 r) {
@@ -131,84 +189,23 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_du(DevScene s) {
     }
 }
 
-// p_i += sum_c Gamma_c,i du_c over the incidence list of vertex i, entries
-// [b, e) (update_p, contact_solver.cu:381-399).
-ADMM_DEV void contact_gather_one(const DevScene& s, int i, int b, int e) {
-    float dx = 0.f, dy = 0.f, dz = 0.f;
-    for (int k = b; k < e; k++) {
-        const int slot = s.vlist[k];
-        const int c = slot >> 2;
-        const float g = comp(s.gamma[c], slot & 3);
-        const float4 d = s.du[c];
-        dx = dx + d.x * g;
-        dy = dy + d.y * g;
-        dz = dz + d.z * g;
-    }
-    float4 p = s.p[i];
-    p.x += dx;
-    p.y += dy;
-    p.z += dz;
-    s.p[i] = p;
-}
-
+// p_i += sum_c Gamma_c,i du_c over the incidence list of vertex i (update_p,
+// contact_solver.cu:381-399), kGatherLanes lanes per vertex.
 __global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s) {
     ADMM_PDL_PROLOGUE();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.nd) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / kGatherLanes, sub = t % kGatherLanes;
+    if (i >= s.nd) return;  // whole groups
     const int b = s.vstart[i], e = s.vstart[i + 1];
     if (b == e) return;
-    contact_gather_one(s, i, b, e);
-}
-
-// One whole Jacobi pass of the contact solve in one kernel (k_contact_du and
-// k_contact_gather fused): every vertex with contacts recomputes the du of its
-// incident contacts from the previous pass's p (pin) and r (rin) -- the same
-// arithmetic as k_contact_du -- and sums them in incidence-list order into
-// pout; r_c + du_c goes to rout, written by the contact's lowest slot that holds
-// a dynamic vertex.  Bit-identical to the two-kernel pass, half the launches.
-__global__ void __launch_bounds__(kContactThreads) k_contact_pass(DevScene s, const float4* __restrict__ pin,
-                                                                  float4* __restrict__ pout,
-                                                                  const float4* __restrict__ rin,
-                                                                  float4* __restrict__ rout) {
-    ADMM_PDL_PROLOGUE();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.nd) return;
-    const int b = s.vstart[i], e = s.vstart[i + 1];
-    if (b == e) return;
-    float dx = 0.f, dy = 0.f, dz = 0.f;
-    for (int k = b; k < e; k++) {
-        const int slot = s.vlist[k];
-        const int c = slot >> 2;
-        float ux, uy, uz;
-        contact_u(s, c, pin, ux, uy, uz);
-        const float4 r = rin[c];
-        const float4 d = friction_cone_du(s, c, ux, uy, uz, r);
-        const float g = comp(s.gamma[c], slot & 3);
-        dx = dx + d.x * g;
-        dy = dy + d.y * g;
-        dz = dz + d.z * g;
-        const int4 q = s.pairs[c];
-        const int writer = q.x < s.nd ? 0 : q.y < s.nd ? 1 : q.z < s.nd ? 2 : 3;
-        if ((slot & 3) == writer) rout[c] = f4(r.x + d.x, r.y + d.y, r.z + d.z);
-    }
-    float4 p = pin[i];
-    p.x += dx;
-    p.y += dy;
-    p.z += dz;
-    pout[i] = p;
-}
-
-// Copies p and r of the vertices / contacts that the passes update back from
-// the second buffers (odd pass counts).
-__global__ void __launch_bounds__(kContactThreads) k_contact_pass_copy(DevScene s, const float4* __restrict__ pin,
-                                                                       const float4* __restrict__ rin) {
-    ADMM_PDL_PROLOGUE();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < s.nd && s.vstart[i] != s.vstart[i + 1]) s.p[i] = pin[i];
-    const int nc = ccount(s);
-    for (int c = i; c < nc; c += gridDim.x * blockDim.x) {
-        const int4 q = s.pairs[c];
-        if (q.x < s.nd || q.y < s.nd || q.z < s.nd || q.w < s.nd) s.rc[c] = rin[c];
+    const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kGatherLanes - 1));
+    const float4 acc = gather_group(s, s.du, b, e, sub, gmask);
+    if (sub == 0) {
+        float4 p = s.p[i];
+        p.x += acc.x;
+        p.y += acc.y;
+        p.z += acc.z;
+        s.p[i] = p;
     }
 }
 

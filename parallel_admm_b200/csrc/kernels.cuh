@@ -186,8 +186,21 @@ __global__ void __launch_bounds__(kVertThreads) k_pre_integration(DevScene s) {
 //   p = ((x - x0) + Uc) / h                (admm_impl_gpu.cu:296-298)
 //   WARM  : p += sum_c Gamma_c,i r_c        (update_p_kernel, contact_solver.cu:316-335)
 // ---------------------------------------------------------------------------
+// p = (x - x0 + Uc) / h (after Uc += (x - x0) - h p when DUALC), plus the warm
+// start p += sum_c Gamma_c,i r_c over the incidence list (WARM); kGatherLanes
+// lanes per vertex.
 template <bool DUALC, bool WARM>
-ADMM_DEV void contact_p_one(const DevScene& s, int i) {
+__global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
+    ADMM_PDL_PROLOGUE();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / kGatherLanes, sub = t % kGatherLanes;
+    if (i >= s.nd) return;  // whole groups
+    float4 warm = f4(0.f, 0.f, 0.f);
+    if (WARM) {
+        const int b = s.vstart[i], e = s.vstart[i + 1];
+        if (b != e) warm = gather_group(s, s.rc, b, e, sub, 0xffu << (threadIdx.x & 31 & ~(kGatherLanes - 1)));
+    }
+    if (sub != 0) return;
     const float4 x = s.x[i], x0 = s.x0[i];
     float4 uc = s.uc[i];
     if (DUALC) {
@@ -199,28 +212,10 @@ ADMM_DEV void contact_p_one(const DevScene& s, int i) {
     }
     float4 p = f4(((x.x - x0.x) + uc.x) * s.dt_inv, ((x.y - x0.y) + uc.y) * s.dt_inv,
                   ((x.z - x0.z) + uc.z) * s.dt_inv);
-    if (WARM) {
-        const int b = s.vstart[i], e = s.vstart[i + 1];
-        for (int k = b; k < e; k++) {
-            const int slot = s.vlist[k];
-            const int c = slot >> 2;
-            const float4 gm = s.gamma[c];
-            const float g = (slot & 3) == 0 ? gm.x : (slot & 3) == 1 ? gm.y : (slot & 3) == 2 ? gm.z : gm.w;
-            const float4 r = s.rc[c];
-            p.x += g * r.x;
-            p.y += g * r.y;
-            p.z += g * r.z;
-        }
-    }
+    p.x += warm.x;
+    p.y += warm.y;
+    p.z += warm.z;
     s.p[i] = p;
-}
-
-template <bool DUALC, bool WARM>
-__global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
-    ADMM_PDL_PROLOGUE();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.nd) return;
-    contact_p_one<DUALC, WARM>(s, i);
 }
 
 // Gather of one sliced-ELL row: the warp `w` (a slice) accumulates sum val * v[col]

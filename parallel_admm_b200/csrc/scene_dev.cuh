@@ -110,13 +110,12 @@ struct DevScene {
     float4* gamma = nullptr;              // Gamma_c per contact slot
     float4* kc = nullptr;
     float4* rc = nullptr;
-    float4* rc2 = nullptr;                // second r_c buffer of the fused contact passes
-    float4* p2 = nullptr;                 // [n] second p buffer of the fused contact passes
     float4* du = nullptr;
     int* vcnt = nullptr;                  // [n] contacts per vertex
     int* vfill = nullptr;                 // [n]
     int* vstart = nullptr;                // [n+1]
     int* vlist = nullptr;                 // [4*cap] contact*4 + slot, sorted per vertex
+    float2* ginc = nullptr;               // [4*cap] (contact as int bits, Gamma_c,i) in list order
     // collision geometry
     int nst = 0, nse = 0, nsv = 0;
     const int4* st = nullptr;             // surface triangles (w unused)

@@ -61,7 +61,6 @@ class SolverParams:
     ell_lanes: int = 0
     jacobi_mode: int = 0  # 0 autotuned, 1 one kernel per sweep, 2 persistent global step
     broad_phase: int = 0  # 0 default (grid), 1 LBVH, 2 uniform grid
-    contact_mode: int = 0  # 0 default (1), 1 two kernels per pass, 2 one fused kernel per pass
 
 
 @dataclasses.dataclass

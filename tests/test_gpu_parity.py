@@ -458,38 +458,3 @@ def test_persistent_jacobi_entry_bitwise():
         h.close()
     for a, c in zip(*out):
         np.testing.assert_array_equal(a, c)
-
-
-@pytest.mark.parametrize("case", ["cloth_fold", "cube_impact", "cube_impact_odd_passes", "cloth_fold_large"])
-def test_contact_fused_bitwise(case):
-    """contact_mode 2 (one fused kernel per friction-cone pass) reproduces contact_mode 1
-    (projection and gather kernels per pass) bit for bit, with few and with many contacts."""
-    if case.startswith("cloth_fold"):
-        sc, x0 = _crumpled_cloth(64 if case.endswith("large") else 16)
-        v0 = np.zeros_like(x0)
-    else:
-        sc, x0, v0 = _cube_at_impact(10)
-        if case.endswith("odd_passes"):
-            sc.params.gs_max_iter = 3
-    sc.params.ell_lanes = 2
-    hs = []
-    for mode in (1, 2):
-        sc.params.contact_mode = mode
-        h = B.Handle(sc)
-        h.set_state(x0, v0)
-        hs.append(h)
-    seen = peak = 0
-    for k in range(4):
-        st = [h.step(1) for h in hs]
-        assert st[0]["n_contacts"] == st[1]["n_contacts"]
-        seen += st[0]["n_contacts"]
-        peak = max(peak, st[0]["n_contacts"])
-        xa, va = hs[0].get_state()
-        xb, vb = hs[1].get_state()
-        np.testing.assert_array_equal(xa, xb)
-        np.testing.assert_array_equal(va, vb)
-    assert seen > 0
-    if case.endswith("large"):
-        assert peak > 4096
-    for h in hs:
-        h.close()
