@@ -318,7 +318,7 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
         h->launch_counter += 3;
     }
     LAUNCH(k_contact_fill, h->contact_grid, kContactThreads, s);
-    LAUNCH(k_contact_sort_lists, blocks(s.nd * 32, kContactThreads), kContactThreads, s);
+    LAUNCH(k_contact_sort_lists, blocks(s.n * 32, kContactThreads), kContactThreads, s);
     LAUNCH(k_contact_scc, h->contact_grid, kContactThreads, s);
     LAUNCH(k_contact_incidence, h->contact_grid, kContactThreads, s);
 }
@@ -887,6 +887,9 @@ int setup_grid(AdmmB200* h, const AdmmB200Desc* d) {
     TRY(dalloc(h, &g.big_edge, std::max(s.nse, 1)));
     TRY(dalloc(h, &g.mode, std::max(ne, 1)));
     TRY(dalloc(h, &g.qkey, std::max(s.cap, 1)));
+    const size_t lanes = (size_t)std::max(s.nsv + s.nse, 1) * kQueryLanes;
+    TRY(dalloc(h, &g.qhits, lanes * kQueryHits));
+    TRY(dalloc(h, &g.qlane, lanes));
     return ADMM_OK;
 }
 
@@ -1073,6 +1076,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.kc, s.cap));
     TRY(dalloc(h, &s.rc, s.cap));
     TRY(dalloc(h, &s.ginc, 4 * (size_t)s.cap));
+    TRY(dalloc(h, &s.vtmp, 4 * (size_t)s.cap));
     TRY(dalloc(h, &s.du, s.cap));
     TRY(dalloc(h, &s.vcnt, n));
     TRY(dalloc(h, &s.vfill, n));

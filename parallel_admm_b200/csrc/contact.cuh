@@ -37,48 +37,45 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_fill(DevScene s) {
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const int pos = atomicAdd(&s.vfill[v[k]], 1);
-            s.vlist[s.vstart[v[k]] + pos] = 4 * c + k;
+            s.vtmp[s.vstart[v[k]] + pos] = 4 * c + k;
         }
     }
 }
 
 // Sort each vertex's incidence list by (contact, slot) so the gathers below
-// sum in a fixed order (the reference's order depends on atomics, F13).  One
-// warp per vertex: the keys are distinct, so each key's position is its rank,
-// counted over the list held in two registers per lane (lists up to 64); a
-// longer list is sorted by one lane.
-constexpr int kRankSortMax = 64;
+// sum in a fixed order (the reference's order depends on atomics, F13).  The
+// fill leaves the lists unsorted in vtmp; one warp per vertex writes each key
+// to vlist at its rank (the keys are distinct), counted against the list held
+// in two registers per lane up to 64 keys, else read back from vtmp.  Static
+// vertices are sorted too: their lists are read by no gather, but k_contact_p
+// and the incidence entries cover all positions.
+constexpr int kRankSortRegs = 64;
 
 __global__ void __launch_bounds__(kContactThreads) k_contact_sort_lists(DevScene s) {
     ADMM_PDL_PROLOGUE();
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (i >= s.nd) return;  // whole warps
+    if (i >= s.n) return;  // whole warps
     const int b = s.vstart[i], e = s.vstart[i + 1], L = e - b;
-    if (L <= 1) return;
-    if (L <= kRankSortMax) {
-        const int k0 = lane < L ? s.vlist[b + lane] : 0x7fffffff;
-        const int k1 = lane + 32 < L ? s.vlist[b + 32 + lane] : 0x7fffffff;
+    if (L <= 0) return;
+    if (L <= kRankSortRegs) {
+        const int k0 = lane < L ? s.vtmp[b + lane] : 0x7fffffff;
+        const int k1 = lane + 32 < L ? s.vtmp[b + 32 + lane] : 0x7fffffff;
         int r0 = 0, r1 = 0;
         for (int j = 0; j < L; j++) {
             const int kj = __shfl_sync(0xffffffffu, j < 32 ? k0 : k1, j & 31);
             r0 += kj < k0;
             r1 += kj < k1;
         }
-        __syncwarp();
         if (lane < L) s.vlist[b + r0] = k0;
         if (lane + 32 < L) s.vlist[b + r1] = k1;
         return;
     }
-    if (lane != 0) return;
-    for (int k = b + 1; k < e; k++) {
-        const int key = s.vlist[k];
-        int j = k - 1;
-        while (j >= b && s.vlist[j] > key) {
-            s.vlist[j + 1] = s.vlist[j];
-            j--;
-        }
-        s.vlist[j + 1] = key;
+    for (int m = lane; m < L; m += 32) {
+        const int key = s.vtmp[b + m];
+        int r = 0;
+        for (int j = 0; j < L; j++) r += s.vtmp[b + j] < key;
+        s.vlist[b + r] = key;
     }
 }
 

@@ -192,7 +192,7 @@ ADMM_DEV void grid_sort_segment(const DevScene& s, int b, int e) {
 // the index rules and the narrow phase.
 // ---------------------------------------------------------------------------
 constexpr int kQueryLanes = 8;
-constexpr int kQueryHits = 8;  // hits a lane keeps in registers between counting and writing
+constexpr int kQueryHits = 4;  // hits per lane that the count pass records for the write pass
 
 ADMM_DEV int3 grid_cell_at(int3 a, int3 b, int ci) {
     const int dx = b.x - a.x + 1, dy = b.y - a.y + 1;
@@ -341,18 +341,26 @@ __global__ void __launch_bounds__(128) k_grid_query(DevScene s) {
     } else {
         lo = edge_box_lo(s, e, up);
     }
-    int hits[kQueryHits];
+    // Count pass: walk the grid, record up to kQueryHits partners per lane in
+    // qhits and the lane's hit count in qlane.  Write pass: take the recorded
+    // partners (the walk again only for a lane with more hits).
+    int* my_hits = s.grid.qhits + (size_t)t * kQueryHits;
     int n = 0;
-    auto consider = [&](int partner) {
-        int4 ids;
-        NpResult r;
-        if (vf ? grid_hit_vf(s, v, P, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r)) {
-            if (n < kQueryHits) hits[n] = partner;
-            n++;
-        }
-    };
-    if (vf) grid_walk_vf(s, P, sub, consider);
-    else grid_walk_ee(s, e, lo, up, sub, consider);
+    if (!WRITE) {
+        auto consider = [&](int partner) {
+            int4 ids;
+            NpResult r;
+            if (vf ? grid_hit_vf(s, v, P, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r)) {
+                if (n < kQueryHits) my_hits[n] = partner;
+                n++;
+            }
+        };
+        if (vf) grid_walk_vf(s, P, sub, consider);
+        else grid_walk_ee(s, e, lo, up, sub, consider);
+        s.grid.qlane[t] = n;
+    } else {
+        n = s.grid.qlane[t];
+    }
     // group sum / exclusive prefix of the lane counts
     int incl = n;
 #pragma unroll
@@ -380,7 +388,7 @@ __global__ void __launch_bounds__(128) k_grid_query(DevScene s) {
         }
     };
     if (n <= kQueryHits) {
-        for (int k = 0; k < n; k++) emit(hits[k]);
+        for (int k = 0; k < n; k++) emit(my_hits[k]);
     } else if (vf) {
         grid_walk_vf(s, P, sub, emit);
     } else {

@@ -63,6 +63,8 @@ struct GridDev {
     int* big_edge = nullptr;       // [n surface edges]
     int* mode = nullptr;           // [triangles + edges] 1 = in the grid, 0 = big list
     int* qkey = nullptr;           // [contact capacity] partner index per contact slot
+    int* qhits = nullptr;          // [queries * lanes * hits] partners found by the count pass
+    int* qlane = nullptr;          // [queries * lanes] hits per lane
 };
 
 struct DevScene {
@@ -116,6 +118,7 @@ struct DevScene {
     int* vstart = nullptr;                // [n+1]
     int* vlist = nullptr;                 // [4*cap] contact*4 + slot, sorted per vertex
     float2* ginc = nullptr;               // [4*cap] (contact as int bits, Gamma_c,i) in list order
+    int* vtmp = nullptr;                  // [4*cap] incidence lists before sorting
     // collision geometry
     int nst = 0, nse = 0, nsv = 0;
     const int4* st = nullptr;             // surface triangles (w unused)
