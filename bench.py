@@ -249,7 +249,8 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="open a CUDA profiler range (cudaProfilerStart/Stop) around the first N timed steps, "
                          "for ncu --profile-from-start off")
-    ap.add_argument("--profile", action="store_true", help="also print a per-phase kernel-time breakdown")
+    ap.add_argument("--profile", action="store_true", help="phase pass over all timed frames (default: the first 50)")
+    ap.add_argument("--phase-steps", type=int, default=50, help="substeps of the phase-probe pass (roofline)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -344,18 +345,24 @@ def main():
     e2e_value = world * args.steps / float(te.item())
     bytes_io = 2 * sc.n_vert * 3 * 4
 
+    # Device time per phase inside the step graph (events at phase changes, so the launch gaps
+    # inside a phase are included), over the same frames as the timed region (the first
+    # --phase-steps of them); with a residual tolerance only the first chunk of each step is
+    # covered.  The roofline below divides the probed kernel's bytes by its phase's time per launch.
     phases = None
-    if args.profile and rank == 0:
-        # device time per phase inside the step graph (events at phase changes), same frames;
-        # with a residual tolerance only the first chunk of each step is covered
+    if rank == 0:
+        nph = args.steps if args.profile else min(args.steps, args.phase_steps)
         h.reset()
+        for _ in range(args.start_frame):
+            h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
         h.set_probe("phases")
         h.phase_times()
-        for _ in range(args.steps):
+        for _ in range(nph):
             h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
-        phases = {k: {"ms_per_step": v["ms"] / args.steps, "launches_per_step": v["launches"] / args.steps}
-                  for k, v in h.phase_times().items()}
-        phases["scope"] = "first chunk of each step" if args.tol > 0 else "whole step"
+        raw = h.phase_times()
+        phases = {k: {"ms_per_step": v["ms"] / nph, "launches_per_step": v["launches"] / nph} for k, v in raw.items()}
+        phases["scope"] = (f"frames {args.start_frame}..{args.start_frame + nph - 1}, "
+                           + ("first chunk of each step" if args.tol > 0 else "whole step"))
         h.set_probe(args.probe)
 
     if world > 1:
@@ -365,7 +372,9 @@ def main():
 
     peak_gbs, peak_kind = load_peaks()
     alg = algorithmic_bytes(sc, args.probe)
-    achieved = alg / (probe_ms * 1e-3) / 1e9 if probe_ms > 0 else None
+    ph = phases.get(args.probe, {}) if phases else {}
+    phase_ms = ph["ms_per_step"] / ph["launches_per_step"] if ph.get("launches_per_step") else 0.0
+    achieved = alg / (phase_ms * 1e-3) / 1e9 if phase_ms > 0 else None
     traffic = None
     tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tp):
@@ -394,7 +403,11 @@ def main():
         "roofline": {"bound": "hbm", "kernel": args.probe, "achieved": achieved, "peak": peak_gbs,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak_gbs) if achieved else None, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": alg, "mean_launch_ms": probe_ms, "launches_timed": probe_n},
+                     "algorithmic_bytes_per_launch": alg, "mean_launch_ms": phase_ms,
+                     "mean_launch_ms_how": "device time of the kernel's phase in the step graph / its launches",
+                     "isolated_launch_ms": probe_ms, "isolated_launches": probe_n,
+                     "isolated_how": "event pair around each of the first launches of the class (adds the "
+                                     "event overhead, breaks the programmatic overlap)"},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "status": status,
