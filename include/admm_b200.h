@@ -116,6 +116,13 @@ typedef struct AdmmB200Desc {
      * structure, bvh_refit applies); 2 = uniform-grid spatial hash.  Both report
      * the same pair set; the order of the contact list differs. */
     int32_t broad_phase;
+    /* Global step solver (no reference counterpart beyond 0): 0 = jacobi_iter
+     * Jacobi sweeps (ADMMImplGPU); 1 = pcg_iter iterations of conjugate gradients
+     * preconditioned by diag(A); 2 = the same with the per-vertex 3x3 blocks set
+     * by admm_b200_set_preconditioner (diag(A) until then).  pcg_iter 0 =
+     * max(1, jacobi_iter / 2): the same kernel count as the Jacobi sweeps. */
+    int32_t global_solver;
+    int32_t pcg_iter;
 } AdmmB200Desc;
 
 /* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */
@@ -275,6 +282,10 @@ int  admm_b200_kernels_per_step(AdmmB200* h, int* n);
 /* Autotuner choices made at create: lanes per row of the sliced-ELL copies of
  * A (Jacobi) and h^2 D^T W^2 (right-hand side), and the measured ms per launch. */
 int  admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float* ms_r);
+/* Per-vertex 3x3 preconditioner blocks (row-major, 9 floats per dynamic
+ * vertex) for global_solver 2, e.g. the output of the learned preconditioner.
+ * No reference counterpart. */
+int  admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd);
 /* How the global step runs (jacobi_mode): persistent = 1 for the one-kernel
  * global step (blocks = its grid), 0 for one kernel per sweep; the autotuner's
  * ms per global step in both modes (0 when not timed). */

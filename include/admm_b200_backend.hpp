@@ -35,6 +35,8 @@ public:
     int ell_lanes = 0;    // 0 = autotuned
     int jacobi_mode = 0;  // 0 = autotuned
     int broad_phase = 0;  // 0 = default (uniform grid)
+    int global_solver = 0;  // 0 = Jacobi as the reference
+    int pcg_iter = 0;
 
     ~ADMMInnerB200() override {
         if (h_) admm_b200_destroy(h_);
@@ -193,6 +195,8 @@ private:
         d.ell_lanes = ell_lanes;
         d.jacobi_mode = jacobi_mode;
         d.broad_phase = broad_phase;
+        d.global_solver = global_solver;
+        d.pcg_iter = pcg_iter;
     }
 };
 

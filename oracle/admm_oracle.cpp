@@ -219,6 +219,8 @@ struct Oracle {
     bool contact, ws_ue, ws_uc;
     float residual_tol = 0.f;
     int chunk = 0;
+    int global_solver = 0, pcg_iter = 0;
+    std::vector<R> pblock;  // [9 nd] learned 3x3 preconditioner blocks (global_solver 2)
     // matrices
     Csr D;        // m x nd
     Csr A;        // nd x nd off-diagonal part
@@ -275,6 +277,8 @@ struct Oracle {
         gs_max_iter = d->gs_max_iter; jacobi_iter = d->jacobi_iter;
         contact = d->enable_contact != 0; ws_ue = d->warmstart_ue != 0; ws_uc = d->warmstart_uc != 0;
         residual_tol = d->residual_tol;
+        global_solver = d->global_solver;
+        pcg_iter = d->pcg_iter > 0 ? d->pcg_iter : std::max(1, d->jacobi_iter / 2);
         {
             const int every = d->residual_check_every > 0 ? d->residual_check_every : dcd_interval;
             chunk = (every + dcd_interval - 1) / dcd_interval * dcd_interval;
@@ -589,6 +593,70 @@ struct Oracle {
         }
     }
 
+    // Global step with preconditioned CG (global_solver > 0; no reference
+    // counterpart): Chronopoulos-Gear PCG on A (x) I3 over the 3 nd unknowns,
+    // warm-started from x, `iters` updates, the same recurrences as the GPU
+    // kernels (k_pcg_init / k_pcg_spmv / k_pcg_update), dot products in FP64.
+    void apply_A(const std::vector<R>& v, std::vector<R>& out) {
+        for (int i = 0; i < nd; i++)
+            for (int k = 0; k < 3; k++) {
+                R acc = 0;
+                for (int a = A.start[i]; a < A.start[i + 1]; a++) acc += v[3 * A.col[a] + k] * (R)A.val[a];
+                out[3 * i + k] = acc + Adiag[i] * v[3 * i + k];
+            }
+    }
+    void precond(const std::vector<R>& r, std::vector<R>& u) {
+        for (int i = 0; i < nd; i++) {
+            if (global_solver == 2 && !pblock.empty()) {
+                const R* B = &pblock[9 * i];
+                for (int k = 0; k < 3; k++)
+                    u[3 * i + k] = B[3 * k] * r[3 * i] + B[3 * k + 1] * r[3 * i + 1] + B[3 * k + 2] * r[3 * i + 2];
+            } else {
+                for (int k = 0; k < 3; k++) u[3 * i + k] = r[3 * i + k] / Adiag[i];
+            }
+        }
+    }
+    void pcg(int iters) {
+        const int N = 3 * nd;
+        std::vector<R> r(N), u(N), w(N), pv(N, R(0)), sv(N, R(0)), ax(N);
+        apply_A(x, ax);
+        for (int i = 0; i < N; i++) r[i] = b[i] - ax[i];
+        precond(r, u);
+        double gamma_prev = 0, alpha_prev = 0;
+        for (int it = 0; it < iters; it++) {
+            apply_A(u, w);
+            double gamma = 0, delta = 0;
+            for (int i = 0; i < N; i++) {
+                gamma += (double)r[i] * (double)u[i];
+                delta += (double)w[i] * (double)u[i];
+            }
+            double alpha, beta;
+            if (it == 0) {
+                beta = 0;
+                alpha = delta != 0 ? gamma / delta : 0;
+            } else {
+                beta = gamma_prev != 0 ? gamma / gamma_prev : 0;
+                const double den = delta - beta * gamma / (alpha_prev != 0 ? alpha_prev : 1.0);
+                alpha = den != 0 ? gamma / den : 0;
+            }
+            gamma_prev = gamma;
+            alpha_prev = alpha;
+            const R a = (R)alpha, bt = (R)beta;
+            for (int i = 0; i < N; i++) {
+                pv[i] = u[i] + bt * pv[i];
+                sv[i] = w[i] + bt * sv[i];
+                x[i] = x[i] + a * pv[i];
+                r[i] = r[i] - a * sv[i];
+            }
+            precond(r, u);
+        }
+    }
+
+    void global_solve() {
+        if (global_solver > 0) pcg(pcg_iter);
+        else jacobi(jacobi_iter);
+    }
+
     // Residuals after the global solve of an iteration, before its dual update:
     //   primal^2 = sum w^2 |D x - z|^2 + sum w_c |x - x0 - h p|^2
     //   dual^2   = sum w^2 |D (x - x_prev)|^2 + sum w_c |x - x_prev|^2
@@ -647,7 +715,7 @@ struct Oracle {
             xprev = x;
             std::vector<R> dxprev;
             Dx_rows(dxprev);
-            jacobi(jacobi_iter);
+            global_solve();
             std::vector<R> dx;
             Dx_rows(dx);
             double prim, dual, den;
@@ -777,6 +845,18 @@ void orc_rhs(void* hp) {
 void orc_jacobi(void* hp, int sweeps) {
     Handle* h = (Handle*)hp;
     if (h->d) h->d->jacobi(sweeps); else h->f->jacobi(sweeps);
+}
+
+void orc_pcg(void* hp, int iters) {
+    Handle* h = (Handle*)hp;
+    if (h->d) h->d->pcg(iters); else h->f->pcg(iters);
+}
+
+// Learned preconditioner blocks (9 per dynamic vertex, row-major) for global_solver 2.
+void orc_set_preconditioner(void* hp, const float* blocks, int nd) {
+    Handle* h = (Handle*)hp;
+    if (h->d) h->d->pblock.assign(blocks, blocks + 9 * (size_t)nd);
+    else h->f->pblock.assign(blocks, blocks + 9 * (size_t)nd);
 }
 
 // The contact sub-problem on the last detection, from the current x, x0, Uc:

@@ -50,6 +50,8 @@ def lib():
         for fn in ("orc_local_step", "orc_pre_integration", "orc_rhs", "orc_contact_step"):
             getattr(L, fn).argtypes = [ctypes.c_void_p]
         L.orc_jacobi.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_pcg.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_preconditioner.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.orc_detect.restype = ctypes.c_int
         L.orc_detect.argtypes = [ctypes.c_void_p]
         L.orc_contacts.restype = ctypes.c_int
@@ -147,6 +149,13 @@ class Oracle:
 
     def jacobi(self, sweeps: int):
         lib().orc_jacobi(self.h, sweeps)
+
+    def pcg(self, iters: int):
+        lib().orc_pcg(self.h, iters)
+
+    def set_preconditioner(self, blocks: np.ndarray):
+        blk = np.ascontiguousarray(blocks, np.float32).reshape(-1, 9)
+        lib().orc_set_preconditioner(self.h, blk.ctypes.data, blk.shape[0])
 
     def contact_step(self):
         lib().orc_contact_step(self.h)

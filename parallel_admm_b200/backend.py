@@ -72,7 +72,7 @@ class AdmmB200Desc(ctypes.Structure):
         ("enable_contact", ctypes.c_int32), ("warmstart_ue", ctypes.c_int32), ("warmstart_uc", ctypes.c_int32),
         ("residual_tol", ctypes.c_float), ("residual_check_every", ctypes.c_int32),
         ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32), ("jacobi_mode", ctypes.c_int32),
-        ("broad_phase", ctypes.c_int32),
+        ("broad_phase", ctypes.c_int32), ("global_solver", ctypes.c_int32), ("pcg_iter", ctypes.c_int32),
     ]
 
 
@@ -137,6 +137,8 @@ class DescHolder:
         d.ell_lanes = int(p.ell_lanes)
         d.jacobi_mode = int(p.jacobi_mode)
         d.broad_phase = int(p.broad_phase)
+        d.global_solver = int(p.global_solver)
+        d.pcg_iter = int(p.pcg_iter)
         for k, v in overrides.items():
             setattr(d, k, v)
         self.desc = d
@@ -190,6 +192,7 @@ def lib():
             "admm_b200_probe_time": (ctypes.c_int, [vp, _d, ctypes.POINTER(ctypes.c_int64)]),
             "admm_b200_tuning": (ctypes.c_int, [vp, _i, _i, _f, _f]),
             "admm_b200_global_mode": (ctypes.c_int, [vp, _i, _i, _f, _f]),
+            "admm_b200_set_preconditioner": (ctypes.c_int, [vp, _f, ctypes.c_int]),
             "admm_b200_jacobi_noalloc": (ctypes.c_int, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int,
                                                         vp]),
         }
@@ -213,7 +216,7 @@ def exported_symbols():
         "admm_b200_clear_contacts", "admm_b200_residuals", "admm_b200_last_step_device_ms",
         "admm_b200_set_profiling", "admm_b200_kernels_per_step", "admm_b200_step_host",
         "admm_b200_phase_times", "admm_b200_set_probe", "admm_b200_probe_time", "admm_b200_tuning",
-        "admm_b200_jacobi_noalloc", "admm_b200_global_mode",
+        "admm_b200_jacobi_noalloc", "admm_b200_global_mode", "admm_b200_set_preconditioner",
     ]
 
 
@@ -382,6 +385,11 @@ class Handle:
         self.check(lib().admm_b200_tuning(self.h, ctypes.byref(la), ctypes.byref(lr), ctypes.byref(ma),
                                           ctypes.byref(mr)), "tuning")
         return {"jacobi_lanes": la.value, "rhs_lanes": lr.value, "jacobi_ms": ma.value, "rhs_ms": mr.value}
+
+    def set_preconditioner(self, blocks: np.ndarray):
+        """Per-vertex 3x3 blocks (n_dyn x 9 or n_dyn x 3 x 3) for global_solver 2."""
+        blk = np.ascontiguousarray(blocks, np.float32).reshape(self.n_dyn, 9)
+        self.check(lib().admm_b200_set_preconditioner(self.h, _p(blk), self.n_dyn), "set_preconditioner")
 
     def global_mode(self) -> Dict[str, float]:
         """Global-step mode: persistent kernel (and its grid) or one kernel per sweep."""

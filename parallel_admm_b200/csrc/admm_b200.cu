@@ -55,6 +55,10 @@ struct AdmmB200 {
     bool warmstart_ue = true, warmstart_uc = true;
     bool bvh_refit = true;
     bool use_grid = true;           // broad phase: uniform grid (true) or LBVH
+    int global_solver = 0;          // 0 Jacobi, 1 PCG diag(A), 2 PCG learned blocks
+    int pcg_iter = 0;
+    PcgDev pcg;
+    float* pcg_blocks = nullptr;    // [9 nd] learned blocks (global_solver 2)
     int enqueue_rc = ADMM_OK;       // first error while enqueueing or capturing a substep
     float grid_cell_size = 0.f;
     int grid_buckets = 0;
@@ -437,7 +441,40 @@ void enqueue_jacobi(AdmmB200* h, int sweeps) {
     }
 }
 
+// PCG global step: init, then `iters` updates with an A u product between them
+// (2 iters + 1 launches); the result is in x.
+void enqueue_pcg(AdmmB200* h, int iters) {
+    DevScene& s = h->s;
+    set_phase(h, ADMM_PHASE_JACOBI);
+    if (iters <= 0 || s.nd <= 0) return;
+    const int ga = blocks(s.A.nslices * 32, kVertThreads), gv = blocks(s.nd, kVertThreads);
+    PcgDev& g = h->pcg;
+    g.block = (h->global_solver == 2 && h->pcg_blocks) ? h->pcg_blocks : nullptr;
+#define PCG_T(T)                                                                        \
+    do {                                                                                \
+        LAUNCH(k_pcg_init<T>, ga, kVertThreads, s, g);                                  \
+        LAUNCH(k_pcg_spmv<T>, ga, kVertThreads, s, g);                                  \
+        for (int it = 0; it < iters; it++) {                                            \
+            LAUNCH_P(ADMM_KERNEL_JACOBI, k_pcg_update, gv, kVertThreads, s, g, it);     \
+            if (it + 1 < iters) LAUNCH(k_pcg_spmv<T>, ga, kVertThreads, s, g);          \
+        }                                                                               \
+    } while (0)
+    switch (s.A.lanes) {
+        case 1: PCG_T(1); break;
+        case 2: PCG_T(2); break;
+        case 4: PCG_T(4); break;
+        default: PCG_T(8); break;
+    }
+#undef PCG_T
+}
+
 void enqueue_global(AdmmB200* h, bool save_prev) {
+    if (h->global_solver > 0) {
+        set_phase(h, ADMM_PHASE_RHS);
+        launch_rhs(h, save_prev);
+        enqueue_pcg(h, h->pcg_iter);
+        return;
+    }
     if (h->persist && h->jac_iter >= 2) {
         set_phase(h, ADMM_PHASE_JACOBI);
         launch_persist(h, true, save_prev, h->jac_iter);
@@ -1123,6 +1160,21 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         return fail(h, ADMM_ERR_INVALID, "ell_lanes must be 0, 1, 2, 4 or 8");
     TRY(autotune_ell(h, as, d->ell_lanes, &h->tune_lanes_a, &h->tune_lanes_r, &h->tune_ms_a, &h->tune_ms_r));
     if (d->jacobi_mode < 0 || d->jacobi_mode > 2) return fail(h, ADMM_ERR_INVALID, "jacobi_mode must be 0, 1 or 2");
+    if (d->global_solver < 0 || d->global_solver > 2) return fail(h, ADMM_ERR_INVALID, "global_solver must be 0, 1 or 2");
+    if (d->pcg_iter < 0) return fail(h, ADMM_ERR_INVALID, "pcg_iter");
+    h->global_solver = d->global_solver;
+    h->pcg_iter = d->pcg_iter > 0 ? d->pcg_iter : std::max(1, d->jacobi_iter / 2);
+    {
+        PcgDev& g = h->pcg;
+        TRY(dalloc(h, &g.r, nd));
+        TRY(dalloc(h, &g.u, nd));
+        TRY(dalloc(h, &g.w, nd));
+        TRY(dalloc(h, &g.p, nd));
+        TRY(dalloc(h, &g.s, nd));
+        g.blocks = blocks(s.A.nslices * 32, kVertThreads);
+        TRY(dalloc(h, &g.part, 2 * (size_t)g.blocks));
+        TRY(dalloc(h, &g.scal, 8));
+    }
     TRY(build_persist_plan(h, as.A));
     h->persist = false;
     if (h->persist_ok && h->jac_iter >= 2 && d->jacobi_mode != 1) {
@@ -1624,6 +1676,21 @@ int admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float
     if (lanes_r) *lanes_r = h->tune_lanes_r;
     if (ms_a) *ms_a = h->tune_ms_a;
     if (ms_r) *ms_r = h->tune_ms_r;
+    return ADMM_OK;
+}
+
+int admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd) {
+    if (!h || !blocks9) return ADMM_ERR_INVALID;
+    if (nd != h->s.nd) return fail(h, ADMM_ERR_INVALID, "nd must equal n_dyn");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (!h->pcg_blocks) TRY(dalloc(h, &h->pcg_blocks, 9 * (size_t)nd));
+    CK(cudaMemcpy(h->pcg_blocks, blocks9, sizeof(float) * 9 * (size_t)nd, cudaMemcpyHostToDevice));
+    // the step graph holds the preconditioner pointer: capture it again
+    if (h->step_exec) {
+        cudaGraphExecDestroy(h->step_exec);
+        h->step_exec = nullptr;
+    }
     return ADMM_OK;
 }
 

@@ -397,6 +397,144 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_global_persist(DevScene 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Preconditioned conjugate gradients for the global step (global_solver > 0),
+// a north-star addition with no counterpart in the reference.  A (x) I3 is
+// solved for the three coordinate columns at once (one 3nd-vector CG, so that
+// a 3x3 block preconditioner may couple them), warm-started from the current x.
+// Chronopoulos-Gear form: one reduction pair per iteration, two kernels:
+//   KA (k_pcg_update): alpha, beta from the reduced (gamma, delta);
+//        p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s, u = M^-1 r
+//   KB (k_pcg_spmv):   w = A u, per-block partial sums of (r, u) and (w, u)
+// Reductions are deterministic: each block writes its FP64 partials, every
+// block of the next kernel sums all of them in the same order.  The scalars
+// (gamma, alpha) of iteration i live in scal[i & 1].
+// ---------------------------------------------------------------------------
+struct PcgDev {
+    float4 *r = nullptr, *u = nullptr, *w = nullptr, *p = nullptr, *s = nullptr;
+    double* part = nullptr;        // [2 * blocks] gamma partials, then delta partials
+    double* scal = nullptr;        // [2 x 4] per iteration parity: gamma, alpha
+    const float* block = nullptr;  // [9 * nd] per-vertex 3x3 preconditioner blocks (row-major), or null
+    int blocks = 0;                // grid of k_pcg_spmv (= number of partials)
+};
+
+ADMM_DEV float4 pcg_precond(const DevScene& s, const PcgDev& g, int i, float4 r) {
+    if (g.block) {
+        const float* B = g.block + 9 * (size_t)i;
+        return f4(B[0] * r.x + B[1] * r.y + B[2] * r.z, B[3] * r.x + B[4] * r.y + B[5] * r.z,
+                  B[6] * r.x + B[7] * r.y + B[8] * r.z);
+    }
+    const float d = s.a_diag[i];
+    return f4(r.x / d, r.y / d, r.z / d);
+}
+
+ADMM_DEV double dot3d(float4 a, float4 b) {
+    return (double)a.x * (double)b.x + (double)a.y * (double)b.y + (double)a.z * (double)b.z;
+}
+
+// Sum of the n partials at part (every block, same order); result in all threads.
+ADMM_DEV double pcg_reduce(const double* __restrict__ part, int n, double* sh) {
+    double v = 0.0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) v += part[k];
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) sh[32] = v;
+    __syncthreads();
+    const double r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+// w = A v for the rows of slice w (lanes of a row hold the result), A = diag + off-diagonal ELL.
+template <int T>
+ADMM_DEV float4 pcg_apply(const DevScene& s, const float4* __restrict__ v, int wslice, int lane, int& row) {
+    const float4 acc = ell_row_sum<T>(s.A, v, wslice, lane, row);
+    if (row >= s.nd) return acc;
+    const float d = s.a_diag[row];
+    const float4 vi = v[row];
+    return f4(fmaf(d, vi.x, acc.x), fmaf(d, vi.y, acc.y), fmaf(d, vi.z, acc.z));
+}
+
+// Init, part 1: r = b - A x, u = M^-1 r, p = s = 0 (with beta = 0 the first update sets p = u, s = w).
+template <int T>
+__global__ void __launch_bounds__(kVertThreads) k_pcg_init(DevScene s, PcgDev g) {
+    ADMM_PDL_PROLOGUE();
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= s.A.nslices) return;
+    int i;
+    const float4 ax = pcg_apply<T>(s, s.x, w, lane, i);
+    if (lane >= 32 / T || i >= s.nd) return;
+    const float4 b = s.b[i];
+    const float4 r = f4(b.x - ax.x, b.y - ax.y, b.z - ax.z);
+    g.r[i] = r;
+    g.u[i] = pcg_precond(s, g, i, r);
+    g.p[i] = f4(0.f, 0.f, 0.f);
+    g.s[i] = f4(0.f, 0.f, 0.f);
+}
+
+// KB: w = A u and the block partials of (r, u), (w, u).
+template <int T>
+__global__ void __launch_bounds__(kVertThreads) k_pcg_spmv(DevScene s, PcgDev g) {
+    ADMM_PDL_PROLOGUE();
+    __shared__ double sh[40];
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    double ga = 0.0, de = 0.0;
+    if (w < s.A.nslices) {
+        int i;
+        const float4 au = pcg_apply<T>(s, g.u, w, lane, i);
+        if (lane < 32 / T && i < s.nd) {
+            g.w[i] = au;
+            const float4 u = g.u[i];
+            ga = dot3d(g.r[i], u);
+            de = dot3d(au, u);
+        }
+    }
+    ga = block_sum(ga, sh);
+    de = block_sum(de, sh);
+    if (threadIdx.x == 0) {
+        g.part[blockIdx.x] = ga;
+        g.part[g.blocks + blockIdx.x] = de;
+    }
+}
+
+// KA of iteration `it` (it = 0: beta = 0, alpha = gamma / delta).
+__global__ void __launch_bounds__(kVertThreads) k_pcg_update(DevScene s, PcgDev g, int it) {
+    ADMM_PDL_PROLOGUE();
+    __shared__ double sh[40];
+    const double gamma = pcg_reduce(g.part, g.blocks, sh);
+    const double delta = pcg_reduce(g.part + g.blocks, g.blocks, sh);
+    double alpha, beta;
+    if (it == 0) {
+        beta = 0.0;
+        alpha = delta != 0.0 ? gamma / delta : 0.0;
+    } else {
+        const double* prev = g.scal + 4 * ((it - 1) & 1);
+        beta = prev[0] != 0.0 ? gamma / prev[0] : 0.0;
+        const double den = delta - beta * gamma / (prev[1] != 0.0 ? prev[1] : 1.0);
+        alpha = den != 0.0 ? gamma / den : 0.0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* cur = g.scal + 4 * (it & 1);
+        cur[0] = gamma;
+        cur[1] = alpha;
+    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.nd) return;
+    const float a = (float)alpha, bt = (float)beta;
+    const float4 u = g.u[i], w = g.w[i];
+    float4 p = g.p[i], sv = g.s[i], x = s.x[i], r = g.r[i];
+    p = f4(fmaf(bt, p.x, u.x), fmaf(bt, p.y, u.y), fmaf(bt, p.z, u.z));
+    sv = f4(fmaf(bt, sv.x, w.x), fmaf(bt, sv.y, w.y), fmaf(bt, sv.z, w.z));
+    x = f4(fmaf(a, p.x, x.x), fmaf(a, p.y, x.y), fmaf(a, p.z, x.z));
+    r = f4(fmaf(-a, sv.x, r.x), fmaf(-a, sv.y, r.y), fmaf(-a, sv.z, r.z));
+    g.p[i] = p;
+    g.s[i] = sv;
+    s.x[i] = x;
+    g.r[i] = r;
+    g.u[i] = pcg_precond(s, g, i, r);
+}
+
 __global__ void k_copy_dyn(DevScene s, const float4* __restrict__ src, float4* __restrict__ dst) {
     ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -61,6 +61,8 @@ class SolverParams:
     ell_lanes: int = 0
     jacobi_mode: int = 0  # 0 autotuned, 1 one kernel per sweep, 2 persistent global step
     broad_phase: int = 0  # 0 default (grid), 1 LBVH, 2 uniform grid
+    global_solver: int = 0  # 0 Jacobi (reference), 1 PCG with diag(A), 2 PCG with learned blocks
+    pcg_iter: int = 0  # 0 = jacobi_iter // 2
 
 
 @dataclasses.dataclass
