@@ -65,16 +65,23 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def make_scene(cfg):
+def make_scene(args):
+    """The configured scene with the solver options of the command line applied."""
     from parallel_admm_b200 import scene
-    c = CONFIGS[cfg]
-    return getattr(scene, c["fn"])(**c["kw"])
+    c = CONFIGS[args.config]
+    sc = getattr(scene, c["fn"])(**c["kw"])
+    sc.params.jacobi_mode = args.jacobi_mode
+    sc.params.ell_lanes = args.ell_lanes
+    sc.params.global_solver = args.global_solver
+    sc.params.pcg_iter = args.pcg_iter
+    return sc
 
 
-def metric_name(tol, cap):
+def metric_name(tol, cap, solver=0, pcg_iter=0):
+    how = {0: "plain Jacobi", 1: f"PCG diag(A) x{pcg_iter}", 2: f"PCG learned blocks x{pcg_iter}"}[solver]
     if tol > 0:
-        return f"sim steps/s to ADMM residual {tol:g} (plain Jacobi, cap {cap} ADMM iterations = reference count)"
-    return f"sim steps/s (plain Jacobi, fixed {cap} ADMM iterations = reference count)"
+        return f"sim steps/s to ADMM residual {tol:g} ({how}, cap {cap} ADMM iterations = reference count)"
+    return f"sim steps/s ({how}, fixed {cap} ADMM iterations = reference count)"
 
 
 def pair_nnz(sc):
@@ -198,7 +205,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sc = make_scene(args.config)
+    sc = make_scene(args)
     from oracle import oracle as O
     from parallel_admm_b200 import backend as B
     holder = B.DescHolder(sc, residual_tol=args.tol)
@@ -215,7 +222,8 @@ def run_reference(args):
     sample = (f"frames 0..{k - 1} of the workload ({k} of {args.steps} steps; CPU time bounded), "
               f"mean {iters / k:.1f} ADMM iterations per step")
     line = {
-        "impl": "reference", "metric": metric_name(args.tol, sc.params.admm_max_iter),
+        "impl": "reference", "metric": metric_name(args.tol, sc.params.admm_max_iter, args.global_solver,
+                              args.pcg_iter or max(1, sc.params.jacobi_iter // 2)),
         "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": k, "warmup": min(args.warmup, 3),
         "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "config": {"workload": CONFIGS[args.config]["workload"]},
@@ -242,6 +250,9 @@ def main():
                          "whose serialised launches mislead the autotuner)")
     ap.add_argument("--jacobi-mode", type=int, default=0, choices=[0, 1, 2],
                     help="global step: 0 autotuned, 1 one kernel per sweep, 2 persistent kernel")
+    ap.add_argument("--global-solver", type=int, default=0, choices=[0, 1, 2],
+                    help="global step: 0 Jacobi sweeps (the reference's), 1 PCG with diag(A), 2 PCG with blocks")
+    ap.add_argument("--pcg-iter", type=int, default=0, help="PCG iterations per global step (0 = jacobi_iter / 2)")
     ap.add_argument("--ref-steps", type=int, default=200, help="cap on steps timed by --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--start-frame", type=int, default=0,
@@ -269,9 +280,7 @@ def main():
     torch.cuda.set_device(local)
     from parallel_admm_b200 import backend as B
 
-    sc = make_scene(args.config)
-    sc.params.jacobi_mode = args.jacobi_mode
-    sc.params.ell_lanes = args.ell_lanes
+    sc = make_scene(args)
     h = B.Handle(sc, device=local, residual_tol=args.tol)
     h.set_probe(args.probe)
     for _ in range(args.warmup):
@@ -388,7 +397,8 @@ def main():
                          f"each from the GPU run's state; {secs:.1f} s of CPU time (oracle FP32, OpenMP), "
                          f"mean {it_mean:.1f} ADMM iterations per step"}
     line = {
-        "metric": metric_name(args.tol, sc.params.admm_max_iter),
+        "metric": metric_name(args.tol, sc.params.admm_max_iter, args.global_solver,
+                              args.pcg_iter or max(1, sc.params.jacobi_iter // 2)),
         "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",

@@ -847,6 +847,22 @@ void orc_jacobi(void* hp, int sweeps) {
     if (h->d) h->d->jacobi(sweeps); else h->f->jacobi(sweeps);
 }
 
+// The constant global-step matrix: nnz of the off-diagonal CSR (when start is
+// null), else start[nd+1], col[nnz], val[nnz] and diag[nd] (FP64 oracle).
+int orc_system(void* hp, int32_t* start, int32_t* col, double* val, double* diag) {
+    Handle* h = (Handle*)hp;
+    if (!h->d) return -1;
+    const auto& o = *h->d;
+    if (!start) return (int)o.A.col.size();
+    for (size_t i = 0; i < o.A.start.size(); i++) start[i] = o.A.start[i];
+    for (size_t k = 0; k < o.A.col.size(); k++) {
+        col[k] = o.A.col[k];
+        val[k] = o.A.val[k];
+    }
+    for (int i = 0; i < o.nd; i++) diag[i] = o.Adiag[i];
+    return (int)o.A.col.size();
+}
+
 void orc_pcg(void* hp, int iters) {
     Handle* h = (Handle*)hp;
     if (h->d) h->d->pcg(iters); else h->f->pcg(iters);

@@ -51,6 +51,8 @@ def lib():
             getattr(L, fn).argtypes = [ctypes.c_void_p]
         L.orc_jacobi.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_pcg.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_system.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_system.restype = ctypes.c_int
         L.orc_set_preconditioner.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.orc_detect.restype = ctypes.c_int
         L.orc_detect.argtypes = [ctypes.c_void_p]
@@ -149,6 +151,20 @@ class Oracle:
 
     def jacobi(self, sweeps: int):
         lib().orc_jacobi(self.h, sweeps)
+
+    def system(self):
+        """The constant global-step matrix A as a scipy CSR (nd x nd, FP64 oracle only)."""
+        import scipy.sparse as sp
+        nnz = lib().orc_system(self.h, None, None, None, None)
+        if nnz < 0:
+            raise ValueError("system() needs the FP64 oracle")
+        start = np.zeros(self.n_dyn + 1, np.int32)
+        col = np.zeros(nnz, np.int32)
+        val = np.zeros(nnz, np.float64)
+        diag = np.zeros(self.n_dyn, np.float64)
+        lib().orc_system(self.h, start.ctypes.data, col.ctypes.data, val.ctypes.data, diag.ctypes.data)
+        off = sp.csr_matrix((val, col, start), shape=(self.n_dyn, self.n_dyn))
+        return (off + sp.diags(diag)).tocsr()
 
     def pcg(self, iters: int):
         lib().orc_pcg(self.h, iters)

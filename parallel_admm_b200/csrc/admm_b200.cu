@@ -38,6 +38,8 @@ struct AdmmB200 {
     int admm_max_iter = 0, dcd_interval = 1, gs_iter = 0, jac_iter = 0;
     int tet_blocks = 0, tri_blocks = 0, bend_blocks = 0, pin_blocks = 0;
     int contact_grid = 1;
+    int group_grid = 1;             // blocks of the kernels that walk the touched list in lane groups
+    int warp_grid = 1;              // blocks of the kernels that walk it one warp per vertex
     int* hist = nullptr;       // radix histograms
     int sort_max = 0;
     std::vector<float4> x_init, v_init;
@@ -321,8 +323,14 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
         exclusive_scan(s.vcnt, s.vstart, s.n, s.scan_tmp, s.vstart + s.n, h->cstream, h->pdl);
         h->launch_counter += 3;
     }
+    {
+        LaunchTimer lt(h, 0);
+        exclusive_scan(s.vcnt, s.tpos, s.n, s.scan_tmp, s.ntv, h->cstream, h->pdl, true);
+        h->launch_counter += 3;
+    }
+    LAUNCH(k_contact_touched, blocks(s.n, kContactThreads), kContactThreads, s);
     LAUNCH(k_contact_fill, h->contact_grid, kContactThreads, s);
-    LAUNCH(k_contact_sort_lists, blocks(s.n * 32, kContactThreads), kContactThreads, s);
+    LAUNCH(k_contact_sort_lists, h->warp_grid, kContactThreads, s);
     LAUNCH(k_contact_scc, h->contact_grid, kContactThreads, s);
     LAUNCH(k_contact_incidence, h->contact_grid, kContactThreads, s);
 }
@@ -344,13 +352,13 @@ void enqueue_local(AdmmB200* h, int mode) {
 // gather.
 int enqueue_contact(AdmmB200* h, bool dual) {
     DevScene& s = h->s;
-    const int gb = blocks(s.nd * kGatherLanes, kContactThreads);
     set_phase(h, ADMM_PHASE_CONTACT);
-    if (dual) LAUNCH((k_contact_p<true, true>), blocks(s.nd * kGatherLanes, kVertThreads), kVertThreads, s);
-    else LAUNCH((k_contact_p<false, true>), blocks(s.nd * kGatherLanes, kVertThreads), kVertThreads, s);
+    const int split = blocks(s.nd, kVertThreads);
+    if (dual) LAUNCH(k_contact_p<true>, split + h->group_grid, kVertThreads, s, split);
+    else LAUNCH(k_contact_p<false>, split + h->group_grid, kVertThreads, s, split);
     for (int g = 0; g < h->gs_iter; g++) {
         LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
-        LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, gb, kContactThreads, s);
+        LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, h->group_grid, kContactThreads, s);
     }
     return ADMM_OK;
 }
@@ -919,6 +927,7 @@ int setup_grid(AdmmB200* h, const AdmmB200Desc* d) {
     TRY(dalloc(h, &g.start, nb + 1));
     TRY(dalloc(h, &g.ent_lo, g.cap));
     TRY(dalloc(h, &g.ent_up, g.cap));
+    TRY(dalloc(h, &g.ent_key, g.cap));
     TRY(dalloc(h, &g.ctr, 4));
     TRY(dalloc(h, &g.big_tri, std::max(s.nst, 1)));
     TRY(dalloc(h, &g.big_edge, std::max(s.nse, 1)));
@@ -1136,6 +1145,11 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.res, 4));
     TRY(dalloc(h, &s.done, 4));
     h->contact_grid = std::max(1, std::min(blocks(s.cap, kContactThreads), 2 * 148));
+    h->group_grid = std::max(1, std::min(blocks(std::min(n, 4 * s.cap) * kGatherLanes, kContactThreads), 8 * 148));
+    h->warp_grid = std::max(1, std::min(blocks(std::min(n, 4 * s.cap) * 32, kContactThreads), 8 * 148));
+    TRY(dalloc(h, &s.tpos, n));
+    TRY(dalloc(h, &s.tv, n));
+    TRY(dalloc(h, &s.ntv, 1));
 
     h->tet_blocks = s.ntet ? blocks(s.ntet, kLocalThreads) : 0;
     h->tri_blocks = s.ntri ? blocks(s.ntri, kLocalThreads) : 0;

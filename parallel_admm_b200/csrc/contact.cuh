@@ -51,31 +51,41 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_fill(DevScene s) {
 // and the incidence entries cover all positions.
 constexpr int kRankSortRegs = 64;
 
+// The vertices with contacts, ascending: tv[tpos[i]] = i for vcnt[i] > 0
+// (tpos = exclusive scan of vcnt != 0, *ntv = their number).
+__global__ void __launch_bounds__(kContactThreads) k_contact_touched(DevScene s) {
+    ADMM_PDL_PROLOGUE();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < s.n && s.vcnt[i] > 0) s.tv[s.tpos[i]] = i;
+}
+
+// One warp per vertex with contacts (grid-stride over the touched list).
 __global__ void __launch_bounds__(kContactThreads) k_contact_sort_lists(DevScene s) {
     ADMM_PDL_PROLOGUE();
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (i >= s.n) return;  // whole warps
-    const int b = s.vstart[i], e = s.vstart[i + 1], L = e - b;
-    if (L <= 0) return;
-    if (L <= kRankSortRegs) {
-        const int k0 = lane < L ? s.vtmp[b + lane] : 0x7fffffff;
-        const int k1 = lane + 32 < L ? s.vtmp[b + 32 + lane] : 0x7fffffff;
-        int r0 = 0, r1 = 0;
-        for (int j = 0; j < L; j++) {
-            const int kj = __shfl_sync(0xffffffffu, j < 32 ? k0 : k1, j & 31);
-            r0 += kj < k0;
-            r1 += kj < k1;
+    const int ntv = *s.ntv;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntv; t += (gridDim.x * blockDim.x) >> 5) {
+        const int i = s.tv[t];
+        const int b = s.vstart[i], e = s.vstart[i + 1], L = e - b;
+        if (L <= kRankSortRegs) {
+            const int k0 = lane < L ? s.vtmp[b + lane] : 0x7fffffff;
+            const int k1 = lane + 32 < L ? s.vtmp[b + 32 + lane] : 0x7fffffff;
+            int r0 = 0, r1 = 0;
+            for (int j = 0; j < L; j++) {
+                const int kj = __shfl_sync(0xffffffffu, j < 32 ? k0 : k1, j & 31);
+                r0 += kj < k0;
+                r1 += kj < k1;
+            }
+            if (lane < L) s.vlist[b + r0] = k0;
+            if (lane + 32 < L) s.vlist[b + r1] = k1;
+        } else {
+            for (int m = lane; m < L; m += 32) {
+                const int key = s.vtmp[b + m];
+                int r = 0;
+                for (int j = 0; j < L; j++) r += s.vtmp[b + j] < key;
+                s.vlist[b + r] = key;
+            }
         }
-        if (lane < L) s.vlist[b + r0] = k0;
-        if (lane + 32 < L) s.vlist[b + r1] = k1;
-        return;
-    }
-    for (int m = lane; m < L; m += 32) {
-        const int key = s.vtmp[b + m];
-        int r = 0;
-        for (int j = 0; j < L; j++) r += s.vtmp[b + j] < key;
-        s.vlist[b + r] = key;
     }
 }
 
@@ -187,22 +197,26 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_du(DevScene s) {
 }
 
 // p_i += sum_c Gamma_c,i du_c over the incidence list of vertex i (update_p,
-// contact_solver.cu:381-399), kGatherLanes lanes per vertex.
+// contact_solver.cu:381-399), kGatherLanes lanes per vertex with contacts
+// (grid-stride over the touched list; static vertices skipped).
 __global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s) {
     ADMM_PDL_PROLOGUE();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = t / kGatherLanes, sub = t % kGatherLanes;
-    if (i >= s.nd) return;  // whole groups
-    const int b = s.vstart[i], e = s.vstart[i + 1];
-    if (b == e) return;
+    const int sub = threadIdx.x % kGatherLanes;
     const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kGatherLanes - 1));
-    const float4 acc = gather_group(s, s.du, b, e, sub, gmask);
-    if (sub == 0) {
-        float4 p = s.p[i];
-        p.x += acc.x;
-        p.y += acc.y;
-        p.z += acc.z;
-        s.p[i] = p;
+    const int ntv = *s.ntv;
+    const int g0 = (blockIdx.x * blockDim.x + threadIdx.x) / kGatherLanes;
+    const int gs = gridDim.x * blockDim.x / kGatherLanes;
+    for (int t = g0; t < ntv; t += gs) {  // uniform per group
+        const int i = s.tv[t];
+        if (i >= s.nd) continue;
+        const float4 acc = gather_group(s, s.du, s.vstart[i], s.vstart[i + 1], sub, gmask);
+        if (sub == 0) {
+            float4 p = s.p[i];
+            p.x += acc.x;
+            p.y += acc.y;
+            p.z += acc.z;
+            s.p[i] = p;
+        }
     }
 }
 

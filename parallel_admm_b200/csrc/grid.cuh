@@ -11,7 +11,9 @@
 // Layout: every surface triangle and edge whose box spans at most kGridMaxSpan
 // cells per axis is inserted into each cell it overlaps, in a hash table of
 // (cell, type) buckets built by count -> scan -> scatter; each entry carries
-// the element's box, so that the box test needs no further load.  Larger
+// the element's box and the key of the cell it was entered for, so that other
+// cells sharing the bucket are rejected by one 8-byte compare and the box test
+// needs no further load.  Larger
 // elements (and any that do not fit the entry capacity) go to a per-type "big"
 // list that the queries scan directly.
 //
@@ -30,18 +32,40 @@
 
 namespace admm {
 
-constexpr int kGridMaxSpan = 4;  // cells per axis an element may span in the grid
+constexpr int kGridMaxSpan = 16;  // cells per axis an element may span in the grid
 
 ADMM_DEV int grid_cell(float v, float inv_c) {
     float f = floorf(v * inv_c);
-    f = fminf(fmaxf(f, -1073741824.f), 1073741824.f);
+    f = fminf(fmaxf(f, -1048575.f), 1048575.f);  // the cell key holds 21 bits per coordinate
     return (int)f;
 }
 
+// Bucket of a cell: the low bits of the cell's Morton code, triangles in the
+// lower half of the table, edges in the upper half.  Neighbouring cells land in
+// neighbouring buckets, so the queries of neighbouring mesh vertices (which run
+// in the same warps) read the same cache lines; cells whose codes differ only
+// above the table size share a bucket and are told apart by the entry's cell key.
+ADMM_DEV unsigned grid_spread10(unsigned v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
 ADMM_DEV int grid_bucket(int ix, int iy, int iz, int type, int hmask) {
-    const unsigned h = ((unsigned)ix * 73856093u) ^ ((unsigned)iy * 19349663u) ^ ((unsigned)iz * 83492791u) ^
-                       ((unsigned)type * 2654435761u);
-    return (int)(h & (unsigned)hmask);
+    const unsigned m = grid_spread10((unsigned)ix) | (grid_spread10((unsigned)iy) << 1) |
+                       (grid_spread10((unsigned)iz) << 2);
+    const unsigned half = (unsigned)hmask >> 1;  // hmask + 1 is a power of two >= 2
+    return (int)((m & half) + (type ? half + 1u : 0u));
+}
+
+// 64-bit key of a cell (21 bits per coordinate, offset to non-negative).
+ADMM_DEV unsigned long long grid_cell_key(int ix, int iy, int iz) {
+    const unsigned long long o = 1ull << 20, m = (1ull << 21) - 1ull;
+    return (((unsigned long long)(ix + (int)o) & m) << 42) | (((unsigned long long)(iy + (int)o) & m) << 21) |
+           ((unsigned long long)(iz + (int)o) & m);
 }
 
 // Box of surface element u (triangles first, then edges); type 0 = triangle.
@@ -76,7 +100,7 @@ ADMM_DEV float grid_pad(float v, float gap) { return gap + fmaxf(gap, fabsf(v)) 
 
 // A query whose cell range is larger than this (a stretched element or far-out
 // coordinates) tests every grid element of the type directly instead.
-constexpr int kGridMaxQueryCells = 512;
+constexpr int kGridMaxQueryCells = 8192;
 
 ADMM_DEV bool grid_range_small(int3 a, int3 b) {
     const long long n = (long long)(b.x - a.x + 1) * (long long)(b.y - a.y + 1) * (long long)(b.z - a.z + 1);
@@ -90,24 +114,12 @@ ADMM_DEV void grid_query_range(const float4& lo, const float4& up, float gap, fl
                   grid_cell(up.z + grid_pad(up.z, gap), inv_c));
 }
 
-// Calls f(bucket) once for every distinct bucket of the cells [a, b] of one
-// element (two cells of an element may hash to the same bucket; the element is
-// entered there once).  Spans are at most kGridMaxSpan per axis.
+// Calls f(cell, bucket) for every cell [a, b] of one element.
 template <class F>
-ADMM_DEV void grid_for_buckets(int3 a, int3 b, int type, int hmask, F f) {
-    int seen[kGridMaxSpan * kGridMaxSpan * kGridMaxSpan];
-    int ns = 0;
+ADMM_DEV void grid_for_cells(int3 a, int3 b, int type, int hmask, F f) {
     for (int iz = a.z; iz <= b.z; iz++)
         for (int iy = a.y; iy <= b.y; iy++)
-            for (int ix = a.x; ix <= b.x; ix++) {
-                const int bk = grid_bucket(ix, iy, iz, type, hmask);
-                bool dup = false;
-                for (int j = 0; j < ns; j++) dup |= seen[j] == bk;
-                if (!dup) {
-                    seen[ns++] = bk;
-                    f(bk);
-                }
-            }
+            for (int ix = a.x; ix <= b.x; ix++) f(make_int4(ix, iy, iz, 0), grid_bucket(ix, iy, iz, type, hmask));
 }
 
 // Pass 1: bucket counts; elements that are too large (or beyond the entry
@@ -132,7 +144,7 @@ __global__ void __launch_bounds__(256) k_grid_count(DevScene s) {
     }
     g.mode[u] = in_grid ? 1 : 0;
     if (in_grid) {
-        grid_for_buckets(a, b, type, g.hmask, [&](int bk) { atomicAdd(&g.cnt[bk], 1); });
+        grid_for_cells(a, b, type, g.hmask, [&](int4, int bk) { atomicAdd(&g.cnt[bk], 1); });
     } else {
         const int k = atomicAdd(&g.ctr[1 + type], 1);
         (type == 0 ? g.big_tri : g.big_edge)[k] = id;
@@ -153,10 +165,11 @@ __global__ void __launch_bounds__(256) k_grid_scatter(DevScene s) {
     grid_range(lo, up, g.inv_c, a, b);
     lo.w = __int_as_float(id);
     up.w = __int_as_float(type);
-    grid_for_buckets(a, b, type, g.hmask, [&](int bk) {
+    grid_for_cells(a, b, type, g.hmask, [&](int4 c, int bk) {
         const int pos = g.start[bk] + atomicSub(&g.cnt[bk], 1) - 1;
         g.ent_lo[pos] = lo;
         g.ent_up[pos] = up;
+        g.ent_key[pos] = grid_cell_key(c.x, c.y, c.z);
     });
 }
 
@@ -232,8 +245,10 @@ ADMM_DEV void grid_walk_vf(const DevScene& s, float4 P, int sub, F f) {
         for (int ci = sub; ci < nc; ci += kQueryLanes) {
             const int3 c = grid_cell_at(a, b, ci);
             const int bk = grid_bucket(c.x, c.y, c.z, 0, g.hmask);
+            const unsigned long long key = grid_cell_key(c.x, c.y, c.z);
             const int k1 = g.start[bk + 1];
             for (int k = g.start[bk]; k < k1; k++) {
+                if (g.ent_key[k] != key) continue;  // another cell of the bucket
                 const float4 lo = g.ent_lo[k], up = g.ent_up[k];
                 if (__float_as_int(up.w) != 0 || !box_overlap(P, P, lo, up, gap)) continue;
                 int3 ea, eb;
@@ -275,8 +290,10 @@ ADMM_DEV void grid_walk_ee(const DevScene& s, int e, float4 lo, float4 up, int s
             for (int ci = sub; ci < nc; ci += kQueryLanes) {
                 const int3 c = grid_cell_at(a, b, ci);
                 const int bk = grid_bucket(c.x, c.y, c.z, 1, g.hmask);
+                const unsigned long long key = grid_cell_key(c.x, c.y, c.z);
                 const int k1 = g.start[bk + 1];
                 for (int k = g.start[bk]; k < k1; k++) {
+                    if (g.ent_key[k] != key) continue;
                     const float4 elo = g.ent_lo[k], eup = g.ent_up[k];
                     const int o = __float_as_int(elo.w);
                     if (__float_as_int(eup.w) != 1 || o <= e || !box_overlap(lo, up, elo, eup, gap)) continue;

@@ -187,20 +187,12 @@ __global__ void __launch_bounds__(kVertThreads) k_pre_integration(DevScene s) {
 //   WARM  : p += sum_c Gamma_c,i r_c        (update_p_kernel, contact_solver.cu:316-335)
 // ---------------------------------------------------------------------------
 // p = (x - x0 + Uc) / h (after Uc += (x - x0) - h p when DUALC), plus the warm
-// start p += sum_c Gamma_c,i r_c over the incidence list (WARM); kGatherLanes
-// lanes per vertex.
-template <bool DUALC, bool WARM>
-__global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
-    ADMM_PDL_PROLOGUE();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = t / kGatherLanes, sub = t % kGatherLanes;
-    if (i >= s.nd) return;  // whole groups
-    float4 warm = f4(0.f, 0.f, 0.f);
-    if (WARM) {
-        const int b = s.vstart[i], e = s.vstart[i + 1];
-        if (b != e) warm = gather_group(s, s.rc, b, e, sub, 0xffu << (threadIdx.x & 31 & ~(kGatherLanes - 1)));
-    }
-    if (sub != 0) return;
+// start p += sum_c Gamma_c,i r_c over the incidence list of a vertex with
+// contacts.  Blocks [0, split) take the dynamic vertices without contacts, one
+// thread each; the others walk the touched list with kGatherLanes lanes per
+// vertex.
+template <bool DUALC>
+ADMM_DEV float4 contact_p_base(const DevScene& s, int i) {
     const float4 x = s.x[i], x0 = s.x0[i];
     float4 uc = s.uc[i];
     if (DUALC) {
@@ -210,12 +202,34 @@ __global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s) {
         uc.z = uc.z + ((x.z - x0.z) - p.z * s.dt);
         s.uc[i] = uc;
     }
-    float4 p = f4(((x.x - x0.x) + uc.x) * s.dt_inv, ((x.y - x0.y) + uc.y) * s.dt_inv,
-                  ((x.z - x0.z) + uc.z) * s.dt_inv);
-    p.x += warm.x;
-    p.y += warm.y;
-    p.z += warm.z;
-    s.p[i] = p;
+    return f4(((x.x - x0.x) + uc.x) * s.dt_inv, ((x.y - x0.y) + uc.y) * s.dt_inv, ((x.z - x0.z) + uc.z) * s.dt_inv);
+}
+
+template <bool DUALC>
+__global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s, int split) {
+    ADMM_PDL_PROLOGUE();
+    if ((int)blockIdx.x < split) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i < s.nd && s.vstart[i] == s.vstart[i + 1]) s.p[i] = contact_p_base<DUALC>(s, i);
+        return;
+    }
+    const int sub = threadIdx.x % kGatherLanes;
+    const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kGatherLanes - 1));
+    const int ntv = *s.ntv;
+    const int g0 = ((blockIdx.x - split) * blockDim.x + threadIdx.x) / kGatherLanes;
+    const int gs = (gridDim.x - split) * blockDim.x / kGatherLanes;
+    for (int t = g0; t < ntv; t += gs) {
+        const int i = s.tv[t];
+        if (i >= s.nd) continue;
+        const float4 warm = gather_group(s, s.rc, s.vstart[i], s.vstart[i + 1], sub, gmask);
+        if (sub == 0) {
+            float4 p = contact_p_base<DUALC>(s, i);
+            p.x += warm.x;
+            p.y += warm.y;
+            p.z += warm.z;
+            s.p[i] = p;
+        }
+    }
 }
 
 // Gather of one sliced-ELL row: the warp `w` (a slice) accumulates sum val * v[col]

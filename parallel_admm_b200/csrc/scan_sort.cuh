@@ -38,7 +38,9 @@ ADMM_DEV int block_exclusive_scan(int v, int* sh_warp) {
     return r;
 }
 
-// Phase 1: per-tile exclusive scan in place (out) and tile totals.
+// Phase 1: per-tile exclusive scan in place (out) and tile totals.  FLAGS
+// scans (in[i] != 0) instead of in[i].
+template <bool FLAGS>
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int* __restrict__ in, int* __restrict__ out,
                                                             int n, int* __restrict__ tile_sums) {
     ADMM_PDL_PROLOGUE();
@@ -49,6 +51,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int* __restri
 #pragma unroll
     for (int k = 0; k < kScanItems; k++) {
         v[k] = (base + k < n) ? in[base + k] : 0;
+        if (FLAGS) v[k] = v[k] != 0;
         t += v[k];
     }
     const int off = block_exclusive_scan(t, sh);
@@ -96,12 +99,14 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(int* __restrict__ out
 
 inline int scan_tiles(int n) { return (n + kScanTile - 1) / kScanTile; }
 
-// exclusive scan of n ints: out[i] = sum_{j<i} in[j]; *total = sum (device).
-// tmp needs scan_tiles(n) ints.  in and out may alias.
-inline void exclusive_scan(const int* in, int* out, int n, int* tmp, int* total, cudaStream_t st, bool pdl = false) {
+// exclusive scan of n ints: out[i] = sum_{j<i} in[j] (flags: of in[j] != 0);
+// *total = sum (device).  tmp needs scan_tiles(n) ints.  in and out may alias.
+inline void exclusive_scan(const int* in, int* out, int n, int* tmp, int* total, cudaStream_t st, bool pdl = false,
+                           bool flags = false) {
     if (n <= 0) return;
     const int nt = scan_tiles(n);
-    launch_k(k_scan_tiles, dim3(nt), dim3(kScanThreads), 0, st, pdl, in, out, n, tmp);
+    if (flags) launch_k(k_scan_tiles<true>, dim3(nt), dim3(kScanThreads), 0, st, pdl, in, out, n, tmp);
+    else launch_k(k_scan_tiles<false>, dim3(nt), dim3(kScanThreads), 0, st, pdl, in, out, n, tmp);
     launch_k(k_scan_sums, dim3(1), dim3(kScanThreads), 0, st, pdl, tmp, nt, total);
     launch_k(k_scan_add, dim3(nt), dim3(kScanThreads), 0, st, pdl, out, n, (const int*)tmp);
 }

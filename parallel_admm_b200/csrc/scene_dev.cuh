@@ -58,6 +58,7 @@ struct GridDev {
     int* start = nullptr;          // [buckets + 1] bucket offsets
     float4* ent_lo = nullptr;      // [cap] element box lo, w = element index (int bits)
     float4* ent_up = nullptr;      // [cap] element box up, w = type (0 triangle, 1 edge)
+    unsigned long long* ent_key = nullptr;  // [cap] key of the cell the entry was made for
     int* ctr = nullptr;            // [4] entries reserved, big triangles, big edges
     int* big_tri = nullptr;        // [n surface triangles]
     int* big_edge = nullptr;       // [n surface edges]
@@ -119,6 +120,9 @@ struct DevScene {
     int* vlist = nullptr;                 // [4*cap] contact*4 + slot, sorted per vertex
     float2* ginc = nullptr;               // [4*cap] (contact as int bits, Gamma_c,i) in list order
     int* vtmp = nullptr;                  // [4*cap] incidence lists before sorting
+    int* tpos = nullptr;                  // [n] position of a vertex in the touched list
+    int* tv = nullptr;                    // [n] vertices with contacts, ascending
+    int* ntv = nullptr;                   // [1] their number
     // collision geometry
     int nst = 0, nse = 0, nsv = 0;
     const int4* st = nullptr;             // surface triangles (w unused)
