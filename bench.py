@@ -53,6 +53,9 @@ CONFIGS = {
                   workload="cloth 32x32 (1024 verts, 1922 tris) over a unit box, 20 ADMM iters/step, dt=1/200"),
     "sheets": dict(fn="sheets_on_sphere", kw=dict(nx=512, layers=4, seed=0),
                    workload="4 x 512^2 cloth sheets on a sphere r=0.3, 40 ADMM iters/step, dt=1/300"),
+    "sheets_small": dict(fn="sheets_on_sphere", kw=dict(nx=256, layers=2, seed=0),
+                         workload="2 x 256^2 cloth sheets on a sphere r=0.3, 40 ADMM iters/step, dt=1/300 "
+                                  "(profiling stand-in for the sheets workload)"),
 }
 
 

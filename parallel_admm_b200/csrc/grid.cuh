@@ -20,7 +20,9 @@
 // Each pair is reported once: a query visits the cells of its box inflated by
 // the gap (plus a margin that covers the rounding of the overlap test), and
 // accepts an element only in the cell that is the lower corner of the overlap
-// of the two cell ranges.  Edge-edge pairs (a, b), a < b, with both edges in the
+// of the two cell ranges -- the cell that, on every axis, is the first of the
+// query's range or the first of the element's (entries carry the latter as
+// three bits).  Edge-edge pairs (a, b), a < b, with both edges in the
 // grid belong to a; a pair of one grid edge and one big edge belongs to the
 // grid edge; a pair of two big edges to the smaller index.  Every query sorts
 // its output segment by partner index, so the contact list is independent of
@@ -164,11 +166,12 @@ __global__ void __launch_bounds__(256) k_grid_scatter(DevScene s) {
     int3 a, b;
     grid_range(lo, up, g.inv_c, a, b);
     lo.w = __int_as_float(id);
-    up.w = __int_as_float(type);
     grid_for_cells(a, b, type, g.hmask, [&](int4 c, int bk) {
         const int pos = g.start[bk] + atomicSub(&g.cnt[bk], 1) - 1;
+        // w of up: for each axis, whether this cell is the element's first
+        const int first = (c.x == a.x ? 1 : 0) | (c.y == a.y ? 2 : 0) | (c.z == a.z ? 4 : 0);
         g.ent_lo[pos] = lo;
-        g.ent_up[pos] = up;
+        g.ent_up[pos] = make_float4(up.x, up.y, up.z, __int_as_float(first));
         g.ent_key[pos] = grid_cell_key(c.x, c.y, c.z);
     });
 }
@@ -247,13 +250,14 @@ ADMM_DEV void grid_walk_vf(const DevScene& s, float4 P, int sub, F f) {
             const int bk = grid_bucket(c.x, c.y, c.z, 0, g.hmask);
             const unsigned long long key = grid_cell_key(c.x, c.y, c.z);
             const int k1 = g.start[bk + 1];
+            const int qfirst = (c.x == a.x ? 1 : 0) | (c.y == a.y ? 2 : 0) | (c.z == a.z ? 4 : 0);
             for (int k = g.start[bk]; k < k1; k++) {
                 if (g.ent_key[k] != key) continue;  // another cell of the bucket
-                const float4 lo = g.ent_lo[k], up = g.ent_up[k];
-                if (__float_as_int(up.w) != 0 || !box_overlap(P, P, lo, up, gap)) continue;
-                int3 ea, eb;
-                grid_range(lo, up, g.inv_c, ea, eb);
-                if (max(a.x, ea.x) != c.x || max(a.y, ea.y) != c.y || max(a.z, ea.z) != c.z) continue;
+                const float4 up = g.ent_up[k];
+                // once per pair: this cell is the first of the query's or of the element's range on every axis
+                if (((qfirst | __float_as_int(up.w)) & 7) != 7) continue;
+                const float4 lo = g.ent_lo[k];
+                if (!box_overlap(P, P, lo, up, gap)) continue;
                 f(__float_as_int(lo.w));
             }
         }
@@ -292,14 +296,14 @@ ADMM_DEV void grid_walk_ee(const DevScene& s, int e, float4 lo, float4 up, int s
                 const int bk = grid_bucket(c.x, c.y, c.z, 1, g.hmask);
                 const unsigned long long key = grid_cell_key(c.x, c.y, c.z);
                 const int k1 = g.start[bk + 1];
+                const int qfirst = (c.x == a.x ? 1 : 0) | (c.y == a.y ? 2 : 0) | (c.z == a.z ? 4 : 0);
                 for (int k = g.start[bk]; k < k1; k++) {
                     if (g.ent_key[k] != key) continue;
-                    const float4 elo = g.ent_lo[k], eup = g.ent_up[k];
+                    const float4 elo = g.ent_lo[k];
                     const int o = __float_as_int(elo.w);
-                    if (__float_as_int(eup.w) != 1 || o <= e || !box_overlap(lo, up, elo, eup, gap)) continue;
-                    int3 ea, eb;
-                    grid_range(elo, eup, g.inv_c, ea, eb);
-                    if (max(a.x, ea.x) != c.x || max(a.y, ea.y) != c.y || max(a.z, ea.z) != c.z) continue;
+                    if (o <= e) continue;
+                    const float4 eup = g.ent_up[k];
+                    if (((qfirst | __float_as_int(eup.w)) & 7) != 7 || !box_overlap(lo, up, elo, eup, gap)) continue;
                     f(o);
                 }
             }
@@ -322,12 +326,98 @@ ADMM_DEV void grid_walk_ee(const DevScene& s, int e, float4 lo, float4 up, int s
     }
 }
 
+// ---------------------------------------------------------------------------
+// Cheap distance filters in front of the exact narrow phase.  Closest points by
+// the Voronoi-region construction (point-triangle) and the clamped-parameter
+// construction (segment-segment), in ordinary FP32 arithmetic.  A pair is
+// dropped only when this distance exceeds 1.1 x thickness plus 1e-5 of the
+// largest coordinate -- orders of magnitude above the rounding of either
+// computation -- so the exact predicate (d < thickness) could not have accepted
+// it; non-finite intermediate values never drop a pair.  On flat cloth most
+// box-overlapping non-adjacent pairs are neighbours a cell apart, and this
+// keeps them out of the heavy non-contracting narrow phase.
+// ---------------------------------------------------------------------------
+ADMM_DEV float d3(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+ADMM_DEV float fast_pt_dist2(float4 p, float4 a, float4 b, float4 c) {
+    const float4 ab = sub3(b, a), ac = sub3(c, a), ap = sub3(p, a);
+    const float q1 = d3(ab, ap), q2 = d3(ac, ap);
+    float4 x;
+    if (q1 <= 0.f && q2 <= 0.f) {
+        x = a;
+    } else {
+        const float4 bp = sub3(p, b);
+        const float q3 = d3(ab, bp), q4 = d3(ac, bp);
+        const float4 cp = sub3(p, c);
+        const float q5 = d3(ab, cp), q6 = d3(ac, cp);
+        const float vc = q1 * q4 - q3 * q2, vb = q5 * q2 - q1 * q6, va = q3 * q6 - q5 * q4;
+        if (q3 >= 0.f && q4 <= q3) {
+            x = b;
+        } else if (vc <= 0.f && q1 >= 0.f && q3 <= 0.f) {
+            x = add3(a, scale3(ab, q1 / (q1 - q3)));
+        } else if (q6 >= 0.f && q5 <= q6) {
+            x = c;
+        } else if (vb <= 0.f && q2 >= 0.f && q6 <= 0.f) {
+            x = add3(a, scale3(ac, q2 / (q2 - q6)));
+        } else if (va <= 0.f && (q4 - q3) >= 0.f && (q5 - q6) >= 0.f) {
+            x = add3(b, scale3(sub3(c, b), (q4 - q3) / ((q4 - q3) + (q5 - q6))));
+        } else {
+            const float den = 1.f / (va + vb + vc);
+            x = add3(a, add3(scale3(ab, vb * den), scale3(ac, vc * den)));
+        }
+    }
+    const float4 d = sub3(p, x);
+    return d3(d, d);
+}
+
+ADMM_DEV float fast_ee_dist2(float4 p1, float4 q1, float4 p2, float4 q2) {
+    const float4 u = sub3(q1, p1), v = sub3(q2, p2), w = sub3(p1, p2);
+    const float a = d3(u, u), e = d3(v, v), f = d3(v, w);
+    float sp, tp;
+    const float tiny = 1e-30f;
+    if (a <= tiny && e <= tiny) {
+        sp = tp = 0.f;
+    } else if (a <= tiny) {
+        sp = 0.f;
+        tp = fminf(fmaxf(f / e, 0.f), 1.f);
+    } else {
+        const float c = d3(u, w);
+        if (e <= tiny) {
+            tp = 0.f;
+            sp = fminf(fmaxf(-c / a, 0.f), 1.f);
+        } else {
+            const float b = d3(u, v), den = a * e - b * b;
+            sp = den > 0.f ? fminf(fmaxf((b * f - c * e) / den, 0.f), 1.f) : 0.f;
+            tp = (b * sp + f) / e;
+            if (tp < 0.f) {
+                tp = 0.f;
+                sp = fminf(fmaxf(-c / a, 0.f), 1.f);
+            } else if (tp > 1.f) {
+                tp = 1.f;
+                sp = fminf(fmaxf((b - c) / a, 0.f), 1.f);
+            }
+        }
+    }
+    const float4 d = sub3(add3(p1, scale3(u, sp)), add3(p2, scale3(v, tp)));
+    return d3(d, d);
+}
+
+ADMM_DEV bool surely_apart(float d2, float thickness, float4 a, float4 b, float4 c, float4 d) {
+    const float r = fmaxf(fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(a.z), fabsf(b.x))),
+                          fmaxf(fmaxf(fabsf(b.y), fabsf(b.z)), fmaxf(fmaxf(fabsf(c.x), fabsf(c.y)),
+                                                                      fmaxf(fabsf(c.z), fmaxf(fmaxf(fabsf(d.x), fabsf(d.y)), fabsf(d.z))))));
+    const float lim = 1.1f * thickness + 1e-5f * r;
+    return d2 > lim * lim;  // false for NaN
+}
+
 // Narrow phase of vertex v against triangle f (region 0, 0 <= d < thickness).
 ADMM_DEV bool grid_hit_vf(const DevScene& s, int v, float4 P, int f, int4& ids, NpResult& r) {
     const int4 tri = s.st[f];
     if (v == tri.x || v == tri.y || v == tri.z) return false;
     ids = make_int4(v, tri.x, tri.y, tri.z);
-    return narrow_pt(P, s.x[tri.x], s.x[tri.y], s.x[tri.z], r) && r.dist < s.thickness && r.dist >= 0.f;
+    const float4 a = s.x[tri.x], b = s.x[tri.y], c = s.x[tri.z];
+    if (surely_apart(fast_pt_dist2(P, a, b, c), s.thickness, P, a, b, c)) return false;
+    return narrow_pt(P, a, b, c, r) && r.dist < s.thickness && r.dist >= 0.f;
 }
 
 // Narrow phase of edges e and o (no shared vertex), lower index first.
@@ -336,7 +426,9 @@ ADMM_DEV bool grid_hit_ee(const DevScene& s, int e, int o, int4& ids, NpResult& 
     if (ed.x == od.x || ed.x == od.y || ed.y == od.x || ed.y == od.y) return false;
     const int2 lo = o > e ? ed : od, hi = o > e ? od : ed;
     ids = make_int4(lo.x, lo.y, hi.x, hi.y);
-    return narrow_ee(s.x[lo.x], s.x[lo.y], s.x[hi.x], s.x[hi.y], r) && r.dist < s.thickness && r.dist >= 0.f;
+    const float4 p0 = s.x[lo.x], p1 = s.x[lo.y], q0 = s.x[hi.x], q1 = s.x[hi.y];
+    if (surely_apart(fast_ee_dist2(p0, p1, q0, q1), s.thickness, p0, p1, q0, q1)) return false;
+    return narrow_ee(p0, p1, q0, q1, r) && r.dist < s.thickness && r.dist >= 0.f;
 }
 
 // Count (WRITE = false: qcount) or write (WRITE = true: at qoff, then sorted by

@@ -57,7 +57,7 @@ struct GridDev {
     int* cnt = nullptr;            // [buckets] entries per bucket (zero between DCDs)
     int* start = nullptr;          // [buckets + 1] bucket offsets
     float4* ent_lo = nullptr;      // [cap] element box lo, w = element index (int bits)
-    float4* ent_up = nullptr;      // [cap] element box up, w = type (0 triangle, 1 edge)
+    float4* ent_up = nullptr;      // [cap] element box up, w = first-cell bits (x 1, y 2, z 4)
     unsigned long long* ent_key = nullptr;  // [cap] key of the cell the entry was made for
     int* ctr = nullptr;            // [4] entries reserved, big triangles, big edges
     int* big_tri = nullptr;        // [n surface triangles]
