@@ -53,6 +53,10 @@ CONFIGS = {
                   workload="cloth 32x32 (1024 verts, 1922 tris) over a unit box, 20 ADMM iters/step, dt=1/200"),
     "sheets": dict(fn="sheets_on_sphere", kw=dict(nx=512, layers=4, seed=0),
                    workload="4 x 512^2 cloth sheets on a sphere r=0.3, 40 ADMM iters/step, dt=1/300"),
+    "batch": dict(fn="batch_bodies", kw=dict(n_bodies=256, seed=0), per_rank_seed=True,
+                  workload="256 independent tet soft bodies (cubes and ellipsoids, 500-20000 verts log-uniform, "
+                           "E log-U[1e4,1e6], mu U(0.2,0.6) per body) dropped onto the ground, 30 ADMM iters/step, "
+                           "dt=1/100; each rank simulates its own batch (seed = rank)"),
     "sheets_small": dict(fn="sheets_on_sphere", kw=dict(nx=256, layers=2, seed=0),
                          workload="2 x 256^2 cloth sheets on a sphere r=0.3, 40 ADMM iters/step, dt=1/300 "
                                   "(profiling stand-in for the sheets workload)"),
@@ -68,11 +72,14 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def make_scene(args):
+def make_scene(args, rank=0):
     """The configured scene with the solver options of the command line applied."""
     from parallel_admm_b200 import scene
     c = CONFIGS[args.config]
-    sc = getattr(scene, c["fn"])(**c["kw"])
+    kw = dict(c["kw"])
+    if c.get("per_rank_seed"):
+        kw["seed"] = kw.get("seed", 0) + rank
+    sc = getattr(scene, c["fn"])(**kw)
     sc.params.jacobi_mode = args.jacobi_mode
     sc.params.ell_lanes = args.ell_lanes
     sc.params.global_solver = args.global_solver
@@ -283,7 +290,7 @@ def main():
     torch.cuda.set_device(local)
     from parallel_admm_b200 import backend as B
 
-    sc = make_scene(args)
+    sc = make_scene(args, rank)
     h = B.Handle(sc, device=local, residual_tol=args.tol)
     h.set_probe(args.probe)
     for _ in range(args.warmup):

@@ -123,6 +123,11 @@ typedef struct AdmmB200Desc {
      * max(1, jacobi_iter / 2): the same kernel count as the Jacobi sweeps. */
     int32_t global_solver;
     int32_t pcg_iter;
+    /* Optional [n_vert] friction coefficient per vertex (NULL: mu for all).  A
+     * contact uses the coefficient of its first vertex (in slot order) that is
+     * dynamic.  No reference counterpart (the reference has one mu per scene);
+     * used by batches of bodies with different materials. */
+    const float*   vert_mu;
 } AdmmB200Desc;
 
 /* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */

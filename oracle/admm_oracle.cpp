@@ -214,6 +214,8 @@ struct Oracle {
     std::vector<R> cw, cwinv;
     std::vector<char> is_surf;
     R dt, g, mu, kappa, beta;
+    std::vector<R> vmu;  // per-vertex friction (empty: mu everywhere)
+    std::vector<R> cmu;  // per contact: the coefficient of its first dynamic vertex
     float thickness;
     int admm_max_iter, dcd_interval, gs_max_iter, jacobi_iter;
     bool contact, ws_ue, ws_uc;
@@ -273,6 +275,7 @@ struct Oracle {
         is_surf.assign(n, 0);
         for (int s : surf_verts) is_surf[s] = 1;
         dt = d->dt; g = d->g; mu = d->mu; kappa = d->kappa; beta = d->beta; thickness = d->thickness;
+        if (d->vert_mu) vmu.assign(d->vert_mu, d->vert_mu + d->n_vert);
         admm_max_iter = d->admm_max_iter; dcd_interval = std::max(1, d->dcd_interval);
         gs_max_iter = d->gs_max_iter; jacobi_iter = d->jacobi_iter;
         contact = d->enable_contact != 0; ws_ue = d->warmstart_ue != 0; ws_uc = d->warmstart_uc != 0;
@@ -518,6 +521,13 @@ struct Oracle {
     // gs_max_iter x {friction-cone projection per contact, gather into p}.
     void project() {
         int nc = (int)cts.size();
+        cmu.assign(nc, mu);
+        if (!vmu.empty())
+            for (int c = 0; c < nc; c++) {
+                int k = 0;
+                while (k < 3 && cts[c].v[k] >= nd) k++;
+                cmu[c] = vmu[cts[c].v[k]];
+            }
         for (int c = 0; c < nc; c++)
             for (int k = 0; k < 4; k++) {
                 int vi = cts[c].v[k];
@@ -538,7 +548,7 @@ struct Oracle {
                 for (int a = 0; a < 3; a++) uT[a] = us[a] - uN * nrm[a];
                 if (uN < 0) {
                     R tau = std::sqrt((uT[0] * uT[0] + uT[1] * uT[1]) + uT[2] * uT[2]);
-                    R alpha = -mu * uN;
+                    R alpha = -cmu[c] * uN;
                     uN = 0;
                     if (tau <= alpha) uT[0] = uT[1] = uT[2] = 0;
                     else { R s = R(1) - alpha / tau; for (int a = 0; a < 3; a++) uT[a] = s * uT[a]; }

@@ -73,6 +73,7 @@ class AdmmB200Desc(ctypes.Structure):
         ("residual_tol", ctypes.c_float), ("residual_check_every", ctypes.c_int32),
         ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32), ("jacobi_mode", ctypes.c_int32),
         ("broad_phase", ctypes.c_int32), ("global_solver", ctypes.c_int32), ("pcg_iter", ctypes.c_int32),
+        ("vert_mu", ctypes.POINTER(ctypes.c_float)),
     ]
 
 
@@ -139,6 +140,8 @@ class DescHolder:
         d.broad_phase = int(p.broad_phase)
         d.global_solver = int(p.global_solver)
         d.pcg_iter = int(p.pcg_iter)
+        vm = getattr(sc, "vert_mu", None)
+        d.vert_mu = arr("vm", vm, np.float32) if vm is not None else None
         for k, v in overrides.items():
             setattr(d, k, v)
         self.desc = d

@@ -1121,6 +1121,14 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.gamma, s.cap));
     TRY(dalloc(h, &s.kc, s.cap));
     TRY(dalloc(h, &s.rc, s.cap));
+    TRY(dalloc(h, &s.cmu, s.cap));
+    if (d->vert_mu) {
+        for (int i = 0; i < n; i++)
+            if (!(d->vert_mu[i] >= 0.f)) return fail(h, ADMM_ERR_INVALID, "vert_mu must be >= 0");
+        float* vm;
+        TRY(dupload(h, &vm, d->vert_mu, n));
+        s.vmu = vm;
+    }
     TRY(dalloc(h, &s.ginc, 4 * (size_t)s.cap));
     TRY(dalloc(h, &s.vtmp, 4 * (size_t)s.cap));
     TRY(dalloc(h, &s.du, s.cap));

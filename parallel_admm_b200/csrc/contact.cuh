@@ -108,6 +108,9 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_scc(DevScene s) {
         s.kc[c] = f4(k * nr.x * s.gam, k * nr.y * s.gam, k * nr.z * s.gam);
         s.rc[c] = f4(0.f, 0.f, 0.f);
         s.du[c] = f4(0.f, 0.f, 0.f);
+        float mu = s.mu;
+        if (s.vmu) mu = s.vmu[q.x < s.nd ? q.x : q.y < s.nd ? q.y : q.z < s.nd ? q.z : q.w];
+        s.cmu[c] = mu;
     }
 }
 
@@ -157,7 +160,7 @@ ADMM_DEV float4 friction_cone_du(const DevScene& s, int c, float ux, float uy, f
     float tx = sx - uN * n.x, ty = sy - uN * n.y, tz = sz - uN * n.z;
     if (uN < 0.f) {
         const float tau = sqrtf(tx * tx + ty * ty + tz * tz);
-        const float alpha = -s.mu * uN;
+        const float alpha = -s.cmu[c] * uN;
         uN = 0.f;
         if (tau <= alpha) {
             tx = ty = tz = 0.f;

@@ -113,6 +113,8 @@ struct DevScene {
     float4* gamma = nullptr;              // Gamma_c per contact slot
     float4* kc = nullptr;
     float4* rc = nullptr;
+    float* cmu = nullptr;                 // [cap] friction coefficient per contact
+    const float* vmu = nullptr;           // [n] per-vertex coefficient, or null
     float4* du = nullptr;
     int* vcnt = nullptr;                  // [n] contacts per vertex
     int* vfill = nullptr;                 // [n]

@@ -97,6 +97,7 @@ class Scene:
     contact_w: np.ndarray        # (n,) float32
     params: SolverParams
     meta: Dict[str, object] = dataclasses.field(default_factory=dict)
+    vert_mu: Optional[np.ndarray] = None  # (n,) float32 per-vertex friction, or None (params.mu)
 
     # --- row bookkeeping (mesh_to_constraint.h order) ---
     @property
@@ -385,6 +386,34 @@ def tet_cube(n: int, side: float) -> Tuple[np.ndarray, np.ndarray]:
     return verts, tets
 
 
+def tet_lattice(dims: Tuple[int, int, int], cell: float, keep=None) -> Tuple[np.ndarray, np.ndarray]:
+    """Lattice of dims cells (edge `cell`), 5 tets per kept cell with alternating orientation
+    (conforming), unused lattice vertices removed.  keep(centres) -> bool mask of cells."""
+    nx, ny, nz = dims
+    gx, gy, gz = [np.arange(d + 1) * cell for d in dims]
+    xx, yy, zz = np.meshgrid(gx, gy, gz, indexing="ij")
+    verts = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], 1)
+    idx = np.arange((nx + 1) * (ny + 1) * (nz + 1)).reshape(nx + 1, ny + 1, nz + 1)
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
+    if keep is not None:
+        m = keep(np.stack([(ii + 0.5) * cell, (jj + 0.5) * cell, (kk + 0.5) * cell], 1))
+        ii, jj, kk = ii[m], jj[m], kk[m]
+    corner = np.stack([idx[ii + a, jj + b, kk + c] for a in (0, 1) for b in (0, 1) for c in (0, 1)], 1)
+    even = ((ii + jj + kk) % 2 == 0)
+    pat_e = np.array([(0, 4, 2, 1), (6, 2, 4, 7), (5, 1, 7, 4), (3, 7, 1, 2), (1, 2, 4, 7)])
+    pat_o = np.array([(4, 0, 6, 5), (2, 6, 0, 3), (1, 5, 3, 0), (7, 3, 5, 6), (0, 3, 5, 6)])
+    tets = np.concatenate([corner[even][:, pat_e].reshape(-1, 4), corner[~even][:, pat_o].reshape(-1, 4)])
+    used, inv = np.unique(tets.ravel(), return_inverse=True)
+    tets = inv.reshape(-1, 4).astype(np.int32)
+    verts = verts[used]
+    d = np.stack([verts[tets[:, 1]] - verts[tets[:, 0]], verts[tets[:, 2]] - verts[tets[:, 0]],
+                  verts[tets[:, 3]] - verts[tets[:, 0]]], 2)
+    neg = np.linalg.det(d) < 0
+    tets[neg] = tets[neg][:, [0, 2, 1, 3]]
+    return verts, tets
+
+
 def _rot_y(theta: float) -> np.ndarray:
     c, s = math.cos(theta), math.sin(theta)
     return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
@@ -412,6 +441,7 @@ class _Body:
     k_stretch: float
     k_bend: float = 0.0
     static: bool = False
+    mu: Optional[float] = None    # friction of this body's vertices (None: the scene's mu)
 
 
 def assemble(name: str, bodies: List[_Body], pins: List[int], params: SolverParams,
@@ -494,13 +524,17 @@ def assemble(name: str, bodies: List[_Body], pins: List[int], params: SolverPara
     SV = np.unique(ST.ravel()).astype(np.int32)
     cw = np.full(n, 1e12, np.float64)
     cw[:n_dyn] = mass[:n_dyn] / (params.dt * params.dt) * params.w_scale
+    vert_mu = None
+    if any(b.mu is not None for b in bodies):
+        vert_mu = np.concatenate([np.full(len(b.verts), params.mu if b.mu is None else b.mu)
+                                  for b in dyn + sta]).astype(np.float32)
     sc = Scene(name=name, verts=V32, n_dyn=n_dyn, mass=mass.astype(np.float32), is_fixed=is_fixed,
                tri_inds=TF.astype(np.int32), tri_binv=tri_binv, tri_w=tri_w,
                tet_inds=TT.astype(np.int32), tet_binv=tet_binv, tet_w=tet_w,
                bend_offsets=bend_offsets, bend_inds=bend_inds, bend_coeffs=bend_coeffs, bend_w=bend_w,
                pin_inds=pin_inds, pin_pos=pin_pos.astype(np.float32), pin_w=pin_w,
                surf_tris=ST, surf_edges=SE, surf_verts=SV, contact_w=cw.astype(np.float32),
-               params=params, meta=dict(meta or {}))
+               params=params, meta=dict(meta or {}), vert_mu=vert_mu)
     return sc
 
 
@@ -576,8 +610,63 @@ def sheets_on_sphere(nx: int = 512, layers: int = 4, seed: int = 0, side: float 
                     meta={"config": "sheets on sphere", "seed": seed, "nx": nx, "layers": layers})
 
 
+def batch_bodies(n_bodies: int = 256, seed: int = 0, vmin: int = 500, vmax: int = 20000) -> Scene:
+    """`n_bodies` independent tet soft bodies of uneven size: cubes and voxelised ellipsoids with
+    log-uniform vertex counts in [vmin, vmax], E log-uniform in [1e4, 1e6], friction U(0.2, 0.6)
+    per body, each dropped 0.1-0.5 m onto the ground.  The bodies sit on a square layout with
+    gaps wider than any body, over one ground quad (for bodies that never meet, the same as a
+    ground each); h = 1/100, 30 ADMM iterations.  The engine treats the batch as one scene:
+    one block-diagonal segmented matrix, one collision grid.
+    """
+    rng = np.random.default_rng(seed)
+    cell = 0.02
+    bodies = []
+    nside = int(math.ceil(math.sqrt(n_bodies)))
+    pitch = 0.0
+    specs = []
+    for b in range(n_bodies):
+        target = math.exp(rng.uniform(math.log(vmin), math.log(vmax)))
+        ellipsoid = bool(rng.random() < 0.5)
+        if ellipsoid:
+            r = rng.uniform(0.6, 1.4, size=3)
+            r = r / np.cbrt(r.prod())
+            # voxelised ellipsoid keeps ~pi/6 of the box's cells
+            n = max(3, int(round((target / (math.pi / 6 * r.prod())) ** (1 / 3))) - 1)
+            dims = tuple(max(2, int(round(n * ri))) for ri in r)
+        else:
+            n = max(2, int(round(target ** (1 / 3))) - 1)
+            dims = (n, n, n)
+        specs.append((ellipsoid, dims))
+        pitch = max(pitch, max(dims) * cell)
+    pitch = pitch * 1.5 + 0.1
+    for b, (ellipsoid, dims) in enumerate(specs):
+        if ellipsoid:
+            half = np.array(dims) * cell / 2
+
+            def keep(c, half=half):
+                q = (c - half) / half
+                return (q * q).sum(1) <= 1.0
+            v, t = tet_lattice(dims, cell, keep)
+        else:
+            v, t = tet_lattice(dims, cell)
+        v = v - v.mean(0)
+        v = v @ _rand_rot(rng).T
+        gx, gz = (b % nside - (nside - 1) / 2) * pitch, (b // nside - (nside - 1) / 2) * pitch
+        v = v + np.array([gx, -v[:, 1].min() + rng.uniform(0.1, 0.5), gz])
+        E = float(10 ** rng.uniform(4, 6))
+        bodies.append(_Body(v, np.zeros((0, 3), np.int32), t, 1000.0, E / (1 + 0.4),
+                            mu=float(rng.uniform(0.2, 0.6))))
+    gv, gf = ground_quad(nside * pitch / 2 + 1.0, 0.0)
+    bodies.append(_Body(gv, gf, np.zeros((0, 4), np.int32), 1e12, 0.0, static=True))
+    params = SolverParams(dt=1.0 / 100, g=9.8, mu=0.4, thickness=0.6 * cell, admm_max_iter=30,
+                          dcd_interval=5, gs_max_iter=10, jacobi_iter=20, max_contacts=2_000_000)
+    return assemble(f"batch{n_bodies}", bodies, [], params,
+                    meta={"config": "batched soft bodies", "seed": seed, "bodies": n_bodies})
+
+
 CONFIGS = {
     "cloth": cloth_on_box,
     "cube": cube_on_ground,
     "sheets": sheets_on_sphere,
+    "batch": batch_bodies,
 }
