@@ -258,8 +258,8 @@ def main():
     ap.add_argument("--ell-lanes", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="pin the lanes per row of both sliced-ELL matrices (0 = autotuned; pin it under a profiler, "
                          "whose serialised launches mislead the autotuner)")
-    ap.add_argument("--jacobi-mode", type=int, default=0, choices=[0, 1, 2],
-                    help="global step: 0 autotuned, 1 one kernel per sweep, 2 persistent kernel")
+    ap.add_argument("--jacobi-mode", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="global step: 0 autotuned, 1 one kernel per sweep, 2 persistent kernel, 3 two sweeps per launch")
     ap.add_argument("--global-solver", type=int, default=0, choices=[0, 1, 2],
                     help="global step: 0 Jacobi sweeps (the reference's), 1 PCG with diag(A), 2 PCG with blocks")
     ap.add_argument("--pcg-iter", type=int, default=0, help="PCG iterations per global step (0 = jacobi_iter / 2)")

@@ -110,7 +110,9 @@ typedef struct AdmmB200Desc {
      * kernel for the right-hand side and one per Jacobi sweep; 2 = one persistent
      * kernel for the right-hand side and all sweeps, its blocks synchronised
      * through per-block sweep counters (falls back to 1 when the device cannot
-     * hold all blocks at once or jacobi_iter < 2).  Both give identical bits. */
+     * hold all blocks at once or jacobi_iter < 2); 3 = two sweeps per launch,
+     * one block per spatially compact tile of rows, the halo rows computed
+     * into shared memory.  All give identical bits. */
     int32_t jacobi_mode;
     /* Broad phase of the DCD: 0 = default (2); 1 = LBVH (the reference's
      * structure, bvh_refit applies); 2 = uniform-grid spatial hash.  Both report
@@ -292,8 +294,9 @@ int  admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, floa
  * No reference counterpart. */
 int  admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd);
 /* How the global step runs (jacobi_mode): persistent = 1 for the one-kernel
- * global step (blocks = its grid), 0 for one kernel per sweep; the autotuner's
- * ms per global step in both modes (0 when not timed). */
+ * global step (blocks = its grid), 3 for two sweeps per launch over row tiles,
+ * 0 for one kernel per sweep; the autotuner's ms per global step with one
+ * kernel per sweep and with the persistent kernel (0 when not timed). */
 int  admm_b200_global_mode(AdmmB200* h, int* persistent, int* blocks, float* ms_sweeps, float* ms_persist);
 
 /* --- allocation-free Jacobi solve (no counterpart in the reference) ---

@@ -400,7 +400,8 @@ class Handle:
         ms, mp = ctypes.c_float(), ctypes.c_float()
         self.check(lib().admm_b200_global_mode(self.h, ctypes.byref(pe), ctypes.byref(nb), ctypes.byref(ms),
                                                ctypes.byref(mp)), "global_mode")
-        return {"persistent": bool(pe.value), "blocks": nb.value, "ms_sweeps": ms.value, "ms_persist": mp.value}
+        return {"mode": {0: "sweeps", 1: "persistent", 3: "tiled"}.get(pe.value, "?"), "persistent": pe.value == 1,
+                "blocks": nb.value, "ms_sweeps": ms.value, "ms_persist": mp.value}
 
     def max_slots(self) -> int:
         n = ctypes.c_int32()

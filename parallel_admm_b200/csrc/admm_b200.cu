@@ -77,7 +77,11 @@ struct AdmmB200 {
     // global step: persistent kernel (RHS + all sweeps) or one kernel per sweep
     PersistPlan pp;
     bool persist_ok = false;        // plan built and all blocks fit on the device at once
-    bool persist = false;           // chosen mode
+    bool persist = false;           // chosen mode: persistent global step
+    bool tiled = false;             // chosen mode: two sweeps per launch over row tiles
+    TileSet ts;
+    int tile_smem = 0;
+    float tune_ms_tiled = 0.f;
     float tune_ms_persist = 0.f, tune_ms_sweeps = 0.f;  // one global step, both modes
     // host-buffer stepping
     float* stage = nullptr;    // [6n] row-major x then v
@@ -245,6 +249,12 @@ void set_phase(AdmmB200* h, int ph) {
         h->launch_counter++;                                                         \
     } while (0)
 #define LAUNCH(kernel, grid, block, ...) LAUNCH_P(0, kernel, grid, block, __VA_ARGS__)
+#define LAUNCH_SMEM(pid, kernel, grid, block, smem, ...)                                  \
+    do {                                                                                 \
+        LaunchTimer lt_(h, (pid));                                                       \
+        launch_k(kernel, dim3(grid), dim3(block), smem, h->cstream, h->pdl, __VA_ARGS__); \
+        h->launch_counter++;                                                             \
+    } while (0)
 
 void enqueue_refit(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tri) {
     const int n = t.n;
@@ -375,6 +385,17 @@ void launch_jacobi(AdmmB200* h, const float4* src, float4* dst) {
     }
 }
 
+void launch_jacobi2(AdmmB200* h, const float4* src, float4* dst) {
+    DevScene& s = h->s;
+    const size_t sm = (size_t)h->tile_smem;
+    switch (s.A.lanes) {
+        case 1: LAUNCH_SMEM(ADMM_KERNEL_JACOBI, k_jacobi2<1>, h->ts.ntiles, kTileThreads, sm, s, h->ts, src, dst); break;
+        case 2: LAUNCH_SMEM(ADMM_KERNEL_JACOBI, k_jacobi2<2>, h->ts.ntiles, kTileThreads, sm, s, h->ts, src, dst); break;
+        case 4: LAUNCH_SMEM(ADMM_KERNEL_JACOBI, k_jacobi2<4>, h->ts.ntiles, kTileThreads, sm, s, h->ts, src, dst); break;
+        default: LAUNCH_SMEM(ADMM_KERNEL_JACOBI, k_jacobi2<8>, h->ts.ntiles, kTileThreads, sm, s, h->ts, src, dst); break;
+    }
+}
+
 void launch_rhs(AdmmB200* h, bool save_prev) {
     DevScene& s = h->s;
     const int g = blocks(s.R.nslices * 32, kVertThreads);
@@ -440,6 +461,20 @@ void enqueue_jacobi(AdmmB200* h, int sweeps) {
     if (sweeps == 1) {
         launch_jacobi(h, s.x, s.jac[0]);
         LAUNCH(k_copy_dyn, vb, kVertThreads, s, s.jac[0], s.x);
+        return;
+    }
+    if (h->tiled) {
+        // pairs of sweeps x -> jac0 -> jac1 -> ...; the last pair writes x when its
+        // source is not x, an odd sweep count ends with one plain sweep into x
+        const int pairs = sweeps / 2, odd = sweeps & 1;
+        const float4* src = s.x;
+        for (int p = 0; p < pairs; p++) {
+            float4* dst = (p == pairs - 1 && !odd && src != s.x) ? s.x : s.jac[p & 1];
+            launch_jacobi2(h, src, dst);
+            src = dst;
+        }
+        if (odd) launch_jacobi(h, src, s.x);
+        else if (src != s.x) LAUNCH(k_copy_dyn, vb, kVertThreads, s, src, s.x);
         return;
     }
     for (int k = 0; k < sweeps; k++) {
@@ -545,10 +580,61 @@ int build_persist_plan(AdmmB200* h, const HostCsr& A) {
     return ADMM_OK;
 }
 
+// Row tiles of the two-sweep kernel for the lanes A was tuned to, uploaded.
+int upload_host_ell(AdmmB200* h, const HostEll& e, SlicedEll& out) {
+    int *p = nullptr, *c = nullptr;
+    float* v = nullptr;
+    TRY(dupload(h, &p, e.ptr.data(), e.ptr.size()));
+    TRY(dupload(h, &c, e.col.data(), e.col.size()));
+    TRY(dupload(h, &v, e.val.data(), e.val.size()));
+    out.rows = e.rows;
+    out.nslices = e.nslices;
+    out.lanes = e.lanes;
+    out.ptr = p;
+    out.col = c;
+    out.val = v;
+    return ADMM_OK;
+}
+
+int build_tiles_dev(AdmmB200* h, const HostCsr& A) {
+    DevScene& s = h->s;
+    if (s.nd <= 0) return ADMM_OK;
+    std::vector<float> pos(3 * (size_t)s.nd);
+    for (int i = 0; i < s.nd; i++) {
+        pos[3 * i] = h->x_init[i].x;
+        pos[3 * i + 1] = h->x_init[i].y;
+        pos[3 * i + 2] = h->x_init[i].z;
+    }
+    const HostTiles t = build_tiles(A, s.nd, pos.data(), 3, kTileOwn, s.A.lanes);
+    TileSet& d = h->ts;
+    d.ntiles = t.ntiles;
+    int* a;
+    TRY(dupload(h, &a, t.row0.data(), t.row0.size())); d.row0 = a;
+    TRY(dupload(h, &a, t.nlocal.data(), t.nlocal.size())); d.nlocal = a;
+    TRY(dupload(h, &a, t.nown.data(), t.nown.size())); d.nown = a;
+    TRY(dupload(h, &a, t.s1_0.data(), t.s1_0.size())); d.s1_0 = a;
+    TRY(dupload(h, &a, t.s1_n.data(), t.s1_n.size())); d.s1_n = a;
+    TRY(dupload(h, &a, t.s2_0.data(), t.s2_0.size())); d.s2_0 = a;
+    TRY(dupload(h, &a, t.s2_n.data(), t.s2_n.size())); d.s2_n = a;
+    TRY(dupload(h, &a, t.trow.data(), t.trow.size())); d.trow = a;
+    TRY(upload_host_ell(h, t.e1, d.e1));
+    TRY(upload_host_ell(h, t.e2, d.e2));
+    h->tile_smem = (int)(sizeof(float4) * (size_t)std::max(t.max_local, 1));
+    if (h->tile_smem > 48 * 1024) {
+        const int lim = h->tile_smem;
+        CK(cudaFuncSetAttribute(k_jacobi2<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_jacobi2<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_jacobi2<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+        CK(cudaFuncSetAttribute(k_jacobi2<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    }
+    return ADMM_OK;
+}
+
 // Milliseconds of one global step (RHS + jac_iter sweeps), eager, in either mode.
-int time_global(AdmmB200* h, bool persist, float* ms) {
-    const bool keep = h->persist;
-    h->persist = persist;
+int time_global(AdmmB200* h, int mode, float* ms) {
+    const bool keep = h->persist, keep_t = h->tiled;
+    h->persist = mode == 2;
+    h->tiled = mode == 3;
     h->cstream = h->stream;
     enqueue_global(h, false);
     CK(cudaEventRecord(h->ev0, h->stream));
@@ -557,6 +643,7 @@ int time_global(AdmmB200* h, bool persist, float* ms) {
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
     h->persist = keep;
+    h->tiled = keep_t;
     CK(cudaGetLastError());
     int e[4] = {0, 0, 0, 0};
     CK(cudaMemcpy(e, h->s.err, sizeof(e), cudaMemcpyDeviceToHost));
@@ -667,10 +754,10 @@ int autotune_ell(AdmmB200* h, const Assembly& as, int fixed, int* chosen_a, int*
 void enqueue_residual(AdmmB200* h) {
     DevScene& s = h->s;
     set_phase(h, ADMM_PHASE_RESIDUAL);
-    cudaMemsetAsync(s.res, 0, sizeof(double) * 4, h->cstream);
     const int vb = blocks(s.nd, kLocalThreads);
     const int g = h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks + vb;
     LAUNCH(k_residual, g, kLocalThreads, s, h->tet_blocks, h->tri_blocks, h->bend_blocks, h->pin_blocks);
+    LAUNCH(k_residual_reduce, 1, 256, s, g);
 }
 
 // One ADMM iteration `it` of a substep (first: no dual update before it).  The
@@ -1164,6 +1251,8 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     h->bend_blocks = s.nbend ? blocks(s.nbend, kLocalThreads) : 0;
     h->pin_blocks = s.npin ? blocks(s.npin, kLocalThreads) : 0;
     if (h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks == 0) return fail(h, ADMM_ERR_INVALID, "no constraints");
+    TRY(dalloc(h, &s.res_part, 3 * (size_t)(h->tet_blocks + h->tri_blocks + h->bend_blocks + h->pin_blocks +
+                                            blocks(s.nd, kLocalThreads))));
 
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking));
@@ -1181,7 +1270,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     if (d->ell_lanes != 0 && d->ell_lanes != 1 && d->ell_lanes != 2 && d->ell_lanes != 4 && d->ell_lanes != 8)
         return fail(h, ADMM_ERR_INVALID, "ell_lanes must be 0, 1, 2, 4 or 8");
     TRY(autotune_ell(h, as, d->ell_lanes, &h->tune_lanes_a, &h->tune_lanes_r, &h->tune_ms_a, &h->tune_ms_r));
-    if (d->jacobi_mode < 0 || d->jacobi_mode > 2) return fail(h, ADMM_ERR_INVALID, "jacobi_mode must be 0, 1 or 2");
+    if (d->jacobi_mode < 0 || d->jacobi_mode > 3) return fail(h, ADMM_ERR_INVALID, "jacobi_mode must be 0, 1, 2 or 3");
     if (d->global_solver < 0 || d->global_solver > 2) return fail(h, ADMM_ERR_INVALID, "global_solver must be 0, 1 or 2");
     if (d->pcg_iter < 0) return fail(h, ADMM_ERR_INVALID, "pcg_iter");
     h->global_solver = d->global_solver;
@@ -1198,14 +1287,26 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         TRY(dalloc(h, &g.scal, 8));
     }
     TRY(build_persist_plan(h, as.A));
-    h->persist = false;
-    if (h->persist_ok && h->jac_iter >= 2 && d->jacobi_mode != 1) {
-        if (d->jacobi_mode == 2) {
+    TRY(build_tiles_dev(h, as.A));
+    h->persist = h->tiled = false;
+    if (h->jac_iter >= 2 && d->global_solver == 0) {
+        if (d->jacobi_mode == 2 && h->persist_ok) {
             h->persist = true;
-        } else {
-            TRY(time_global(h, false, &h->tune_ms_sweeps));
-            TRY(time_global(h, true, &h->tune_ms_persist));
-            h->persist = h->tune_ms_persist < h->tune_ms_sweeps;
+        } else if (d->jacobi_mode == 3) {
+            h->tiled = true;
+        } else if (d->jacobi_mode == 0) {
+            TRY(time_global(h, 1, &h->tune_ms_sweeps));
+            TRY(time_global(h, 3, &h->tune_ms_tiled));
+            if (h->persist_ok) TRY(time_global(h, 2, &h->tune_ms_persist));
+            float best = h->tune_ms_sweeps;
+            if (h->tune_ms_tiled < best) {
+                best = h->tune_ms_tiled;
+                h->tiled = true;
+            }
+            if (h->persist_ok && h->tune_ms_persist < best) {
+                h->tiled = false;
+                h->persist = true;
+            }
         }
     }
     TRY(upload_state(h, h->x_init, h->v_init));
@@ -1718,7 +1819,7 @@ int admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd) {
 
 int admm_b200_global_mode(AdmmB200* h, int* persistent, int* blocks, float* ms_sweeps, float* ms_persist) {
     if (!h) return ADMM_ERR_INVALID;
-    if (persistent) *persistent = h->persist ? 1 : 0;
+    if (persistent) *persistent = h->persist ? 1 : h->tiled ? 3 : 0;
     if (blocks) *blocks = h->persist ? h->pp.blocks : 0;
     if (ms_sweeps) *ms_sweeps = h->tune_ms_sweeps;
     if (ms_persist) *ms_persist = h->tune_ms_persist;

@@ -321,6 +321,49 @@ __global__ void __launch_bounds__(kVertThreads) k_jacobi(DevScene s, const float
 }
 
 // ---------------------------------------------------------------------------
+// Two Jacobi sweeps in one launch (jacobi_mode 3).  One block per row tile:
+// phase 1 computes the first sweep for the tile's own and halo rows from the
+// global src into shared memory, phase 2 the second sweep for the own rows
+// from shared memory into dst.  Every row is summed with the same entries in
+// the same order and lane layout as k_jacobi, so two launches of k_jacobi and
+// one of k_jacobi2 give identical bits; the halo rows are computed twice (by
+// their own tile and by their neighbours'), the price of half the launches.
+// ---------------------------------------------------------------------------
+constexpr int kTileThreads = 1024;
+constexpr int kTileOwn = 64;
+
+template <int T>
+__global__ void __launch_bounds__(kTileThreads) k_jacobi2(DevScene s, TileSet ts, const float4* __restrict__ src,
+                                                          float4* __restrict__ dst) {
+    ADMM_PDL_PROLOGUE();
+    extern __shared__ float4 ysh[];
+    constexpr int S = 32 / T;
+    const int t = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int r0 = ts.row0[t], n1 = ts.nlocal[t], no = ts.nown[t];
+    const int a1 = ts.s1_0[t], b1 = a1 + ts.s1_n[t];
+    for (int w = a1 + warp; w < b1; w += nw) {
+        int lr;
+        const float4 acc = ell_row_sum<T>(ts.e1, src, w, lane, lr);
+        const int li = lr - a1 * S;
+        if (lane < S && li < n1) {
+            const int g = ts.trow[r0 + li];
+            const float4 bi = s.b[g];
+            const float d = s.a_diag[g];
+            ysh[li] = f4((bi.x - acc.x) / d, (bi.y - acc.y) / d, (bi.z - acc.z) / d);
+        }
+    }
+    __syncthreads();
+    const int a2 = ts.s2_0[t], b2 = a2 + ts.s2_n[t];
+    for (int w = a2 + warp; w < b2; w += nw) {
+        int lr;
+        const float4 acc = ell_row_sum<T>(ts.e2, ysh, w, lane, lr);
+        const int li = lr - a2 * S;
+        if (lane < S && li < no) jacobi_row(s, ts.trow[r0 + li], acc, dst);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // The whole global step in one persistent kernel: the right-hand side (RHS)
 // and `sweeps` Jacobi sweeps, bit-identical to k_rhs + k_jacobi launches.
 //
@@ -660,10 +703,24 @@ __global__ void __launch_bounds__(kLocalThreads) k_residual(DevScene s, int tet_
     pr = block_sum(pr, sh);
     du = block_sum(du, sh);
     sc = block_sum(sc, sh);
-    if (threadIdx.x == 0) {
-        atomicAdd(&s.res[0], pr);
-        atomicAdd(&s.res[1], du);
-        atomicAdd(&s.res[2], sc);
+    if (threadIdx.x == 0) {  // per-block partials, summed in a fixed order by k_residual_reduce
+        s.res_part[3 * blockIdx.x] = pr;
+        s.res_part[3 * blockIdx.x + 1] = du;
+        s.res_part[3 * blockIdx.x + 2] = sc;
+    }
+}
+
+// res[0..2] = the sums of the n block partials of k_residual, in a fixed order
+// (run to run identical residuals, hence identical convergence decisions).
+__global__ void __launch_bounds__(256) k_residual_reduce(DevScene s, int n) {
+    ADMM_PDL_PROLOGUE();
+    __shared__ double sh[8];
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < n; b += blockDim.x)
+        for (int k = 0; k < 3; k++) v[k] += s.res_part[3 * b + k];
+    for (int k = 0; k < 3; k++) {
+        const double t = block_sum(v[k], sh);
+        if (threadIdx.x == 0) s.res[k] = t;
     }
 }
 

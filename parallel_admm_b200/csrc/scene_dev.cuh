@@ -39,6 +39,15 @@ struct BvhDev {
     float4* node4 = nullptr;     // [4(n-1)]
 };
 
+// Row tiles of the two-sweep Jacobi kernel (see build_tiles in setup.hpp).
+struct TileSet {
+    int ntiles = 0;
+    const int *row0 = nullptr, *nlocal = nullptr, *nown = nullptr;
+    const int *s1_0 = nullptr, *s1_n = nullptr, *s2_0 = nullptr, *s2_n = nullptr;
+    const int* trow = nullptr;   // local row -> global row (-1 = padding)
+    SlicedEll e1, e2;            // phase 1 (global columns), phase 2 (tile-local columns)
+};
+
 // Work split and dependency lists of the persistent global-step kernel.
 struct PersistPlan {
     int blocks = 0;                // one per SM at most (cooperative launch)
@@ -137,6 +146,7 @@ struct DevScene {
     int* scan_tmp = nullptr;              // block sums for scans
     // residuals: [0] primal^2, [1] dual^2, [2] scale^2
     double* res = nullptr;
+    double* res_part = nullptr;           // [3 x residual blocks] per-block partial sums
     int* done = nullptr;
 };
 

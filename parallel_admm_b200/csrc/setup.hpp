@@ -68,6 +68,142 @@ inline HostEll csr_to_sliced_ell(const HostCsr& c, int rows, int T) {
     return e;
 }
 
+// ---------------------------------------------------------------------------
+// Row tiles for the two-sweep Jacobi kernel: spatially compact groups of own
+// rows (consecutive in the Morton order of the rest positions) and their halo
+// (the other rows their off-diagonal entries reach).  Phase 1 of a launch
+// computes one sweep for own + halo rows from global x into shared memory,
+// phase 2 the next sweep for the own rows from shared memory.  Each tile's rows
+// are padded to whole ELL slices so that no slice straddles two tiles.
+// ---------------------------------------------------------------------------
+struct HostTiles {
+    int lanes = 1, ntiles = 0, max_local = 0;
+    std::vector<int> row0, nlocal, nown, s1_0, s1_n, s2_0, s2_n;  // per tile
+    std::vector<int> trow;                                        // local row -> global row (-1 = padding)
+    HostEll e1, e2;                                               // phase 1 (global cols), phase 2 (local cols)
+};
+
+// Sliced ELL of explicit rows: rows[k] = (columns, values); padding column pad[k].
+inline HostEll rows_to_sliced_ell(const std::vector<std::vector<int>>& cols, const std::vector<std::vector<double>>& vals,
+                                  const std::vector<int>& pad, int T) {
+    HostCsr c;
+    const int rows = (int)cols.size();
+    c.start.assign(rows + 1, 0);
+    for (int r = 0; r < rows; r++) {
+        c.start[r + 1] = c.start[r] + (int)cols[r].size();
+        c.col.insert(c.col.end(), cols[r].begin(), cols[r].end());
+        c.val.insert(c.val.end(), vals[r].begin(), vals[r].end());
+    }
+    HostEll e = csr_to_sliced_ell(c, rows, T);
+    const int S = 32 / T;
+    for (int sl = 0; sl < e.nslices; sl++) {  // padding entries: the row's own (valid) column
+        const int w = (e.ptr[sl + 1] - e.ptr[sl]) / S;
+        for (int lr = 0; lr < S; lr++) {
+            const int r = sl * S + lr;
+            const int len = r < rows ? (int)cols[r].size() : 0;
+            for (int k = len; k < w; k++) e.col[e.ptr[sl] + (k / T) * 32 + (k % T) * S + lr] = r < rows ? pad[r] : pad[0];
+        }
+    }
+    return e;
+}
+
+inline uint32_t spread10_host(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// Tiles of `own` rows of the nd x nd off-diagonal CSR A (columns sorted), in the
+// Morton order of the positions pos (xyz per row).
+inline HostTiles build_tiles(const HostCsr& A, int nd, const float* pos, int pos_stride, int own, int T) {
+    HostTiles t;
+    t.lanes = T;
+    const int S = 32 / T;
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    for (int i = 0; i < nd; i++)
+        for (int k = 0; k < 3; k++) {
+            lo[k] = std::min(lo[k], pos[pos_stride * i + k]);
+            hi[k] = std::max(hi[k], pos[pos_stride * i + k]);
+        }
+    std::vector<std::pair<uint32_t, int>> key(nd);
+    for (int i = 0; i < nd; i++) {
+        uint32_t q[3];
+        for (int k = 0; k < 3; k++) {
+            const float ext = hi[k] - lo[k];
+            const float u = ext > 0.f ? (pos[pos_stride * i + k] - lo[k]) / ext : 0.f;
+            q[k] = (uint32_t)std::min(1023.f, std::max(0.f, u * 1023.f));
+        }
+        key[i] = {spread10_host(q[0]) | (spread10_host(q[1]) << 1) | (spread10_host(q[2]) << 2), i};
+    }
+    std::stable_sort(key.begin(), key.end());
+    std::vector<int> local_of(nd, -1);
+    std::vector<std::vector<int>> c1, c2;
+    std::vector<std::vector<double>> v1, v2;
+    std::vector<int> pad1, pad2;
+    for (int b = 0; b < nd; b += own) {
+        const int e = std::min(nd, b + own);
+        std::vector<int> rows;
+        for (int k = b; k < e; k++) rows.push_back(key[k].second);
+        std::vector<int> halo;
+        for (int r : rows) local_of[r] = -2;  // mark own
+        for (int r : rows)
+            for (int a = A.start[r]; a < A.start[r + 1]; a++)
+                if (local_of[A.col[a]] == -1) {
+                    local_of[A.col[a]] = -3;
+                    halo.push_back(A.col[a]);
+                }
+        std::sort(halo.begin(), halo.end());
+        std::vector<int> loc(rows);
+        loc.insert(loc.end(), halo.begin(), halo.end());
+        for (int k = 0; k < (int)loc.size(); k++) local_of[loc[k]] = k;
+        const int n1 = (int)loc.size(), n1p = (n1 + S - 1) / S * S, nop = ((int)rows.size() + S - 1) / S * S;
+        t.row0.push_back((int)t.trow.size());
+        t.nlocal.push_back(n1);
+        t.nown.push_back((int)rows.size());
+        t.s1_0.push_back((int)c1.size() / S);
+        t.s1_n.push_back(n1p / S);
+        t.s2_0.push_back((int)c2.size() / S);
+        t.s2_n.push_back(nop / S);
+        t.max_local = std::max(t.max_local, n1p);
+        for (int k = 0; k < n1p; k++) {
+            const int g = k < n1 ? loc[k] : -1;
+            t.trow.push_back(g);
+            std::vector<int> cc;
+            std::vector<double> vv;
+            if (g >= 0)
+                for (int a = A.start[g]; a < A.start[g + 1]; a++) {
+                    cc.push_back(A.col[a]);
+                    vv.push_back(A.val[a]);
+                }
+            c1.push_back(cc);
+            v1.push_back(vv);
+            pad1.push_back(g >= 0 ? g : loc[0]);
+        }
+        for (int k = 0; k < nop; k++) {
+            std::vector<int> cc;
+            std::vector<double> vv;
+            if (k < (int)rows.size()) {
+                const int g = rows[k];
+                for (int a = A.start[g]; a < A.start[g + 1]; a++) {
+                    cc.push_back(local_of[A.col[a]]);
+                    vv.push_back(A.val[a]);
+                }
+            }
+            c2.push_back(cc);
+            v2.push_back(vv);
+            pad2.push_back(k < (int)rows.size() ? k : 0);
+        }
+        for (int r : loc) local_of[r] = -1;
+    }
+    t.ntiles = (int)t.row0.size();
+    t.e1 = rows_to_sliced_ell(c1, v1, pad1, T);
+    t.e2 = rows_to_sliced_ell(c2, v2, pad2, T);
+    return t;
+}
+
 struct Assembly {
     std::vector<float> a_diag;      // [nd]
     HostCsr A;                      // off-diagonal part, nd x nd (columns sorted)

@@ -405,10 +405,12 @@ def _cube_at_impact(n=8):
     return sc, x0, v0
 
 
+@pytest.mark.parametrize("mode", [2, 3], ids=["persistent", "tiled"])
 @pytest.mark.parametrize("case", ["cloth", "cube_impact", "cube_impact_tol"])
-def test_persistent_global_step_bitwise(case):
+def test_persistent_global_step_bitwise(case, mode):
     """jacobi_mode 2 (RHS and all sweeps in one cooperative kernel, blocks synchronised by
-    sweep counters) reproduces jacobi_mode 1 (one kernel per sweep) bit for bit."""
+    sweep counters) and jacobi_mode 3 (two sweeps per launch over row tiles with halos in
+    shared memory) reproduce jacobi_mode 1 (one kernel per sweep) bit for bit."""
     if case == "cloth":
         sc, x0, v0 = scene.cloth_on_box(24), None, None
     else:
@@ -416,15 +418,15 @@ def test_persistent_global_step_bitwise(case):
     over = {"residual_tol": 1e-4} if case.endswith("_tol") else {}
     sc.params.ell_lanes = 4
     hs = []
-    for mode in (1, 2):
-        sc.params.jacobi_mode = mode
+    for m in (1, mode):
+        sc.params.jacobi_mode = m
         h = B.Handle(sc, **over)
         if x0 is not None:
             h.set_state(x0, v0)
         hs.append(h)
     gm = hs[1].global_mode()
-    assert gm["persistent"] and gm["blocks"] >= 1
-    assert not hs[0].global_mode()["persistent"]
+    assert gm["mode"] == ("persistent" if mode == 2 else "tiled")
+    assert hs[0].global_mode()["mode"] == "sweeps"
     for k in range(4):
         st = [h.step(1) for h in hs]
         assert st[0]["iters"] == st[1]["iters"] and st[0]["n_contacts"] == st[1]["n_contacts"]
@@ -437,7 +439,8 @@ def test_persistent_global_step_bitwise(case):
         h.close()
 
 
-def test_persistent_jacobi_entry_bitwise():
+@pytest.mark.parametrize("mode", [2, 3], ids=["persistent", "tiled"])
+def test_persistent_jacobi_entry_bitwise(mode):
     """admm_b200_jacobi (standalone sweeps) in both modes, odd and even sweep counts."""
     sc = scene.cube_on_ground(12)
     sc.params.ell_lanes = 2
@@ -445,11 +448,11 @@ def test_persistent_jacobi_entry_bitwise():
     x = _perturbed(sc, 1e-3, seed=22)
     b = rng.normal(size=(sc.n_dyn, 3))
     out = []
-    for mode in (1, 2):
-        sc.params.jacobi_mode = mode
+    for m in (1, mode):
+        sc.params.jacobi_mode = m
         h = B.Handle(sc)
         res = []
-        for sweeps in (2, 3, 7):
+        for sweeps in (2, 3, 4, 7):
             h.write(B.BUF_X, x)
             h.write(B.BUF_B, b)
             h.jacobi(sweeps)
