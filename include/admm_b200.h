@@ -299,6 +299,32 @@ int  admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd);
  * kernel per sweep and with the persistent kernel (0 when not timed). */
 int  admm_b200_global_mode(AdmmB200* h, int* persistent, int* blocks, float* ms_sweeps, float* ms_persist);
 
+/* --- learned block preconditioner (north-star addition, no reference counterpart) ---
+ * A 3-layer message-passing network (width 64) over the graph of the global
+ * matrix A predicts per dynamic vertex a 3x3 SPD block B_i = L_i L_i^T / a_ii
+ * for admm_b200_set_preconditioner (global_solver 2); o = 0 gives diag(A)^-1.
+ * It is trained on residual samples r of A x = b with the loss
+ * mean_k |A B r_k - r_k|^2 / |r_k|^2 by the kernels of gnn.cu (forward,
+ * backward, Adam).  The graph is A's off-diagonal CSR (symmetric pattern,
+ * sorted columns); node features [n x 6], edge features [nnz x 2] as described
+ * in parallel_admm_b200/gnn.py; set_graph swaps the system and keeps the
+ * parameters and the Adam state.  bf16 = 1 rounds the weights to BF16 in the
+ * forward and input-gradient products (FP32 accumulation). */
+typedef struct AdmmGnn AdmmGnn;
+int  admm_gnn_create(int bf16, AdmmGnn** out);
+int  admm_gnn_set_graph(AdmmGnn* g, int n, int n_edges, const int32_t* start, const int32_t* col, const float* val,
+                        const float* adiag, const float* node_feat, const float* edge_feat);
+void admm_gnn_destroy(AdmmGnn* g);
+int  admm_gnn_num_params(void);
+int  admm_gnn_set_params(AdmmGnn* g, const float* theta, int n_params);
+int  admm_gnn_get_params(AdmmGnn* g, float* theta, int n_params);
+int  admm_gnn_forward(AdmmGnn* g, float* blocks9);
+int  admm_gnn_loss_grad(AdmmGnn* g, const float* residuals, int k, double* loss, float* grad);
+int  admm_gnn_adam(AdmmGnn* g, float lr);
+/* The global-step matrix A of a handle: nnz of the off-diagonal part when start
+ * is NULL, else its CSR (start[n_dyn+1], col, val) and diagonal (host). */
+int  admm_b200_system(AdmmB200* h, int32_t* start, int32_t* col, float* val, float* diag);
+
 /* --- allocation-free Jacobi solve (no counterpart in the reference) ---
  * For callers that cannot allocate device memory themselves or through a handle
  * (their memory is owned by their own pool allocator, or cudaMalloc's latency and

@@ -220,6 +220,8 @@ def exported_symbols():
         "admm_b200_set_profiling", "admm_b200_kernels_per_step", "admm_b200_step_host",
         "admm_b200_phase_times", "admm_b200_set_probe", "admm_b200_probe_time", "admm_b200_tuning",
         "admm_b200_jacobi_noalloc", "admm_b200_global_mode", "admm_b200_set_preconditioner",
+        "admm_b200_system", "admm_gnn_create", "admm_gnn_set_graph", "admm_gnn_destroy", "admm_gnn_num_params",
+        "admm_gnn_set_params", "admm_gnn_get_params", "admm_gnn_forward", "admm_gnn_loss_grad", "admm_gnn_adam",
     ]
 
 

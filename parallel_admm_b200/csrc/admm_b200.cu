@@ -81,6 +81,8 @@ struct AdmmB200 {
     bool tiled = false;             // chosen mode: two sweeps per launch over row tiles
     TileSet ts;
     int tile_smem = 0;
+    HostCsr hostA;                  // the global matrix on the host (admm_b200_system)
+    std::vector<float> hostAdiag;
     float tune_ms_tiled = 0.f;
     float tune_ms_persist = 0.f, tune_ms_sweeps = 0.f;  // one global step, both modes
     // host-buffer stepping
@@ -1286,6 +1288,8 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         TRY(dalloc(h, &g.part, 2 * (size_t)g.blocks));
         TRY(dalloc(h, &g.scal, 8));
     }
+    h->hostA = as.A;
+    h->hostAdiag = as.a_diag;
     TRY(build_persist_plan(h, as.A));
     TRY(build_tiles_dev(h, as.A));
     h->persist = h->tiled = false;
@@ -1800,6 +1804,21 @@ int admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float
     if (ms_a) *ms_a = h->tune_ms_a;
     if (ms_r) *ms_r = h->tune_ms_r;
     return ADMM_OK;
+}
+
+int admm_b200_system(AdmmB200* h, int32_t* start, int32_t* col, float* val, float* diag) {
+    if (!h) return ADMM_ERR_INVALID;
+    const HostCsr& A = h->hostA;
+    const int nnz = (int)A.col.size();
+    if (!start) return nnz;
+    if (!col || !val || !diag) return ADMM_ERR_INVALID;
+    for (size_t i = 0; i < A.start.size(); i++) start[i] = A.start[i];
+    for (int k = 0; k < nnz; k++) {
+        col[k] = A.col[k];
+        val[k] = (float)A.val[k];
+    }
+    for (size_t i = 0; i < h->hostAdiag.size(); i++) diag[i] = h->hostAdiag[i];
+    return nnz;
 }
 
 int admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd) {

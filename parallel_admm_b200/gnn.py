@@ -1,0 +1,265 @@
+"""Learned per-vertex block preconditioner for the PCG global step (global_solver 2).
+
+A north-star addition with no counterpart in the reference.  The network (3 message-passing
+layers of width 64 over the graph of the global matrix A) and its training run on the GPU in
+the library's own kernels (csrc/gnn.cu, C ABI ``admm_gnn_*``); this module builds the inputs,
+drives training and hands the predicted blocks to a solver handle:
+
+    sysm = system(handle)                       # A of the handle (CSR + diagonal)
+    net = LearnedPreconditioner()
+    net.fit([(sysm, feats, residuals), ...])   # (system, residual samples) from plain runs
+    handle.set_preconditioner(net.blocks(sysm, feats))
+
+Node features per dynamic vertex: [log a_ii, log m_i, h^2 w_c,i / a_ii, degree / 16,
+sum_j |a_ij| / a_ii, 1], the first five standardised per system; edge features per
+off-diagonal entry: [a_ij / sqrt(a_ii a_jj),
+|p_i - p_j| / mean edge length].  Block i = L_i L_i^T / a_ii with L_i lower triangular from
+the network's 6 outputs (exp of the outputs clamped to [-8, 8] on the diagonal); messages are
+averaged over a vertex's neighbours; all-zero outputs give diag(A)^-1, the plain
+Jacobi preconditioner the network starts from and falls back to.
+"""
+import ctypes
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import backend as B
+
+_i = ctypes.POINTER(ctypes.c_int32)
+_f = ctypes.POINTER(ctypes.c_float)
+_d = ctypes.POINTER(ctypes.c_double)
+vp = ctypes.c_void_p
+
+
+def _lib():
+    L = B.lib()
+    if not getattr(L, "_gnn_sigs", False):
+        sig = {
+            "admm_gnn_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(vp)]),
+            "admm_gnn_set_graph": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, _i, _i, _f, _f, _f, _f]),
+            "admm_gnn_destroy": (None, [vp]),
+            "admm_gnn_num_params": (ctypes.c_int, []),
+            "admm_gnn_set_params": (ctypes.c_int, [vp, _f, ctypes.c_int]),
+            "admm_gnn_get_params": (ctypes.c_int, [vp, _f, ctypes.c_int]),
+            "admm_gnn_forward": (ctypes.c_int, [vp, _f]),
+            "admm_gnn_loss_grad": (ctypes.c_int, [vp, _f, ctypes.c_int, _d, _f]),
+            "admm_gnn_adam": (ctypes.c_int, [vp, ctypes.c_float]),
+            "admm_b200_system": (ctypes.c_int, [vp, _i, _i, _f, _f]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        L._gnn_sigs = True
+    return L
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(ct)
+
+
+class System:
+    """The global matrix A of a handle: off-diagonal CSR (sorted columns) and diagonal, FP32."""
+
+    def __init__(self, start, col, val, diag):
+        self.start = np.ascontiguousarray(start, np.int32)
+        self.col = np.ascontiguousarray(col, np.int32)
+        self.val = np.ascontiguousarray(val, np.float32)
+        self.diag = np.ascontiguousarray(diag, np.float32)
+        self.n = len(self.diag)
+
+    def matvec(self, v: np.ndarray) -> np.ndarray:
+        """A v for v of shape (n, 3), FP64 on the host (data generation, evaluation)."""
+        rows = np.repeat(np.arange(self.n), np.diff(self.start))
+        out = self.diag[:, None].astype(np.float64) * v
+        np.add.at(out, rows, self.val[:, None].astype(np.float64) * v[self.col])
+        return out
+
+
+def system(h: "B.Handle") -> System:
+    L = _lib()
+    nnz = L.admm_b200_system(h.h, None, None, None, None)
+    start = np.zeros(h.n_dyn + 1, np.int32)
+    col = np.zeros(max(nnz, 1), np.int32)
+    val = np.zeros(max(nnz, 1), np.float32)
+    diag = np.zeros(h.n_dyn, np.float32)
+    rc = L.admm_b200_system(h.h, _p(start, _i), _p(col, _i), _p(val, _f), _p(diag, _f))
+    if rc < 0:
+        raise B.AdmmError(rc, "admm_b200_system")
+    return System(start, col[:nnz], val[:nnz], diag)
+
+
+def features(sysm: System, mass: np.ndarray, wc_dt2: np.ndarray, pos: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """Node features [n x 6] and edge features [nnz x 2] (see the module docstring)."""
+    n = sysm.n
+    a = sysm.diag.astype(np.float64)
+    val = sysm.val.astype(np.float64)
+    rows = np.repeat(np.arange(n), np.diff(sysm.start))
+    deg = np.diff(sysm.start).astype(np.float64)
+    off = np.zeros(n)
+    np.add.at(off, rows, np.abs(val))
+    x = np.stack([np.log(a), np.log(np.maximum(mass[:n].astype(np.float64), 1e-30)), wc_dt2[:n] / a, deg / 16.0,
+                  off / a, np.ones(n)], 1)
+    mu, sd = x[:, :5].mean(0), x[:, :5].std(0)
+    x[:, :5] = (x[:, :5] - mu) / np.where(sd > 0, sd, 1.0)
+    d = np.linalg.norm(pos[rows].astype(np.float64) - pos[sysm.col].astype(np.float64), axis=1)
+    ef = np.stack([val / np.sqrt(a[rows] * a[sysm.col]), d / max(d.mean() if len(d) else 1.0, 1e-30)], 1)
+    return x.astype(np.float32), ef.astype(np.float32)
+
+
+def scene_features(sc, sysm: System) -> Tuple[np.ndarray, np.ndarray]:
+    """Features of a scene's system at its rest positions."""
+    wc_dt2 = np.zeros(sysm.n)
+    surf = np.zeros(sc.n_vert, bool)
+    surf[sc.surf_verts] = True
+    wc = sc.contact_w.astype(np.float64) * sc.params.dt * sc.params.dt
+    wc_dt2[:] = np.where(surf[:sysm.n], wc[:sysm.n], 0.0)
+    return features(sysm, sc.mass, wc_dt2, sc.verts[:sysm.n])
+
+
+def global_residuals(h: "B.Handle", sysm: System, frames: int) -> np.ndarray:
+    """Residual samples r = b - A x of the global step after the plain solve, one per frame
+    (the handle steps `frames` substeps)."""
+    out = []
+    for _ in range(frames):
+        h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+        b = h.read(B.BUF_B)[:sysm.n].astype(np.float64)
+        x = h.read(B.BUF_X)[:sysm.n].astype(np.float64)
+        r = b - sysm.matvec(x)
+        if np.linalg.norm(r) > 0:
+            out.append(r.astype(np.float32))
+    return np.array(out, np.float32).reshape(-1, sysm.n, 3)
+
+
+def pcg_iterations(sysm: System, blocks: Optional[np.ndarray], b: np.ndarray, tol: float = 1e-4,
+                   maxit: int = 2000) -> int:
+    """Preconditioned CG iterations to |r| <= tol |b| (FP64 on the host; blocks None = diag(A))."""
+    if blocks is None:
+        apply = lambda r: r / sysm.diag[:, None].astype(np.float64)
+    else:
+        Bk = blocks.reshape(-1, 3, 3).astype(np.float64)
+        apply = lambda r: np.einsum("nij,nj->ni", Bk, r)
+    x = np.zeros_like(b, np.float64)
+    r = b.astype(np.float64).copy()
+    u = apply(r)
+    p = u.copy()
+    rz = np.sum(r * u)
+    r0 = np.linalg.norm(r)
+    for k in range(maxit):
+        if np.linalg.norm(r) <= tol * r0:
+            return k
+        q = sysm.matvec(p)
+        a = rz / np.sum(p * q)
+        x += a * p
+        r -= a * q
+        u = apply(r)
+        rzn = np.sum(r * u)
+        if not rzn > 0:
+            return maxit
+        p = u + (rzn / rz) * p
+        rz = rzn
+    return maxit
+
+
+class LearnedPreconditioner:
+    """The network (parameters, Adam state) on the GPU; one system at a time."""
+
+    def __init__(self, bf16: bool = True, seed: int = 0):
+        L = _lib()
+        self.g = vp()
+        rc = L.admm_gnn_create(int(bf16), ctypes.byref(self.g))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_gnn_create")
+        self.P = L.admm_gnn_num_params()
+        self.set_params(init_params(seed))
+        self._bound = None
+
+    def close(self):
+        if self.g:
+            _lib().admm_gnn_destroy(self.g)
+            self.g = vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bind(self, sysm: System, x: np.ndarray, ef: np.ndarray):
+        key = (id(sysm), id(x))
+        if self._bound == key:
+            return
+        self._keep = (sysm, np.ascontiguousarray(x, np.float32), np.ascontiguousarray(ef, np.float32))
+        s, xx, ee = self._keep
+        rc = _lib().admm_gnn_set_graph(self.g, s.n, len(s.col), _p(s.start, _i), _p(s.col, _i), _p(s.val, _f),
+                                       _p(s.diag, _f), _p(xx, _f), _p(ee, _f))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_gnn_set_graph")
+        self._bound = key
+
+    def set_params(self, theta: np.ndarray):
+        th = np.ascontiguousarray(theta, np.float32)
+        assert th.size == self.P
+        rc = _lib().admm_gnn_set_params(self.g, _p(th, _f), self.P)
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_gnn_set_params")
+
+    def params(self) -> np.ndarray:
+        th = np.zeros(self.P, np.float32)
+        _lib().admm_gnn_get_params(self.g, _p(th, _f), self.P)
+        return th
+
+    def blocks(self, sysm: System, x: np.ndarray, ef: np.ndarray) -> np.ndarray:
+        self.bind(sysm, x, ef)
+        out = np.zeros((sysm.n, 9), np.float32)
+        rc = _lib().admm_gnn_forward(self.g, _p(out, _f))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_gnn_forward")
+        return out
+
+    def loss_grad(self, sysm: System, x: np.ndarray, ef: np.ndarray, R: np.ndarray):
+        self.bind(sysm, x, ef)
+        RR = np.ascontiguousarray(R, np.float32)
+        loss = ctypes.c_double()
+        grad = np.zeros(self.P, np.float32)
+        rc = _lib().admm_gnn_loss_grad(self.g, _p(RR, _f), RR.shape[0], ctypes.byref(loss), _p(grad, _f))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_gnn_loss_grad")
+        return loss.value, grad
+
+    def step(self, lr: float):
+        rc = _lib().admm_gnn_adam(self.g, ctypes.c_float(lr))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_gnn_adam")
+
+    def fit(self, data: Sequence[Tuple[System, np.ndarray, np.ndarray, np.ndarray]], epochs: int = 20,
+            lr: float = 1e-3, batch: int = 8, seed: int = 0) -> List[float]:
+        """Adam on the mean loss over (system, node features, edge features, residuals) items;
+        returns the loss per epoch."""
+        rng = np.random.default_rng(seed)
+        hist = []
+        for _ in range(epochs):
+            tot = 0.0
+            for k in rng.permutation(len(data)):
+                sysm, x, ef, R = data[k]
+                sel = rng.choice(len(R), min(batch, len(R)), replace=False)
+                loss, _ = self.loss_grad(sysm, x, ef, R[sel])
+                self.step(lr)
+                tot += loss / len(data)
+            hist.append(tot)
+        return hist
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """Scaled normal weights, zero biases, zero head (the network starts as diag(A)^-1)."""
+    rng = np.random.default_rng(seed)
+    H, F_IN, F_E = 64, 6, 2
+    shapes = [(H, F_IN), (H,)]
+    for _ in range(3):
+        shapes += [(H, 2 * H + F_E), (H,), (H, 2 * H), (H,)]
+    shapes += [(6, H), (6,)]
+    parts = []
+    for s in shapes:
+        parts.append(rng.normal(scale=1.0 / np.sqrt(s[1]), size=s) if len(s) == 2 else np.zeros(s))
+    parts[-2][:] = 0.0
+    return np.concatenate([p.ravel() for p in parts]).astype(np.float32)
