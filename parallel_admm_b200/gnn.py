@@ -217,6 +217,22 @@ class LearnedPreconditioner:
             raise B.AdmmError(rc, "admm_gnn_forward")
         return out
 
+    def blocks_or_fallback(self, sysm: System, x: np.ndarray, ef: np.ndarray, probe: np.ndarray,
+                           tol: float = 1e-4) -> Tuple[np.ndarray, bool, float]:
+        """The learned blocks for a system, judged by plain diag(A): on the probe residuals,
+        PCG with the learned blocks must need fewer iterations than with diag(A), else
+        diag(A) as 3x3 blocks is returned.  Returns (blocks, learned_used, iteration ratio
+        learned / diag(A))."""
+        blk = self.blocks(sysm, x, ef)
+        it_l = np.mean([pcg_iterations(sysm, blk, r.astype(np.float64), tol) for r in probe])
+        it_j = np.mean([pcg_iterations(sysm, None, r.astype(np.float64), tol) for r in probe])
+        ratio = float(it_l / max(it_j, 1e-30))
+        if it_l < it_j:
+            return blk, True, ratio
+        diag = np.zeros((sysm.n, 9), np.float32)
+        diag[:, 0] = diag[:, 4] = diag[:, 8] = 1.0 / sysm.diag
+        return diag, False, ratio
+
     def loss_grad(self, sysm: System, x: np.ndarray, ef: np.ndarray, R: np.ndarray):
         self.bind(sysm, x, ef)
         RR = np.ascontiguousarray(R, np.float32)
