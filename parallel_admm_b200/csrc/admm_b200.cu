@@ -632,20 +632,38 @@ int build_tiles_dev(AdmmB200* h, const HostCsr& A) {
     return ADMM_OK;
 }
 
-// Milliseconds of one global step (RHS + jac_iter sweeps), eager, in either mode.
+// Milliseconds of one global step (RHS + jac_iter sweeps) in the given mode,
+// timed as a captured graph of 8 global steps (as the substep graph runs them,
+// with programmatic dependent launch); +inf when the mode cannot be captured.
 int time_global(AdmmB200* h, int mode, float* ms) {
     const bool keep = h->persist, keep_t = h->tiled;
     h->persist = mode == 2;
     h->tiled = mode == 3;
     h->cstream = h->stream;
-    enqueue_global(h, false);
-    CK(cudaEventRecord(h->ev0, h->stream));
     constexpr int kReps = 8;
-    for (int r = 0; r < kReps; r++) enqueue_global(h, false);
-    CK(cudaEventRecord(h->ev1, h->stream));
-    CK(cudaEventSynchronize(h->ev1));
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        for (int r = 0; r < kReps; r++) enqueue_global(h, false);
+        ok = cudaStreamEndCapture(h->stream, &g) == cudaSuccess && g;
+    }
+    ok = ok && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
     h->persist = keep;
     h->tiled = keep_t;
+    if (!ok) {
+        cudaGetLastError();
+        if (ge) cudaGraphExecDestroy(ge);
+        *ms = 1e30f;
+        return ADMM_OK;
+    }
+    CK(cudaGraphLaunch(ge, h->stream));  // warm-up
+    CK(cudaEventRecord(h->ev0, h->stream));
+    CK(cudaGraphLaunch(ge, h->stream));
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    cudaGraphExecDestroy(ge);
     CK(cudaGetLastError());
     int e[4] = {0, 0, 0, 0};
     CK(cudaMemcpy(e, h->s.err, sizeof(e), cudaMemcpyDeviceToHost));
