@@ -66,6 +66,9 @@ struct AdmmB200 {
     int grid_buckets = 0;
     bool pdl = true;                // programmatic dependent launch between the kernels of a substep
     cudaStream_t cstream = nullptr; // stream the enqueue helpers launch on (capture target)
+    cudaStream_t side = nullptr;    // second branch of an ADMM iteration (local step)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool overlap = true;
     cudaStream_t body_stream = nullptr;
     int chunk = 0;                  // ADMM iterations between residual checks (residual_tol > 0)
     bool in_body = false;           // capturing the body of the conditional node (no event nodes allowed)
@@ -785,12 +788,31 @@ void enqueue_residual(AdmmB200* h) {
 // and refitted by the later ones unless bvh_refit is off.
 void enqueue_iteration(AdmmB200* h, int it, bool first, bool residual) {
     DevScene& s = h->s;
-    if (s.contact && it % h->dcd_interval == 0) enqueue_dcd(h, !h->bvh_refit || first);
-    enqueue_local(h, first ? LOCAL_PROX : (LOCAL_PROX | LOCAL_DUAL));
+    const int local_mode = first ? LOCAL_PROX : (LOCAL_PROX | LOCAL_DUAL);
+    // The local step (z, Ue) and the detection + contact step (p, Uc) read x and
+    // write disjoint data: with contact they run as two branches of the graph,
+    // joined before the right-hand side.  Not inside the body of a conditional
+    // node (iterations after the first chunk of a residual-tolerance substep),
+    // whose capture keeps to one stream, and not under phase probes.
+    const bool branches = s.contact && h->overlap && !h->in_body && h->probe_kernel != ADMM_PROBE_PHASES;
+    cudaStream_t main = h->cstream;
+    if (branches) {
+        cudaEventRecord(h->ev_fork, main);
+        cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+        h->cstream = h->side;
+        enqueue_local(h, local_mode);
+        cudaEventRecord(h->ev_join, h->side);
+        h->cstream = main;
+    } else {
+        if (s.contact && it % h->dcd_interval == 0) enqueue_dcd(h, !h->bvh_refit || first);
+        enqueue_local(h, local_mode);
+    }
+    if (branches && it % h->dcd_interval == 0) enqueue_dcd(h, !h->bvh_refit || first);
     if (s.contact) {
         const int rc = enqueue_contact(h, !first);
         if (rc != ADMM_OK && h->enqueue_rc == ADMM_OK) h->enqueue_rc = rc;
     }
+    if (branches) cudaStreamWaitEvent(main, h->ev_join, 0);
     enqueue_global(h, residual);
     if (residual) enqueue_residual(h);
 }
@@ -1276,6 +1298,9 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
 
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
 
     h->cstream = h->stream;
     {
@@ -1438,6 +1463,9 @@ void admm_b200_destroy(AdmmB200* h) {
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->body_stream) cudaStreamDestroy(h->body_stream);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
 
     delete h;
 }
