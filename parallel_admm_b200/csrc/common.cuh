@@ -12,6 +12,12 @@
 // have completed and their writes are visible.  Results are unchanged; the
 // launch latency of a kernel overlaps the execution of its predecessor.  Both
 // instructions are no-ops for a kernel launched without the PDL attribute.
+// The two halves, for kernels that first load data which no kernel of a substep
+// writes (matrices, constraint records) and only then wait: those loads overlap
+// the tail of the preceding kernels.
+#define ADMM_PDL_TRIGGER() asm volatile("griddepcontrol.launch_dependents;" ::: "memory")
+#define ADMM_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+
 #define ADMM_PDL_PROLOGUE()                                          \
     do {                                                             \
         asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); \

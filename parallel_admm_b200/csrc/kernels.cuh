@@ -53,6 +53,30 @@ ADMM_DEV void store_rows(const DevScene& s, int row, const float (&zz)[3 * NR], 
     }
 }
 
+// D x rows of tet c from its (already loaded) indices and Binv rows.
+ADMM_DEV void tet_dx_from(const float4* __restrict__ x, int4 id, float4 B0, float4 B1, float4 B2, float (&dx)[9]) {
+    const float4 p0 = x[id.x], p1 = x[id.y], p2 = x[id.z], p3 = x[id.w];
+    const float4 e0 = sub3(p1, p0), e1 = sub3(p2, p0), e2 = sub3(p3, p0);
+    const float b[3][3] = {{B0.x, B0.y, B0.z}, {B1.x, B1.y, B1.z}, {B2.x, B2.y, B2.z}};
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        dx[3 * r + 0] = e0.x * b[0][r] + e1.x * b[1][r] + e2.x * b[2][r];
+        dx[3 * r + 1] = e0.y * b[0][r] + e1.y * b[1][r] + e2.y * b[2][r];
+        dx[3 * r + 2] = e0.z * b[0][r] + e1.z * b[1][r] + e2.z * b[2][r];
+    }
+}
+
+ADMM_DEV void tri_dx_from(const float4* __restrict__ x, int4 id, float4 B, float (&dx)[6]) {
+    const float4 p0 = x[id.x], p1 = x[id.y], p2 = x[id.z];
+    const float4 e0 = sub3(p1, p0), e1 = sub3(p2, p0);
+    dx[0] = e0.x * B.x + e1.x * B.z;
+    dx[1] = e0.y * B.x + e1.y * B.z;
+    dx[2] = e0.z * B.x + e1.z * B.z;
+    dx[3] = e0.x * B.y + e1.x * B.w;
+    dx[4] = e0.y * B.y + e1.y * B.w;
+    dx[5] = e0.z * B.y + e1.z * B.w;
+}
+
 ADMM_DEV void tet_dx(const float4* __restrict__ x, const DevScene& s, int c, float (&dx)[9]) {
     const int4 id = s.tet_inds[c];
     const float4 p0 = x[id.x], p1 = x[id.y], p2 = x[id.z], p3 = x[id.w];
@@ -95,14 +119,18 @@ ADMM_DEV void bend_dx(const float4* __restrict__ x, const DevScene& s, int c, fl
 
 template <int MODE>
 __global__ void __launch_bounds__(kLocalThreads) k_local(DevScene s, int tet_blocks, int tri_blocks, int bend_blocks) {
-    ADMM_PDL_PROLOGUE();
+    // constraint records are constant: they are loaded before the programmatic wait
+    ADMM_PDL_TRIGGER();
     int blk = blockIdx.x;
     if (blk < tet_blocks) {
         const int c = blk * kLocalThreads + threadIdx.x;
         if (c >= s.ntet) return;
+        const int4 id = __ldg(&s.tet_inds[c]);
+        const float4 B0 = __ldg(&s.tet_b0[c]), B1 = __ldg(&s.tet_b1[c]), B2 = __ldg(&s.tet_b2[c]);
+        ADMM_PDL_WAIT();
         float dx[9], zz[9];
         float4 ue[3];
-        tet_dx(s.x, s, c, dx);
+        tet_dx_from(s.x, id, B0, B1, B2, dx);
         const int row = s.tet_sr + 3 * c;
         finish_rows<MODE, 3>(s, row, dx, zz, ue);
         if (MODE & LOCAL_PROX) prox_tet(zz);
@@ -113,9 +141,12 @@ __global__ void __launch_bounds__(kLocalThreads) k_local(DevScene s, int tet_blo
     if (blk < tri_blocks) {
         const int c = blk * kLocalThreads + threadIdx.x;
         if (c >= s.ntri) return;
+        const int4 id = __ldg(&s.tri_inds[c]);
+        const float4 Bt = __ldg(&s.tri_binv[c]);
+        ADMM_PDL_WAIT();
         float dx[6], zz[6];
         float4 ue[2];
-        tri_dx(s.x, s, c, dx);
+        tri_dx_from(s.x, id, Bt, dx);
         const int row = s.tri_sr + 2 * c;
         finish_rows<MODE, 2>(s, row, dx, zz, ue);
         if (MODE & LOCAL_PROX) prox_tri(zz);
@@ -126,6 +157,7 @@ __global__ void __launch_bounds__(kLocalThreads) k_local(DevScene s, int tet_blo
     if (blk < bend_blocks) {
         const int c = blk * kLocalThreads + threadIdx.x;
         if (c >= s.nbend) return;
+        ADMM_PDL_WAIT();
         float dx[3], zz[3];
         float4 ue[1];
         bend_dx(s.x, s, c, dx);
@@ -139,7 +171,9 @@ __global__ void __launch_bounds__(kLocalThreads) k_local(DevScene s, int tet_blo
     {
         const int c = blk * kLocalThreads + threadIdx.x;
         if (c >= s.npin) return;
-        const float4 p = s.x[s.pin_inds[c]];
+        const int pi = __ldg(&s.pin_inds[c]);
+        ADMM_PDL_WAIT();
+        const float4 p = s.x[pi];
         float dx[3] = {p.x, p.y, p.z}, zz[3];
         float4 ue[1];
         const int row = s.pin_sr + c;
@@ -283,6 +317,52 @@ ADMM_DEV void rhs_row(const DevScene& s, int i, float4 acc) {
     if (SAVE_PREV) s.xprev[i] = s.x[i];
 }
 
+// ell_row_sum with the matrix entries of the lane's first kPrefetch steps loaded
+// before the programmatic-dependency wait (the matrix is constant), the gathered
+// vector after it.  Same operations in the same order as ell_row_sum.
+constexpr int kPrefetch = 8;
+
+template <int T>
+ADMM_DEV float4 ell_row_sum_pf(const SlicedEll& M, const float4* __restrict__ v, int w, int lane, int& row) {
+    constexpr int S = 32 / T;
+    row = w * S + (lane % S);
+    const int b = M.ptr[w], e = M.ptr[w + 1];
+    int cc[kPrefetch];
+    float vv[kPrefetch];
+#pragma unroll
+    for (int j = 0; j < kPrefetch; j++) {
+        const int k = b + lane + 32 * j;
+        cc[j] = k < e ? __ldg(&M.col[k]) : 0;
+        vv[j] = k < e ? __ldg(&M.val[k]) : 0.f;
+    }
+    ADMM_PDL_WAIT();
+    float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll
+    for (int j = 0; j < kPrefetch; j++) {
+        if (b + lane + 32 * j < e) {
+            const float4 q = v[cc[j]];
+            ax = fmaf(vv[j], q.x, ax);
+            ay = fmaf(vv[j], q.y, ay);
+            az = fmaf(vv[j], q.z, az);
+        }
+    }
+    for (int k = b + lane + 32 * kPrefetch; k < e; k += 32) {
+        const int c = __ldg(&M.col[k]);
+        const float a = __ldg(&M.val[k]);
+        const float4 q = v[c];
+        ax = fmaf(a, q.x, ax);
+        ay = fmaf(a, q.y, ay);
+        az = fmaf(a, q.z, az);
+    }
+#pragma unroll
+    for (int o = S; o < 32; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+    }
+    return f4(ax, ay, az);
+}
+
 template <int T, bool SAVE_PREV>
 __global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
     ADMM_PDL_PROLOGUE();
@@ -310,12 +390,12 @@ ADMM_DEV void jacobi_row(const DevScene& s, int i, float4 acc, float4* __restric
 template <int T>
 __global__ void __launch_bounds__(kVertThreads) k_jacobi(DevScene s, const float4* __restrict__ src,
                                                          float4* __restrict__ dst) {
-    ADMM_PDL_PROLOGUE();
+    ADMM_PDL_TRIGGER();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= s.A.nslices) return;
     int i;
-    const float4 acc = ell_row_sum<T>(s.A, src, w, lane, i);
+    const float4 acc = ell_row_sum_pf<T>(s.A, src, w, lane, i);
     if (lane >= 32 / T || i >= s.nd) return;
     jacobi_row(s, i, acc, dst);
 }
