@@ -84,6 +84,7 @@ def make_scene(args, rank=0):
     sc.params.ell_lanes = args.ell_lanes
     sc.params.global_solver = args.global_solver
     sc.params.pcg_iter = args.pcg_iter
+    sc.params.query_lanes = args.query_lanes
     return sc
 
 
@@ -263,6 +264,8 @@ def main():
     ap.add_argument("--global-solver", type=int, default=0, choices=[0, 1, 2],
                     help="global step: 0 Jacobi sweeps (the reference's), 1 PCG with diag(A), 2 PCG with blocks")
     ap.add_argument("--pcg-iter", type=int, default=0, help="PCG iterations per global step (0 = jacobi_iter / 2)")
+    ap.add_argument("--query-lanes", type=int, default=0, choices=[0, 8, 16, 32],
+                    help="lanes per grid DCD query (0 = chosen from the number of queries)")
     ap.add_argument("--ref-steps", type=int, default=200, help="cap on steps timed by --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--start-frame", type=int, default=0,

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define ADMM_B200_ABI_VERSION 2
+#define ADMM_B200_ABI_VERSION 3
 
 /* status codes */
 #define ADMM_OK                    0
@@ -130,6 +130,11 @@ typedef struct AdmmB200Desc {
      * dynamic.  No reference counterpart (the reference has one mu per scene);
      * used by batches of bodies with different materials. */
     const float*   vert_mu;
+    /* Lanes per DCD query of the grid broad phase (8, 16 or 32); 0 = chosen at
+     * create from the number of queries: 32 while 32 lanes per query fill at most
+     * four waves of the device (a latency-bound detection), else 16 or 8 (a
+     * throughput-bound one).  All give the same contact list. */
+    int32_t query_lanes;
 } AdmmB200Desc;
 
 /* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */

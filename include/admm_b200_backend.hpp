@@ -37,6 +37,7 @@ public:
     int broad_phase = 0;  // 0 = default (uniform grid)
     int global_solver = 0;  // 0 = Jacobi as the reference
     int pcg_iter = 0;
+    int query_lanes = 0;  // 0 = chosen from the number of DCD queries
 
     ~ADMMInnerB200() override {
         if (h_) admm_b200_destroy(h_);
@@ -197,6 +198,7 @@ private:
         d.broad_phase = broad_phase;
         d.global_solver = global_solver;
         d.pcg_iter = pcg_iter;
+        d.query_lanes = query_lanes;
     }
 };
 

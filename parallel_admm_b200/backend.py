@@ -21,7 +21,7 @@ from .scene import Scene
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libadmm_b200.so")
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 OK = 0
 ERR_INVALID = -1
 ERR_CUDA = -2
@@ -73,7 +73,7 @@ class AdmmB200Desc(ctypes.Structure):
         ("residual_tol", ctypes.c_float), ("residual_check_every", ctypes.c_int32),
         ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32), ("jacobi_mode", ctypes.c_int32),
         ("broad_phase", ctypes.c_int32), ("global_solver", ctypes.c_int32), ("pcg_iter", ctypes.c_int32),
-        ("vert_mu", ctypes.POINTER(ctypes.c_float)),
+        ("vert_mu", ctypes.POINTER(ctypes.c_float)), ("query_lanes", ctypes.c_int32),
     ]
 
 
@@ -140,6 +140,7 @@ class DescHolder:
         d.broad_phase = int(p.broad_phase)
         d.global_solver = int(p.global_solver)
         d.pcg_iter = int(p.pcg_iter)
+        d.query_lanes = int(getattr(p, "query_lanes", 0))
         vm = getattr(sc, "vert_mu", None)
         d.vert_mu = arr("vm", vm, np.float32) if vm is not None else None
         for k, v in overrides.items():

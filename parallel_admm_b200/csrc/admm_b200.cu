@@ -64,6 +64,7 @@ struct AdmmB200 {
     int enqueue_rc = ADMM_OK;       // first error while enqueueing or capturing a substep
     float grid_cell_size = 0.f;
     int grid_buckets = 0;
+    int query_lanes = 32;           // lanes per grid DCD query (8, 16, 32)
     bool pdl = true;                // programmatic dependent launch between the kernels of a substep
     cudaStream_t cstream = nullptr; // stream the enqueue helpers launch on (capture target)
     cudaStream_t side = nullptr;    // second branch of an ADMM iteration (local step)
@@ -284,6 +285,20 @@ void enqueue_build(AdmmB200* h, BvhDev& t, const int* elems, int stride, bool tr
     LAUNCH(k_refit, blocks(n, 256), 256, t);
 }
 
+// Grid queries with h->query_lanes lanes per query (count or write pass).
+void launch_grid_query(AdmmB200* h, bool write, int nq) {
+    DevScene& s = h->s;
+    const int g = blocks((int)std::min<int64_t>((int64_t)nq * h->query_lanes, INT32_MAX), kQueryThreads);
+    switch (h->query_lanes * 2 + (write ? 1 : 0)) {
+        case 16: LAUNCH((k_grid_query<false, 8>), g, kQueryThreads, s); break;
+        case 17: LAUNCH_P(ADMM_KERNEL_DCD_VF, (k_grid_query<true, 8>), g, kQueryThreads, s); break;
+        case 32: LAUNCH((k_grid_query<false, 16>), g, kQueryThreads, s); break;
+        case 33: LAUNCH_P(ADMM_KERNEL_DCD_VF, (k_grid_query<true, 16>), g, kQueryThreads, s); break;
+        case 64: LAUNCH((k_grid_query<false, 32>), g, kQueryThreads, s); break;
+        default: LAUNCH_P(ADMM_KERNEL_DCD_VF, (k_grid_query<true, 32>), g, kQueryThreads, s); break;
+    }
+}
+
 // DCD + contact conversion + incidence lists + S_c / Gamma / K_c, all on device.
 // rebuild = false refits the trees of the previous build.
 void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
@@ -303,7 +318,7 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
             }
             LAUNCH(k_grid_scatter, blocks(ne, 256), 256, s);
         }
-        if (nq > 0) LAUNCH(k_grid_query<false>, blocks(nq * kQueryLanes, 128), 128, s);
+        if (nq > 0) launch_grid_query(h, false, nq);
     } else {
         if (rebuild) {
             LAUNCH(k_scene_init, 1, 32, s.bf, s.be);
@@ -325,7 +340,7 @@ void enqueue_dcd(AdmmB200* h, bool rebuild = true) {
     }
     LAUNCH(k_set_count, 1, 1, s);
     if (h->use_grid) {
-        if (nq > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_grid_query<true>, blocks(nq * kQueryLanes, 128), 128, s);
+        if (nq > 0) launch_grid_query(h, true, nq);
     } else {
         if (s.nsv > 0) LAUNCH_P(ADMM_KERNEL_DCD_VF, k_dcd_vf<true>, blocks(s.nsv, 128), 128, s);
         if (s.nse > 0) LAUNCH_P(ADMM_KERNEL_DCD_EE, k_dcd_ee<true>, blocks(s.nse, 128), 128, s);
@@ -1062,9 +1077,19 @@ int setup_grid(AdmmB200* h, const AdmmB200Desc* d) {
     TRY(dalloc(h, &g.big_edge, std::max(s.nse, 1)));
     TRY(dalloc(h, &g.mode, std::max(ne, 1)));
     TRY(dalloc(h, &g.qkey, std::max(s.cap, 1)));
-    const size_t lanes = (size_t)std::max(s.nsv + s.nse, 1) * kQueryLanes;
-    TRY(dalloc(h, &g.qhits, lanes * kQueryHits));
-    TRY(dalloc(h, &g.qlane, lanes));
+    TRY(dalloc(h, &g.qhits, (size_t)std::max(s.nsv + s.nse, 1) * kQueryHitsMax));
+    // lanes per query: 32 while 32 lanes per query fill at most four waves of
+    // the device, else 16 or 8 (a detection of millions of queries is bound by
+    // throughput, not by the latency of one query's loads)
+    if (d->query_lanes != 0) {
+        h->query_lanes = d->query_lanes;
+    } else {
+        int sms = 148;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+        const int64_t four_waves = 4ll * sms * 2048;
+        const int64_t nq = s.nsv + s.nse;
+        h->query_lanes = nq * 32 <= four_waves ? 32 : nq * 16 <= four_waves ? 16 : 8;
+    }
     return ADMM_OK;
 }
 
@@ -1080,6 +1105,8 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     if (!(d->dt > 0.f)) return fail(h, ADMM_ERR_INVALID, "dt");
     if (d->admm_max_iter < 0 || d->gs_max_iter < 0 || d->jacobi_iter < 0) return fail(h, ADMM_ERR_INVALID, "iteration counts");
     if (d->enable_contact && d->max_contacts <= 0) return fail(h, ADMM_ERR_INVALID, "max_contacts");
+    if (d->query_lanes != 0 && d->query_lanes != 8 && d->query_lanes != 16 && d->query_lanes != 32)
+        return fail(h, ADMM_ERR_INVALID, "query_lanes");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
         return fail(h, ADMM_ERR_NO_DEVICE, "no CUDA device");

@@ -201,14 +201,19 @@ ADMM_DEV void grid_sort_segment(const DevScene& s, int b, int e) {
 }
 
 // ---------------------------------------------------------------------------
-// Queries.  kQueryLanes consecutive threads serve one query: they split its
-// cells (and the big lists) between them, so that the loads of different
-// cells are in flight at the same time.  Each walk calls f(partner) for every
-// element that passes the box test and the once-per-pair cell rule; f applies
-// the index rules and the narrow phase.
+// Queries: G consecutive lanes of a warp serve one query (G = 8, 16 or 32).
+// The entries of all cells of the query's range are numbered consecutively (an
+// inclusive scan of the bucket sizes over the group, G cells at a time) and
+// lane k of the group takes entries k, k + G, ..., so every lane has the same
+// share whatever the cell sizes; an entry's cell key, box and first-cell bits
+// are loaded together.  Candidates that pass the cell-key, once-per-pair and
+// box tests are queued in shared memory and handed to the narrow phase G at a
+// time, so that it runs on full groups.  G = 32 suits a few thousand queries
+// (latency bound: more lanes per query shorten each query's chain of loads);
+// G = 8 suits millions (throughput bound: less scan and queue work per entry).
 // ---------------------------------------------------------------------------
-constexpr int kQueryLanes = 8;
-constexpr int kQueryHits = 4;  // hits per lane that the count pass records for the write pass
+constexpr int kQueryThreads = 128;  // block size of the query kernels
+constexpr int kQueryHitsMax = 32;   // partners the count pass records per query
 
 ADMM_DEV int3 grid_cell_at(int3 a, int3 b, int ci) {
     const int dx = b.x - a.x + 1, dy = b.y - a.y + 1;
@@ -236,94 +241,154 @@ ADMM_DEV float4 edge_box_lo(const DevScene& s, int o, float4& up) {
     return lo;
 }
 
-// Candidate triangles of surface vertex position P (lane `sub` of the group).
-template <class F>
-ADMM_DEV void grid_walk_vf(const DevScene& s, float4 P, int sub, F f) {
-    const GridDev& g = s.grid;
-    const float gap = s.thickness;
-    int3 a, b;
-    grid_query_range(P, P, gap, g.inv_c, a, b);
-    if (grid_range_small(a, b)) {
-        const int nc = grid_cells(a, b);
-        for (int ci = sub; ci < nc; ci += kQueryLanes) {
-            const int3 c = grid_cell_at(a, b, ci);
-            const int bk = grid_bucket(c.x, c.y, c.z, 0, g.hmask);
-            const unsigned long long key = grid_cell_key(c.x, c.y, c.z);
-            const int k1 = g.start[bk + 1];
-            const int qfirst = (c.x == a.x ? 1 : 0) | (c.y == a.y ? 2 : 0) | (c.z == a.z ? 4 : 0);
-            for (int k = g.start[bk]; k < k1; k++) {
-                if (g.ent_key[k] != key) continue;  // another cell of the bucket
-                const float4 up = g.ent_up[k];
-                // once per pair: this cell is the first of the query's or of the element's range on every axis
-                if (((qfirst | __float_as_int(up.w)) & 7) != 7) continue;
-                const float4 lo = g.ent_lo[k];
-                if (!box_overlap(P, P, lo, up, gap)) continue;
-                f(__float_as_int(lo.w));
-            }
-        }
-    } else {
-        for (int t = sub; t < s.nst; t += kQueryLanes) {
-            if (!g.mode[t]) continue;
-            float4 up;
-            const float4 lo = tri_box_lo(s, t, up);
-            if (box_overlap(P, P, lo, up, gap)) f(t);
-        }
+// The lanes of one query: sub = lane within the group, mask = the group's lanes.
+template <int G>
+struct QueryGroup {
+    int sub;
+    unsigned mask;
+    ADMM_DEV QueryGroup() {
+        const int lane = threadIdx.x & 31;
+        sub = lane % G;
+        mask = G == 32 ? ~0u : (((1u << G) - 1u) << (lane - sub));
     }
-    const int nb = g.ctr[1];
-    for (int j = sub; j < nb; j += kQueryLanes) {
-        const int t = g.big_tri[j];
-        float4 up;
-        const float4 lo = tri_box_lo(s, t, up);
-        if (box_overlap(P, P, lo, up, gap)) f(t);
+    // bits of the group's lanes with pred set, lane `sub` of the group at bit `sub`
+    ADMM_DEV unsigned ballot(bool pred) const {
+        const unsigned m = __ballot_sync(mask, pred);
+        return G == 32 ? m : (m >> ((threadIdx.x & 31) - sub)) & ((1u << G) - 1u);
+    }
+    ADMM_DEV unsigned below() const { return (1u << sub) - 1u; }
+};
+
+// Candidate partners of one group waiting for the narrow phase (2G slots in
+// shared memory; the fill n is the same in every lane of the group).
+struct GridQueue {
+    int* buf;
+    int n;
+};
+
+// Queues the partner of every lane with ok set (called by the whole group);
+// once G or more wait, hands the first G to narrow(partner, true).
+template <int G, class F>
+ADMM_DEV void grid_queue_push(const QueryGroup<G>& grp, GridQueue& q, bool ok, int partner, F& narrow) {
+    const unsigned m = grp.ballot(ok);
+    if (ok) q.buf[q.n + __popc(m & grp.below())] = partner;
+    q.n += __popc(m);
+    if (q.n >= G) {
+        __syncwarp(grp.mask);
+        const int p = q.buf[grp.sub];
+        if (grp.sub < q.n - G) q.buf[grp.sub] = q.buf[G + grp.sub];
+        __syncwarp(grp.mask);
+        q.n -= G;
+        narrow(p, true);
     }
 }
 
-// Candidate partner edges of surface edge e with box [lo, up]: grid edges with a
-// larger index (grid edge e), every big edge (grid edge e) or big edges with a
-// larger index (big edge e).
-template <class F>
-ADMM_DEV void grid_walk_ee(const DevScene& s, int e, float4 lo, float4 up, int sub, F f) {
+template <int G, class F>
+ADMM_DEV void grid_queue_drain(const QueryGroup<G>& grp, GridQueue& q, F& narrow) {
+    if (q.n == 0) return;
+    __syncwarp(grp.mask);
+    const bool valid = grp.sub < q.n;
+    const int p = valid ? q.buf[grp.sub] : 0;
+    __syncwarp(grp.mask);
+    q.n = 0;
+    narrow(p, valid);
+}
+
+// The group's walk of one query.  Vertex query (vf): position P = lo = up
+// against the triangles.  Edge query: edge e with box [lo, up] against grid
+// edges with a larger index (grid edge e), every big edge (grid edge e) or big
+// edges with a larger index (big edge e).  Grid part: the cells of the query's
+// range, or every grid element of the type when the range is too large.
+template <int G, class F>
+ADMM_DEV void grid_walk(const DevScene& s, const QueryGroup<G>& grp, bool vf, int e, float4 lo, float4 up,
+                        GridQueue& q, F& narrow) {
     const GridDev& g = s.grid;
     const float gap = s.thickness;
-    const bool small = g.mode[s.nst + e] != 0;
+    const int sub = grp.sub;
+    const unsigned gm = grp.mask;
+    const int type = vf ? 0 : 1;
+    const bool small = vf || g.mode[s.nst + e] != 0;
     if (small) {
         int3 a, b;
         grid_query_range(lo, up, gap, g.inv_c, a, b);
         if (grid_range_small(a, b)) {
             const int nc = grid_cells(a, b);
-            for (int ci = sub; ci < nc; ci += kQueryLanes) {
-                const int3 c = grid_cell_at(a, b, ci);
-                const int bk = grid_bucket(c.x, c.y, c.z, 1, g.hmask);
-                const unsigned long long key = grid_cell_key(c.x, c.y, c.z);
-                const int k1 = g.start[bk + 1];
-                const int qfirst = (c.x == a.x ? 1 : 0) | (c.y == a.y ? 2 : 0) | (c.z == a.z ? 4 : 0);
-                for (int k = g.start[bk]; k < k1; k++) {
-                    if (g.ent_key[k] != key) continue;
-                    const float4 elo = g.ent_lo[k];
-                    const int o = __float_as_int(elo.w);
-                    if (o <= e) continue;
-                    const float4 eup = g.ent_up[k];
-                    if (((qfirst | __float_as_int(eup.w)) & 7) != 7 || !box_overlap(lo, up, elo, eup, gap)) continue;
-                    f(o);
+            for (int c0 = 0; c0 < nc; c0 += G) {
+                int cnt = 0, d = 0, qfirst = 0;
+                unsigned long long key = 0ull;
+                if (c0 + sub < nc) {
+                    const int3 c = grid_cell_at(a, b, c0 + sub);
+                    const int bk = grid_bucket(c.x, c.y, c.z, type, g.hmask);
+                    d = g.start[bk];
+                    cnt = g.start[bk + 1] - d;
+                    key = grid_cell_key(c.x, c.y, c.z);
+                    qfirst = (c.x == a.x ? 1 : 0) | (c.y == a.y ? 2 : 0) | (c.z == a.z ? 4 : 0);
+                }
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < G; o <<= 1) {
+                    const int y = __shfl_up_sync(gm, incl, o, G);
+                    if (sub >= o) incl += y;
+                }
+                d -= incl - cnt;  // entry number k of the round lies at d of its cell + k
+                const int tot = __shfl_sync(gm, incl, G - 1, G);
+                for (int k0 = 0; k0 < tot; k0 += G) {
+                    const int k = k0 + sub;
+                    // the cell of entry k: the first lane of the group whose inclusive count exceeds k
+                    int j = 0;
+#pragma unroll
+                    for (int st = G / 2; st >= 1; st >>= 1) {
+                        if (__shfl_sync(gm, incl, j + st - 1, G) <= k) j += st;
+                    }
+                    const int dj = __shfl_sync(gm, d, j, G);
+                    const int fj = __shfl_sync(gm, qfirst, j, G);
+                    const unsigned long long kj = __shfl_sync(gm, key, j, G);
+                    bool ok = false;
+                    int partner = 0;
+                    if (k < tot) {
+                        const int ent = dj + k;
+                        const unsigned long long ek = g.ent_key[ent];
+                        const float4 eup = g.ent_up[ent];
+                        const float4 elo = g.ent_lo[ent];
+                        partner = __float_as_int(elo.w);
+                        // same cell (not another of the bucket); larger edge index; once per pair:
+                        // this cell is the first of the query's or of the element's range on every axis
+                        ok = ek == kj && (vf || partner > e) && ((fj | __float_as_int(eup.w)) & 7) == 7 &&
+                             box_overlap(lo, up, elo, eup, gap);
+                    }
+                    grid_queue_push(grp, q, ok, partner, narrow);
                 }
             }
         } else {
-            for (int o = e + 1 + sub; o < s.nse; o += kQueryLanes) {
-                if (!g.mode[s.nst + o]) continue;
-                float4 oup;
-                const float4 olo = edge_box_lo(s, o, oup);
-                if (box_overlap(lo, up, olo, oup, gap)) f(o);
+            const int n = vf ? s.nst : s.nse;
+            for (int t0 = vf ? 0 : e + 1; t0 < n; t0 += G) {
+                const int t = t0 + sub;
+                bool ok = false;
+                if (t < n && g.mode[vf ? t : s.nst + t]) {
+                    float4 eup;
+                    const float4 elo = vf ? tri_box_lo(s, t, eup) : edge_box_lo(s, t, eup);
+                    ok = box_overlap(lo, up, elo, eup, gap);
+                }
+                grid_queue_push(grp, q, ok, t, narrow);
             }
         }
     }
-    const int nb = g.ctr[2];
-    for (int j = sub; j < nb; j += kQueryLanes) {
-        const int o = g.big_edge[j];
-        if (o == e || (!small && o < e)) continue;
-        float4 oup;
-        const float4 olo = edge_box_lo(s, o, oup);
-        if (box_overlap(lo, up, olo, oup, gap)) f(o);  // the overlap rule is symmetric
+    const int nb = g.ctr[1 + type];
+    for (int j0 = 0; j0 < nb; j0 += G) {
+        const int j = j0 + sub;
+        bool ok = false;
+        int o = 0;
+        if (j < nb) {
+            o = vf ? g.big_tri[j] : g.big_edge[j];
+            if (vf || (o != e && (small || o > e))) {
+                float4 oup;
+                const float4 olo = vf ? tri_box_lo(s, o, oup) : edge_box_lo(s, o, oup);
+                ok = box_overlap(lo, up, olo, oup, gap);  // the overlap rule is symmetric
+            }
+        }
+        grid_queue_push(grp, q, ok, o, narrow);
     }
+    grid_queue_drain(grp, q, narrow);
 }
 
 // ---------------------------------------------------------------------------
@@ -431,80 +496,78 @@ ADMM_DEV bool grid_hit_ee(const DevScene& s, int e, int o, int4& ids, NpResult& 
     return narrow_ee(p0, p1, q0, q1, r) && r.dist < s.thickness && r.dist >= 0.f;
 }
 
-// Count (WRITE = false: qcount) or write (WRITE = true: at qoff, then sorted by
-// partner) the pairs of every query: surface vertices first, then edges.
-template <bool WRITE>
-__global__ void __launch_bounds__(128) k_grid_query(DevScene s) {
+// Count (WRITE = false) or write (WRITE = true) the pairs of every query, G
+// lanes per query: surface vertices first, then edges.  The count pass stores
+// the query's pair count in qcount and up to kQueryHitsMax partners in qhits.
+// The write pass places each recorded partner at qoff + its rank among the
+// query's partners, so the segment comes out sorted by partner; a query with
+// more partners than were recorded walks the grid again, writes in walk order
+// and sorts its segment.
+template <bool WRITE, int G>
+__global__ void __launch_bounds__(kQueryThreads) k_grid_query(DevScene s) {
     ADMM_PDL_PROLOGUE();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int q = t / kQueryLanes, sub = t % kQueryLanes;
+    __shared__ int qbuf[kQueryThreads * 2];
+    const QueryGroup<G> grp;
+    const int q = (blockIdx.x * kQueryThreads + threadIdx.x) / G;
     if (q >= s.nsv + s.nse) return;  // whole groups leave together
-    const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kQueryLanes - 1));
     const bool vf = q < s.nsv;
     const int e = q - s.nsv;
     int v = 0;
-    float4 P = f4(0.f, 0.f, 0.f), lo = P, up = P;
+    float4 lo, up;
     if (vf) {
         v = s.sv[q];
-        P = s.x[v];
+        lo = up = s.x[v];
     } else {
         lo = edge_box_lo(s, e, up);
     }
-    // Count pass: walk the grid, record up to kQueryHits partners per lane in
-    // qhits and the lane's hit count in qlane.  Write pass: take the recorded
-    // partners (the walk again only for a lane with more hits).
-    int* my_hits = s.grid.qhits + (size_t)t * kQueryHits;
-    int n = 0;
+    GridQueue gq{qbuf + 2 * (threadIdx.x - grp.sub), 0};
+    int* qh = s.grid.qhits + (size_t)q * kQueryHitsMax;
+    int nhit = 0;  // the same in every lane of the group
     if (!WRITE) {
-        auto consider = [&](int partner) {
+        auto narrow = [&](int partner, bool valid) {
             int4 ids;
             NpResult r;
-            if (vf ? grid_hit_vf(s, v, P, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r)) {
-                if (n < kQueryHits) my_hits[n] = partner;
-                n++;
-            }
+            const bool hit = valid && (vf ? grid_hit_vf(s, v, lo, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r));
+            const unsigned m = grp.ballot(hit);
+            const int k = nhit + __popc(m & grp.below());
+            if (hit && k < kQueryHitsMax) qh[k] = partner;
+            nhit += __popc(m);
         };
-        if (vf) grid_walk_vf(s, P, sub, consider);
-        else grid_walk_ee(s, e, lo, up, sub, consider);
-        s.grid.qlane[t] = n;
-    } else {
-        n = s.grid.qlane[t];
-    }
-    // group sum / exclusive prefix of the lane counts
-    int incl = n;
-#pragma unroll
-    for (int o = 1; o < kQueryLanes; o <<= 1) {
-        const int y = __shfl_up_sync(gmask, incl, o, kQueryLanes);
-        if (sub >= o) incl += y;
-    }
-    const int total = __shfl_sync(gmask, incl, kQueryLanes - 1, kQueryLanes);
-    if (!WRITE) {
-        if (sub == 0) s.qcount[q] = total;
+        grid_walk(s, grp, vf, e, lo, up, gq, narrow);
+        if (grp.sub == 0) s.qcount[q] = nhit;
         return;
     }
+    const int total = s.qcount[q];
+    if (total == 0) return;
     const int base = s.qoff[q];
-    int slot = base + incl - n;
-    auto emit = [&](int partner) {
+    if (total <= kQueryHitsMax) {
+        for (int k = grp.sub; k < total; k += G) {
+            const int partner = qh[k];
+            int rank = 0;
+            for (int j = 0; j < total; j++) rank += qh[j] < partner ? 1 : 0;
+            int4 ids;
+            NpResult r;
+            const bool hit = vf ? grid_hit_vf(s, v, lo, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r);
+            const int slot = base + rank;
+            if (hit && slot < s.cap) write_contact(s, slot, ids, r, !vf);
+        }
+        return;
+    }
+    auto emit = [&](int partner, bool valid) {
         int4 ids;
         NpResult r;
-        const bool hit = vf ? grid_hit_vf(s, v, P, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r);
-        if (hit) {
-            if (slot < s.cap) {
-                write_contact(s, slot, ids, r, !vf);
-                s.grid.qkey[slot] = partner;
-            }
-            slot++;
+        const bool hit = valid && (vf ? grid_hit_vf(s, v, lo, partner, ids, r) : grid_hit_ee(s, e, partner, ids, r));
+        const unsigned m = grp.ballot(hit);
+        const int slot = base + nhit + __popc(m & grp.below());
+        if (hit && slot < s.cap) {
+            write_contact(s, slot, ids, r, !vf);
+            s.grid.qkey[slot] = partner;
         }
+        nhit += __popc(m);
     };
-    if (n <= kQueryHits) {
-        for (int k = 0; k < n; k++) emit(my_hits[k]);
-    } else if (vf) {
-        grid_walk_vf(s, P, sub, emit);
-    } else {
-        grid_walk_ee(s, e, lo, up, sub, emit);
-    }
-    __syncwarp(gmask);
-    if (sub == 0) {
+    grid_walk(s, grp, vf, e, lo, up, gq, emit);
+    __syncwarp(grp.mask);
+    if (grp.sub == 0) {
         const int end = min(base + total, s.cap);
         if (end - base > 1) grid_sort_segment(s, base, end);
     }

@@ -73,8 +73,7 @@ struct GridDev {
     int* big_edge = nullptr;       // [n surface edges]
     int* mode = nullptr;           // [triangles + edges] 1 = in the grid, 0 = big list
     int* qkey = nullptr;           // [contact capacity] partner index per contact slot
-    int* qhits = nullptr;          // [queries * lanes * hits] partners found by the count pass
-    int* qlane = nullptr;          // [queries * lanes] hits per lane
+    int* qhits = nullptr;          // [queries * kQueryHitsMax] partners found by the count pass
 };
 
 struct DevScene {

@@ -63,6 +63,7 @@ class SolverParams:
     broad_phase: int = 0  # 0 default (grid), 1 LBVH, 2 uniform grid
     global_solver: int = 0  # 0 Jacobi (reference), 1 PCG with diag(A), 2 PCG with learned blocks
     pcg_iter: int = 0  # 0 = jacobi_iter // 2
+    query_lanes: int = 0  # lanes per grid DCD query: 0 chosen from the query count, or 8, 16, 32
 
 
 @dataclasses.dataclass

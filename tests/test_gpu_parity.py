@@ -99,10 +99,15 @@ def _pairset(pairs, canon=True):
     return out
 
 
-@pytest.mark.parametrize("broad", [1, 2], ids=["lbvh", "grid"])
-@pytest.mark.parametrize("case", ["cloth_fold", "cube_squeezed", "cloth_flat_on_box"])
-def test_dcd_pairs_bitexact(case, broad):
-    from oracle import oracle as O
+def _dcd_case(case):
+    if case == "layers_stack":
+        # 40 small sheets stacked within one thickness: every query has dozens of
+        # partners (more than the count pass records, so the write pass walks again)
+        v, f = scene.grid_cloth(6, 0.1)
+        bodies = [scene._Body(v + np.array([0.0, 0.5 + 1e-4 * l, 0.0]), f, np.zeros((0, 4), np.int32),
+                              0.1, 1e3, 1e-3) for l in range(40)]
+        sc = scene.assemble("stack", bodies, [], scene.SolverParams(thickness=5e-3, max_contacts=1_000_000))
+        return sc, np.ascontiguousarray(sc.verts, np.float32)
     if case == "cloth_fold":
         sc, x = _crumpled_cloth()
     elif case == "cube_squeezed":
@@ -116,8 +121,17 @@ def test_dcd_pairs_bitexact(case, broad):
         sc = scene.cloth_on_box(32)
         x = sc.verts.copy()
         x[:sc.n_dyn, 1] = 0.5 + 0.5 * sc.params.thickness  # lying on the box top
-    x = np.ascontiguousarray(x, np.float32)
+    return sc, np.ascontiguousarray(x, np.float32)
+
+
+@pytest.mark.parametrize("broad,lanes", [(1, 0), (2, 8), (2, 16), (2, 32)],
+                         ids=["lbvh", "grid8", "grid16", "grid32"])
+@pytest.mark.parametrize("case", ["cloth_fold", "cube_squeezed", "cloth_flat_on_box", "layers_stack"])
+def test_dcd_pairs_bitexact(case, broad, lanes):
+    from oracle import oracle as O
+    sc, x = _dcd_case(case)
     sc.params.broad_phase = broad
+    sc.params.query_lanes = lanes
     h = B.Handle(sc)
     n = h.detect(x)
     ref_pairs, _ = O.dcd(x, sc.surf_verts, sc.surf_tris, sc.surf_edges, sc.params.thickness)
@@ -126,6 +140,24 @@ def test_dcd_pairs_bitexact(case, broad):
     got = h.contacts()
     # identical multisets (a point-triangle tuple can equal an edge-edge tuple)
     assert sorted(map(tuple, got["pairs"].tolist())) == sorted(map(tuple, ref_pairs.tolist()))
+
+
+@pytest.mark.parametrize("case", ["cloth_fold", "cube_squeezed", "layers_stack"])
+def test_grid_query_lanes_same_contact_list(case):
+    """The lanes per grid query change only the schedule: the contact list (queries in order,
+    each query's partners ascending) and every contact field are identical bit for bit."""
+    sc, x = _dcd_case(case)
+    sc.params.broad_phase = 2
+    out = []
+    for lanes in (8, 16, 32):
+        sc.params.query_lanes = lanes
+        h = B.Handle(sc)
+        assert h.detect(x) > 0
+        out.append(h.contacts())
+        h.close()
+    for other in out[1:]:
+        for k in out[0]:
+            assert np.array_equal(out[0][k], other[k]), k
 
 
 def test_contact_conversion_and_step_parity():
