@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define ADMM_B200_ABI_VERSION 3
+#define ADMM_B200_ABI_VERSION 4
 
 /* status codes */
 #define ADMM_OK                    0
@@ -135,6 +135,14 @@ typedef struct AdmmB200Desc {
      * four waves of the device (a latency-bound detection), else 16 or 8 (a
      * throughput-bound one).  All give the same contact list. */
     int32_t query_lanes;
+    /* Contact predicates: 0 = the GPU backend's (dcdPT / dcdEE of dist_g.cuh:
+     * interior closest points only, 0 <= d < thickness); 1 = the CPU backend's
+     * ProximalQuery (narrow_phase.cpp:192-469: no pair of two static elements,
+     * point-triangle at any closest point with d <= thickness, edge-edge with
+     * d < thickness unless both closest points are segment end points, closest
+     * points by Eberly's queries of distPT.h / distEE.h).  1 uses the grid broad
+     * phase whatever broad_phase says. */
+    int32_t contact_semantics;
 } AdmmB200Desc;
 
 /* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */
@@ -181,6 +189,23 @@ int  admm_b200_reset(AdmmB200* h);
 /* Device pointers of the handle's row-major float4 state (x, v), for callers
  * that keep data on the GPU; valid until destroy. */
 int  admm_b200_device_state(AdmmB200* h, void** x_float4, void** v_float4);
+
+/* --- scripted static meshes (ScriptAnimator, src/solver/animator.cpp:9-204; applied at the
+ * start of every substep as ADMMImplGPU::step does, admm_impl_gpu.cu:265-270) ---
+ * Vertices [v_begin, v_end) of one static mesh (all >= n_dyn) follow a track.  Tracks are
+ * applied in the order they are attached (attach them in mesh-id order, as the reference's
+ * std::map does) and share the reference's frame counter: every substep advances it by one,
+ * and a rigid track by one more before it reads its frame.  A rigid track places the rest
+ * positions at pos[f] + quat[f] * rest (quat as x, y, z, w); a point track at
+ * translate + rot9 * (scale * points[f]) (rot9 row-major).  Velocities are (new - old) / dt,
+ * zero once a track has run past its last frame (which it then holds).  Attaching (and
+ * admm_b200_reset) restarts the counter and places the meshes at their first frame with zero
+ * velocity, as ADMMImplGPU::init does.  A rigid track needs at least 3 frames. */
+int  admm_b200_set_rigid_track(AdmmB200* h, int32_t v_begin, int32_t v_end, int32_t n_frames,
+                               const float* pos3, const float* quat4_xyzw);
+int  admm_b200_set_point_track(AdmmB200* h, int32_t v_begin, int32_t v_end, int32_t n_frames,
+                               const float* points3, const float* rot9, const float* translate3, float scale);
+int  admm_b200_clear_tracks(AdmmB200* h);
 
 /* --- ADMM internals, for parity tests and the fused dual/local step --- */
 

@@ -21,7 +21,7 @@ from .scene import Scene
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libadmm_b200.so")
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 OK = 0
 ERR_INVALID = -1
 ERR_CUDA = -2
@@ -74,6 +74,7 @@ class AdmmB200Desc(ctypes.Structure):
         ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32), ("jacobi_mode", ctypes.c_int32),
         ("broad_phase", ctypes.c_int32), ("global_solver", ctypes.c_int32), ("pcg_iter", ctypes.c_int32),
         ("vert_mu", ctypes.POINTER(ctypes.c_float)), ("query_lanes", ctypes.c_int32),
+        ("contact_semantics", ctypes.c_int32),
     ]
 
 
@@ -141,6 +142,7 @@ class DescHolder:
         d.global_solver = int(p.global_solver)
         d.pcg_iter = int(p.pcg_iter)
         d.query_lanes = int(getattr(p, "query_lanes", 0))
+        d.contact_semantics = int(getattr(p, "contact_semantics", 0))
         vm = getattr(sc, "vert_mu", None)
         d.vert_mu = arr("vm", vm, np.float32) if vm is not None else None
         for k, v in overrides.items():
@@ -197,6 +199,10 @@ def lib():
             "admm_b200_tuning": (ctypes.c_int, [vp, _i, _i, _f, _f]),
             "admm_b200_global_mode": (ctypes.c_int, [vp, _i, _i, _f, _f]),
             "admm_b200_set_preconditioner": (ctypes.c_int, [vp, _f, ctypes.c_int]),
+            "admm_b200_set_rigid_track": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _f, _f]),
+            "admm_b200_set_point_track": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _f, _f,
+                                                         _f, ctypes.c_float]),
+            "admm_b200_clear_tracks": (ctypes.c_int, [vp]),
             "admm_b200_jacobi_noalloc": (ctypes.c_int, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int,
                                                         vp]),
         }
@@ -221,6 +227,7 @@ def exported_symbols():
         "admm_b200_set_profiling", "admm_b200_kernels_per_step", "admm_b200_step_host",
         "admm_b200_phase_times", "admm_b200_set_probe", "admm_b200_probe_time", "admm_b200_tuning",
         "admm_b200_jacobi_noalloc", "admm_b200_global_mode", "admm_b200_set_preconditioner",
+        "admm_b200_set_rigid_track", "admm_b200_set_point_track", "admm_b200_clear_tracks",
         "admm_b200_system", "admm_gnn_create", "admm_gnn_set_graph", "admm_gnn_destroy", "admm_gnn_num_params",
         "admm_gnn_set_params", "admm_gnn_get_params", "admm_gnn_forward", "admm_gnn_loss_grad", "admm_gnn_adam",
     ]
@@ -396,6 +403,27 @@ class Handle:
         """Per-vertex 3x3 blocks (n_dyn x 9 or n_dyn x 3 x 3) for global_solver 2."""
         blk = np.ascontiguousarray(blocks, np.float32).reshape(self.n_dyn, 9)
         self.check(lib().admm_b200_set_preconditioner(self.h, _p(blk), self.n_dyn), "set_preconditioner")
+
+    def set_rigid_track(self, v_begin: int, v_end: int, pos: np.ndarray, quat_xyzw: np.ndarray):
+        """Static vertices [v_begin, v_end) follow pos[f] + quat[f] * rest (one row per frame)."""
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        quat = np.ascontiguousarray(quat_xyzw, np.float32).reshape(-1, 4)
+        if len(pos) != len(quat):
+            raise ValueError("pos and quat need one row per frame")
+        self.check(lib().admm_b200_set_rigid_track(self.h, v_begin, v_end, len(pos), _p(pos), _p(quat)),
+                   "set_rigid_track")
+
+    def set_point_track(self, v_begin: int, v_end: int, points: np.ndarray, rot: np.ndarray,
+                        translate: np.ndarray, scale: float):
+        """Static vertices [v_begin, v_end) follow translate + rot (scale * points[f])."""
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, v_end - v_begin, 3)
+        r = np.ascontiguousarray(rot, np.float32).reshape(9)
+        t = np.ascontiguousarray(translate, np.float32).reshape(3)
+        self.check(lib().admm_b200_set_point_track(self.h, v_begin, v_end, len(pts), _p(pts), _p(r), _p(t),
+                                                   float(scale)), "set_point_track")
+
+    def clear_tracks(self):
+        self.check(lib().admm_b200_clear_tracks(self.h), "clear_tracks")
 
     def global_mode(self) -> Dict[str, float]:
         """Global-step mode: persistent kernel (and its grid) or one kernel per sweep."""

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "admm_b200.h"
+#include "animate.cuh"
 #include "contact.cuh"
 #include "grid.cuh"
 #include "kernels.cuh"
@@ -34,6 +35,9 @@ struct AdmmB200 {
     DevScene s;
     std::vector<void*> allocs;
     std::string last_error;
+    // scripted static meshes
+    std::vector<TrackDev> tracks;   // host copies of the track records (device pointers inside)
+    AnimDev anim;
     // scene scalars
     int admm_max_iter = 0, dcd_interval = 1, gs_iter = 0, jac_iter = 0;
     int tet_blocks = 0, tri_blocks = 0, bend_blocks = 0, pin_blocks = 0;
@@ -835,6 +839,10 @@ void enqueue_iteration(AdmmB200* h, int it, bool first, bool residual) {
 void enqueue_step_begin(AdmmB200* h) {
     DevScene& s = h->s;
     set_phase(h, ADMM_PHASE_PRE);
+    if (h->anim.n_tracks > 0) {
+        LAUNCH(k_anim_advance, 1, 32, h->anim, 0);
+        LAUNCH(k_animate, blocks(h->anim.n_verts, kVertThreads), kVertThreads, s, h->anim);
+    }
     LAUNCH(k_pre_integration, blocks(s.n, kVertThreads), kVertThreads, s);
     if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->cstream);
     if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->cstream);
@@ -915,10 +923,7 @@ int enqueue_step_tol(AdmmB200* h, float tol) {
 // One substep (ADMMImplGPU::step).  The residual of the last iteration is kept.
 void enqueue_step(AdmmB200* h) {
     DevScene& s = h->s;
-    set_phase(h, ADMM_PHASE_PRE);
-    LAUNCH(k_pre_integration, blocks(s.n, kVertThreads), kVertThreads, s);
-    if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->cstream);
-    if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->cstream);
+    enqueue_step_begin(h);
     for (int it = 0; it < h->admm_max_iter; it++) enqueue_iteration(h, it, it == 0, it == h->admm_max_iter - 1);
     if (h->admm_max_iter > 0) enqueue_local(h, LOCAL_DUAL);
     set_phase(h, ADMM_PHASE_FINAL);
@@ -1107,6 +1112,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     if (d->enable_contact && d->max_contacts <= 0) return fail(h, ADMM_ERR_INVALID, "max_contacts");
     if (d->query_lanes != 0 && d->query_lanes != 8 && d->query_lanes != 16 && d->query_lanes != 32)
         return fail(h, ADMM_ERR_INVALID, "query_lanes");
+    if (d->contact_semantics != 0 && d->contact_semantics != 1) return fail(h, ADMM_ERR_INVALID, "contact_semantics");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
         return fail(h, ADMM_ERR_NO_DEVICE, "no CUDA device");
@@ -1300,7 +1306,8 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     const int hist_n = 256 * sort_tiles(std::max(h->sort_max, 1));
     TRY(dalloc(h, &h->hist, hist_n));
     if (d->broad_phase < 0 || d->broad_phase > 2) return fail(h, ADMM_ERR_INVALID, "broad_phase must be 0, 1 or 2");
-    h->use_grid = d->broad_phase != 1;
+    s.cpu_contact = d->contact_semantics == 1 ? 1 : 0;
+    h->use_grid = d->broad_phase != 1 || s.cpu_contact;  // the CPU predicates run on the grid
 
     TRY(setup_grid(h, d));
     const int scan_n = std::max(std::max(std::max(scan_tiles(hist_n), scan_tiles(n + 1)), scan_tiles(s.nsv + s.nse + 1)),
@@ -1449,6 +1456,58 @@ int read_err_flags(AdmmB200* h, int* status) {
 }  // namespace
 
 // ================================ C ABI =====================================
+// Scripted static meshes: publish the track records to the device, place the
+// meshes at their first frame (the animate_all of ADMMImplGPU::init / reset)
+// and drop the step graph, which holds the track count.
+int anim_publish(AdmmB200* h) {
+    AnimDev& a = h->anim;
+    if (!a.tracks) {
+        TRY(dalloc(h, &a.tracks, kMaxTracks));
+        TRY(dalloc(h, &a.counter, 1));
+        TRY(dalloc(h, &a.frame, kMaxTracks));
+        TRY(dalloc(h, &a.moving, kMaxTracks));
+    }
+    int first = 0;
+    for (auto& t : h->tracks) {
+        t.first = first;
+        first += t.v1 - t.v0;
+    }
+    a.n_tracks = (int)h->tracks.size();
+    a.n_verts = first;
+    if (a.n_tracks)
+        CK(cudaMemcpy(a.tracks, h->tracks.data(), sizeof(TrackDev) * h->tracks.size(), cudaMemcpyHostToDevice));
+    if (h->step_exec) {
+        cudaGraphExecDestroy(h->step_exec);
+        h->step_exec = nullptr;
+    }
+    return ADMM_OK;
+}
+
+int anim_init(AdmmB200* h) {
+    if (h->anim.n_tracks == 0) return ADMM_OK;
+    h->cstream = h->stream;
+    LAUNCH(k_anim_advance, 1, 32, h->anim, 1);
+    LAUNCH(k_animate, blocks(h->anim.n_verts, kVertThreads), kVertThreads, h->s, h->anim);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    return ADMM_OK;
+}
+
+int add_track(AdmmB200* h, TrackDev t) {
+    if ((int)h->tracks.size() >= kMaxTracks) return fail(h, ADMM_ERR_INVALID, "too many tracks");
+    for (const auto& o : h->tracks)
+        if (t.v0 < o.v1 && o.v0 < t.v1) return fail(h, ADMM_ERR_INVALID, "track vertex ranges overlap");
+    h->tracks.push_back(t);
+    TRY(anim_publish(h));
+    return anim_init(h);
+}
+
+int check_track_range(AdmmB200* h, int v0, int v1, int n_frames) {
+    if (v0 < h->s.nd || v1 > h->s.n || v0 >= v1) return fail(h, ADMM_ERR_INVALID, "track range must be static vertices");
+    if (n_frames < 1) return fail(h, ADMM_ERR_INVALID, "n_frames");
+    return ADMM_OK;
+}
+
 extern "C" {
 
 const char* admm_b200_errstr(int code) {
@@ -1609,7 +1668,72 @@ int admm_b200_reset(AdmmB200* h) {
     CK(cudaMemset(s.err, 0, sizeof(int) * 4));
     h->frame = 0;
     h->peak = 0;
-    return upload_state(h, h->x_init, h->v_init);
+    TRY(upload_state(h, h->x_init, h->v_init));
+    return anim_init(h);
+}
+
+int admm_b200_set_rigid_track(AdmmB200* h, int32_t v0, int32_t v1, int32_t n_frames, const float* pos,
+                              const float* quat) {
+    if (!h || !pos || !quat) return ADMM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    TRY(check_track_range(h, v0, v1, n_frames));
+    if (n_frames < 3) return fail(h, ADMM_ERR_INVALID, "a rigid track needs at least 3 frames");
+    std::vector<float4> p(n_frames), q(n_frames), rest(h->x_init.begin() + v0, h->x_init.begin() + v1);
+    for (int f = 0; f < n_frames; f++) {
+        p[f] = make_float4(pos[3 * f], pos[3 * f + 1], pos[3 * f + 2], 0.f);
+        q[f] = make_float4(quat[4 * f], quat[4 * f + 1], quat[4 * f + 2], quat[4 * f + 3]);
+    }
+    TrackDev t;
+    t.kind = 0;
+    t.v0 = v0;
+    t.v1 = v1;
+    t.n_frames = n_frames;
+    float4 *dp, *dq, *dr;
+    TRY(dupload(h, &dp, p.data(), p.size()));
+    TRY(dupload(h, &dq, q.data(), q.size()));
+    TRY(dupload(h, &dr, rest.data(), rest.size()));
+    t.pos = dp;
+    t.quat = dq;
+    t.rest = dr;
+    return add_track(h, t);
+}
+
+int admm_b200_set_point_track(AdmmB200* h, int32_t v0, int32_t v1, int32_t n_frames, const float* points,
+                              const float* rot9, const float* translate3, float scale) {
+    if (!h || !points || !rot9 || !translate3) return ADMM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    TRY(check_track_range(h, v0, v1, n_frames));
+    const size_t nv = (size_t)(v1 - v0);
+    std::vector<float4> pts(nv * (size_t)n_frames);
+    for (size_t k = 0; k < pts.size(); k++) pts[k] = make_float4(points[3 * k], points[3 * k + 1], points[3 * k + 2], 0.f);
+    TrackDev t;
+    t.kind = 1;
+    t.v0 = v0;
+    t.v1 = v1;
+    t.n_frames = n_frames;
+    for (int k = 0; k < 9; k++) t.rot[k] = rot9[k];
+    for (int k = 0; k < 3; k++) t.trans[k] = translate3[k];
+    t.scale = scale;
+    float4* dp;
+    TRY(dupload(h, &dp, pts.data(), pts.size()));
+    t.pts = dp;
+    return add_track(h, t);
+}
+
+int admm_b200_clear_tracks(AdmmB200* h) {
+    if (!h) return ADMM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    for (auto& t : h->tracks) {
+        dfree(h, const_cast<float4*>(t.pos));
+        dfree(h, const_cast<float4*>(t.quat));
+        dfree(h, const_cast<float4*>(t.rest));
+        dfree(h, const_cast<float4*>(t.pts));
+    }
+    h->tracks.clear();
+    return anim_publish(h);
 }
 
 int admm_b200_device_state(AdmmB200* h, void** x, void** v) {

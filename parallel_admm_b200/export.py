@@ -165,6 +165,9 @@ def run_scene(path: str, resource_root: Optional[str] = None, frames: Optional[i
         cfg.export_obj = export_obj
     sc = C.load_scene(path, resource_root, cfg)
     h = B.Handle(sc)
+    tracks = C.scene_tracks(cfg, sc, resource_root, path)
+    if tracks:
+        C.attach_tracks(h, tracks)
     r = Runner(h, cfg, sc, out_path)
     return r.run(frames), h
 

@@ -35,9 +35,9 @@ Parsed and kept in :class:`AppConfig` but not used by the substep (as in the ref
 backend): strain limits (``k.use_limit``; the GPU prox ignores them), damping outside the
 heuristic weights (``m_Damp_Mat`` is not part of A on the GPU path), ``use_CCD``, ``unique``,
 ``coloring``, ``use_Jacobi``, broad-phase radius and strategy, plane colliders (used by the
-CPU solver's nodal obstacle constraints), viewer and output settings.  Kinematic static meshes
-(``animate``) are recorded in :attr:`MeshSpec.animate`; the substep treats static meshes as
-fixed.
+CPU solver's nodal obstacle constraints), viewer and output settings.  Scripted static meshes
+(``animate``): :func:`scene_tracks` reads their ``.npz`` tracks (``animator.cpp:9-79``) and
+:func:`attach_tracks` hands them to the backend, which moves them on the device.
 
 Vertex transforms are computed in float64 and rounded to float32 once (the reference rounds
 after every float32 operation), so positions can differ from the reference's by an ulp.
@@ -596,3 +596,68 @@ def load_scene(path: str, resource_root: Optional[str] = None, cfg: Optional[App
     if cfg.contact_enable and cfg.use_heu_wc:
         sc.contact_w = heuristic_contact_weights(sc, h, cfg.damp_kl, cfg.damp_km, cfg.wc_sigma, cfg.wc_beta)
     return sc
+
+
+# ----------------------------------------------------------------------------
+# scripted static meshes (ScriptAnimator)
+# ----------------------------------------------------------------------------
+
+def read_track(path: str) -> Dict[str, np.ndarray]:
+    """A track file (animator.cpp:9-63): a path containing "sequence" holds per-vertex
+    positions ``points`` [frames x vertices x 3]; any other holds a rigid motion ``pos``
+    [frames x 3] and ``quat`` [frames x 4] (x, y, z, w).  Values are converted to float32 (the
+    reference reinterprets the stored bytes as float32, which garbles float64 files such as its
+    own tracks; the values are what the files mean)."""
+    with np.load(path) as d:
+        if "sequence" in path:
+            if "points" not in d.files:
+                raise ValueError(f"{path}: no 'points' array")
+            pts = np.asarray(d["points"], np.float64)
+            if pts.ndim != 3 or pts.shape[2] != 3:
+                raise ValueError(f"{path}: 'points' must be frames x vertices x 3")
+            return {"kind": "points", "points": pts.astype(np.float32)}
+        if "pos" not in d.files or "quat" not in d.files:
+            raise ValueError(f"{path}: rigid track needs 'pos' and 'quat'")
+        pos = np.asarray(d["pos"], np.float64)
+        quat = np.asarray(d["quat"], np.float64)
+    if pos.ndim != 2 or pos.shape[1] != 3 or quat.ndim != 2 or quat.shape[1] != 4 or len(pos) != len(quat):
+        raise ValueError(f"{path}: 'pos' must be frames x 3 and 'quat' frames x 4")
+    if len(pos) < 3:
+        raise ValueError(f"{path}: a rigid track needs at least 3 frames")
+    return {"kind": "rigid", "pos": pos.astype(np.float32), "quat": quat.astype(np.float32)}
+
+
+def scene_tracks(cfg: AppConfig, sc: S.Scene, resource_root: Optional[str] = None,
+                 scene_path: Optional[str] = None) -> List[dict]:
+    """Tracks of the animated static meshes of a loaded scene, in mesh-id order (the order the
+    reference's animator applies them), with their vertex ranges and mesh transforms."""
+    if resource_root is None:
+        base = scene_path or sc.meta.get("path", "")
+        resource_root = os.path.dirname(os.path.dirname(os.path.abspath(base)))
+    order = [m for m in cfg.meshes if m.type in ("tri", "tet")] + [m for m in cfg.meshes if m.type == "static"]
+    meshes = sc.meta.get("meshes")
+    if meshes is None or len(meshes) != len(order):
+        raise ValueError("scene was not loaded from this scene file")
+    out = []
+    for mesh_id, spec in enumerate(order):
+        if spec.type != "static" or not spec.animate:
+            continue
+        tr = read_track(os.path.join(resource_root, spec.animate))
+        m = meshes[mesh_id]
+        tr.update(v_begin=m["start"], v_end=m["end"], mesh_id=mesh_id,
+                  rot=rotation(spec.rotate), translate=np.asarray(spec.translate, np.float64), scale=spec.scale)
+        if tr["kind"] == "points" and tr["points"].shape[1] != m["end"] - m["start"]:
+            raise ValueError(f"{spec.animate}: {tr['points'].shape[1]} points for a mesh of "
+                             f"{m['end'] - m['start']} vertices")
+        out.append(tr)
+    return out
+
+
+def attach_tracks(handle, tracks: Sequence[dict]) -> None:
+    """Attach the tracks to a backend handle (replacing any it had)."""
+    handle.clear_tracks()
+    for tr in tracks:
+        if tr["kind"] == "rigid":
+            handle.set_rigid_track(tr["v_begin"], tr["v_end"], tr["pos"], tr["quat"])
+        else:
+            handle.set_point_track(tr["v_begin"], tr["v_end"], tr["points"], tr["rot"], tr["translate"], tr["scale"])

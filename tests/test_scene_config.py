@@ -175,7 +175,7 @@ def write_msh22(path, V, T, binary):
         f.write(b"$EndElements\n")
 
 
-def _write_scene(root, static_pin):
+def _write_scene(root, static_pin, animate=""):
     os.makedirs(os.path.join(root, "meshes"), exist_ok=True)
     os.makedirs(os.path.join(root, "scene"), exist_ok=True)
     cv, cf = S.grid_cloth(6, 0.4)
@@ -186,8 +186,66 @@ def _write_scene(root, static_pin):
     write_msh41(os.path.join(root, "meshes", "cube.msh"), tv, tt)
     path = os.path.join(root, "scene", "unit.toml")
     with open(path, "w") as f:
-        f.write(SCENE.format(static_pin=static_pin))
+        f.write(SCENE.format(static_pin=static_pin).replace('animate = ""', f'animate = "{animate}"'))
     return path, (cv, cf), (bv, bf), (tv, tt)
+
+
+class AnimatorRef:
+    """Restatement of the reference's animator (animator.cpp:81-204) for the tests: the shared
+    frame counter (one step per animate_all, one more per rigid track), the clamp at the last
+    frame, rigid motion pos[f] + q[f] * rest and point tracks t + R (s * points[f]), velocities
+    (new - old) / dt, zero at init and past the end."""
+
+    def __init__(self, tracks, rest, dt):
+        self.tracks, self.rest, self.dt = tracks, np.asarray(rest, np.float64), dt
+        self.c = -1
+
+    def frames(self, init):
+        c = (-1 if init else self.c) + 1
+        out = []
+        for tr in self.tracks:
+            n = len(tr["pos"]) if tr["kind"] == "rigid" else len(tr["points"])
+            if tr["kind"] == "rigid":
+                c += 1
+            if c >= n:
+                c = n
+                out.append((n - 1, False))
+            else:
+                out.append((c - 1 if tr["kind"] == "rigid" else c, not init))
+        self.c = c
+        return out
+
+    @staticmethod
+    def rotate(q, v):
+        q = np.asarray(q, np.float64)
+        u = 2.0 * np.cross(q[:3], v)
+        return v + q[3] * u + np.cross(q[:3], u)
+
+    def apply(self, x0, v, init=False):
+        for tr, (f, moving) in zip(self.tracks, self.frames(init)):
+            a, b = tr["v_begin"], tr["v_end"]
+            if tr["kind"] == "rigid":
+                new = tr["pos"][f].astype(np.float64) + self.rotate(tr["quat"][f], self.rest[a:b])
+            else:
+                new = tr["translate"] + (tr["scale"] * tr["points"][f].astype(np.float64)) @ tr["rot"].T
+            v[a:b] = (new - x0[a:b]) / self.dt if moving else 0.0
+            x0[a:b] = new
+
+
+def spin_track(n_frames=40, dt=0.01):
+    """A rigid track: rotation about y at 2 rad/s and a slow rise."""
+    t = np.arange(n_frames) * dt
+    ang = 2.0 * t
+    quat = np.stack([np.zeros_like(t), np.sin(ang / 2), np.zeros_like(t), np.cos(ang / 2)], 1)
+    pos = np.stack([np.zeros_like(t), 0.05 * t, np.zeros_like(t)], 1)
+    return pos, quat
+
+
+def wave_sequence(V, n_frames=30):
+    """A point track: the mesh's own vertices with a travelling wave in y."""
+    V = np.asarray(V, np.float64)
+    return np.stack([V + np.stack([np.zeros(len(V)), 0.01 * np.sin(V[:, 0] * 6 + 0.3 * k),
+                                   np.zeros(len(V))], 1) for k in range(n_frames)])
 
 
 def test_parse_all_keys(tmp_path):
@@ -341,3 +399,48 @@ def test_reference_scene_files_parse():
     assert len(ok) >= 25, rejected
     for name, why in rejected:
         assert "missing" in why, (name, why)
+
+
+def test_track_files_and_scene_tracks(tmp_path):
+    root = str(tmp_path)
+    os.makedirs(os.path.join(root, "track"))
+    pos, quat = spin_track()
+    np.savez(os.path.join(root, "track", "spin.npz"), pos=pos, quat=quat)
+    path, _, (bv, bf), _ = _write_scene(root, 65, animate="track/spin.npz")
+    cfg = C.parse_config(path)
+    sc = C.load_scene(path)
+    tr = C.scene_tracks(cfg, sc)
+    assert len(tr) == 1 and tr[0]["kind"] == "rigid" and tr[0]["mesh_id"] == 2
+    assert (tr[0]["v_begin"], tr[0]["v_end"]) == (sc.n_dyn, sc.n_vert)
+    assert tr[0]["pos"].dtype == np.float32 and np.allclose(tr[0]["quat"], quat)
+    # a path with "sequence" holds per-vertex points
+    seq = wave_sequence(bv)
+    np.savez(os.path.join(root, "track", "box_sequence.npz"), points=seq)
+    p2, *_ = _write_scene(root, 65, animate="track/box_sequence.npz")
+    tr2 = C.scene_tracks(C.parse_config(p2), C.load_scene(p2))
+    assert tr2[0]["kind"] == "points" and tr2[0]["points"].shape == seq.shape
+    # too short, wrong shapes
+    np.savez(os.path.join(root, "track", "short.npz"), pos=pos[:2], quat=quat[:2])
+    with pytest.raises(ValueError):
+        C.read_track(os.path.join(root, "track", "short.npz"))
+    np.savez(os.path.join(root, "track", "bad_sequence.npz"), points=seq[:, :3])
+    p3, *_ = _write_scene(root, 65, animate="track/bad_sequence.npz")
+    with pytest.raises(ValueError):
+        C.scene_tracks(C.parse_config(p3), C.load_scene(p3))
+
+
+def test_animator_frame_counter():
+    """The reference's counter: a rigid track reads frames 0 (init), 2, 4, ... and holds its
+    last frame with zero velocity; a point track reads 0, 1, 2, ...; two rigid tracks advance
+    the shared counter three times per substep."""
+    rig = {"kind": "rigid", "pos": np.zeros((7, 3)), "quat": np.zeros((7, 4))}
+    pts = {"kind": "points", "points": np.zeros((5, 1, 3))}
+    a = AnimatorRef([rig], np.zeros((1, 3)), 0.01)
+    seq = [a.frames(True)] + [a.frames(False) for _ in range(5)]
+    assert [f[0] for f in seq] == [(0, False), (2, True), (4, True), (6, False), (6, False), (6, False)]
+    b = AnimatorRef([pts], np.zeros((1, 3)), 0.01)
+    seq = [b.frames(True)] + [b.frames(False) for _ in range(6)]
+    assert [f[0] for f in seq] == [(0, False), (1, True), (2, True), (3, True), (4, True), (4, False), (4, False)]
+    c = AnimatorRef([rig, dict(rig)], np.zeros((1, 3)), 0.01)
+    assert c.frames(True) == [(0, False), (1, False)]
+    assert c.frames(False) == [(3, True), (4, True)]
