@@ -38,6 +38,7 @@ public:
     int global_solver = 0;  // 0 = Jacobi as the reference
     int pcg_iter = 0;
     int query_lanes = 0;  // 0 = chosen from the number of DCD queries
+    int contact_semantics = 0;  // 1 = the CPU backend's contact predicates (ProximalQuery)
 
     ~ADMMInnerB200() override {
         if (h_) admm_b200_destroy(h_);
@@ -199,6 +200,7 @@ private:
         d.global_solver = global_solver;
         d.pcg_iter = pcg_iter;
         d.query_lanes = query_lanes;
+        d.contact_semantics = contact_semantics;
     }
 };
 

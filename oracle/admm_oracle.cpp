@@ -125,8 +125,16 @@ struct RawPair {
 // All DCD pairs on float positions x (n x 3).  VF: each surface vertex against
 // every surface triangle not containing it (lbvh.cu:1693-1748).  EE: each edge
 // against every edge with a larger index sharing no vertex (lbvh.cu:1750-1813).
+// semantics 0: the GPU backend's predicates (region 0, 0 <= d < thickness,
+// boxes within the gap).  semantics 1: the CPU backend's ProximalQuery
+// (narrow_phase.cpp:192-469): no pair of two static elements (first vertex of
+// each at or above static_begin), point-triangle at any closest point with
+// d <= thickness, edge-edge with d < thickness unless both closest points are
+// segment end points; the box test is only a candidate filter there, so the
+// candidates are every element of the cells within the gap.
 static void dcd_all(const float* x, const std::vector<int>& sv, const std::vector<int>& st,
-                    const std::vector<int>& se, float thickness, std::vector<RawPair>& out) {
+                    const std::vector<int>& se, float thickness, std::vector<RawPair>& out,
+                    int semantics = 0, int static_begin = 1 << 30) {
     const int nsv = (int)sv.size(), nst = (int)st.size() / 3, nse = (int)se.size() / 2;
     std::vector<Box<float>> tb(nst), eb(nse);
     for (int i = 0; i < nst; i++) tb[i] = box_of(x, &st[3 * i], 3);
@@ -157,6 +165,12 @@ static void dcd_all(const float* x, const std::vector<int>& sv, const std::vecto
             for (int f : cand) {
                 const int* t = &st[3 * f];
                 if (v == t[0] || v == t[1] || v == t[2]) continue;
+                if (semantics == 1) {
+                    if (v >= static_begin && t[0] >= static_begin) continue;
+                    Result<float> r = gt_point_triangle(P(v), P(t[0]), P(t[1]), P(t[2]));
+                    if (r.distance <= thickness) local[q].push_back(RawPair{{v, t[0], t[1], t[2]}, r});
+                    continue;
+                }
                 if (!overlap(qb, tb[f], thickness)) continue;
                 Result<float> r = dcd_pt(P(v), P(t[0]), P(t[1]), P(t[2]));
                 if (r.distance < thickness && r.distance >= 0.f) local[q].push_back(RawPair{{v, t[0], t[1], t[2]}, r});
@@ -187,6 +201,13 @@ static void dcd_all(const float* x, const std::vector<int>& sv, const std::vecto
                 if (o <= e) continue;
                 const int oa = se[2 * o], ob = se[2 * o + 1];
                 if (ea == oa || ea == ob || eb_ == oa || eb_ == ob) continue;
+                if (semantics == 1) {
+                    if (ea >= static_begin && oa >= static_begin) continue;
+                    Result<float> r = gt_segment_segment(P(ea), P(eb_), P(oa), P(ob));
+                    const bool corner = (r.bary[0] == 0.f || r.bary[0] == 1.f) && (r.bary[1] == 0.f || r.bary[1] == 1.f);
+                    if (r.distance < thickness && !corner) local[e].push_back(RawPair{{ea, eb_, oa, ob}, r});
+                    continue;
+                }
                 if (!overlap(eb[e], eb[o], thickness)) continue;
                 Result<float> r = dcd_ee(P(ea), P(eb_), P(oa), P(ob));
                 if (r.distance < thickness && r.distance >= 0.f) local[e].push_back(RawPair{{ea, eb_, oa, ob}, r});
@@ -217,6 +238,7 @@ struct Oracle {
     std::vector<R> vmu;  // per-vertex friction (empty: mu everywhere)
     std::vector<R> cmu;  // per contact: the coefficient of its first dynamic vertex
     float thickness;
+    int semantics = 0;  // contact predicates: 0 GPU backend, 1 CPU backend
     int admm_max_iter, dcd_interval, gs_max_iter, jacobi_iter;
     bool contact, ws_ue, ws_uc;
     float residual_tol = 0.f;
@@ -275,6 +297,7 @@ struct Oracle {
         is_surf.assign(n, 0);
         for (int s : surf_verts) is_surf[s] = 1;
         dt = d->dt; g = d->g; mu = d->mu; kappa = d->kappa; beta = d->beta; thickness = d->thickness;
+        semantics = d->contact_semantics;
         if (d->vert_mu) vmu.assign(d->vert_mu, d->vert_mu + d->n_vert);
         admm_max_iter = d->admm_max_iter; dcd_interval = std::max(1, d->dcd_interval);
         gs_max_iter = d->gs_max_iter; jacobi_iter = d->jacobi_iter;
@@ -460,7 +483,7 @@ struct Oracle {
         std::vector<float> xf(3 * n);
         for (int i = 0; i < 3 * n; i++) xf[i] = (float)x[i];
         std::vector<RawPair> raw;
-        dcd_all(xf.data(), surf_verts, surf_tris, surf_edges, thickness, raw);
+        dcd_all(xf.data(), surf_verts, surf_tris, surf_edges, thickness, raw, semantics, nd);
         cts.resize(raw.size());
         for (size_t c = 0; c < raw.size(); c++) convert(raw[c], cts[c]);
         peak = std::max(peak, (int)cts.size());
@@ -928,18 +951,24 @@ int orc_contacts(void* hp, int32_t* pairs, double* bary, double* normal, double*
 
 // Standalone DCD on float positions (for pair-set parity): returns the pair count;
 // fills up to cap int4 pairs.
-int orc_dcd(const float* x, int n, const int32_t* sv, int nsv, const int32_t* st, int nst,
-            const int32_t* se, int nse, float thickness, int32_t* pairs, float* dist, int cap) {
+int orc_dcd2(const float* x, int n, const int32_t* sv, int nsv, const int32_t* st, int nst,
+             const int32_t* se, int nse, float thickness, int32_t* pairs, float* dist, int cap,
+             int semantics, int static_begin) {
     (void)n;
     std::vector<int> SV(sv, sv + nsv), ST(st, st + 3 * nst), SE(se, se + 2 * nse);
     std::vector<RawPair> raw;
-    dcd_all(x, SV, ST, SE, thickness, raw);
+    dcd_all(x, SV, ST, SE, thickness, raw, semantics, static_begin);
     int nc = std::min((int)raw.size(), cap);
     for (int i = 0; i < nc; i++) {
         for (int k = 0; k < 4; k++) pairs[4 * i + k] = raw[i].v[k];
         if (dist) dist[i] = raw[i].r.distance;
     }
     return (int)raw.size();
+}
+
+int orc_dcd(const float* x, int n, const int32_t* sv, int nsv, const int32_t* st, int nst,
+            const int32_t* se, int nse, float thickness, int32_t* pairs, float* dist, int cap) {
+    return orc_dcd2(x, n, sv, nsv, st, nst, se, nse, thickness, pairs, dist, cap, 0, 1 << 30);
 }
 
 // Unit-level functions (float and double) for known-answer tests.
@@ -959,6 +988,19 @@ void orc_dcd_pt_f(const float* p, const float* t0, const float* t1, const float*
     float o[11] = {r.distance, r.sqrDistance, r.bary[0], r.bary[1], r.bary[2],
                    r.closest[0].x, r.closest[0].y, r.closest[0].z, r.closest[1].x, r.closest[1].y, r.closest[1].z};
     std::memcpy(out, o, sizeof(o));
+}
+static void pack11(const Result<float>& r, float* out) {
+    float o[11] = {r.distance, r.sqrDistance, r.bary[0], r.bary[1], r.bary[2],
+                   r.closest[0].x, r.closest[0].y, r.closest[0].z, r.closest[1].x, r.closest[1].y, r.closest[1].z};
+    std::memcpy(out, o, sizeof(o));
+}
+void orc_gt_pt_f(const float* p, const float* t0, const float* t1, const float* t2, float* out) {
+    pack11(gt_point_triangle(mk(p[0], p[1], p[2]), mk(t0[0], t0[1], t0[2]), mk(t1[0], t1[1], t1[2]),
+                             mk(t2[0], t2[1], t2[2])), out);
+}
+void orc_gt_ee_f(const float* p0, const float* p1, const float* q0, const float* q1, float* out) {
+    pack11(gt_segment_segment(mk(p0[0], p0[1], p0[2]), mk(p1[0], p1[1], p1[2]), mk(q0[0], q0[1], q0[2]),
+                              mk(q1[0], q1[1], q1[2])), out);
 }
 void orc_dcd_ee_f(const float* p0, const float* p1, const float* q0, const float* q1, float* out) {
     Result<float> r = dcd_ee(mk(p0[0], p0[1], p0[2]), mk(p1[0], p1[1], p1[2]), mk(q0[0], q0[1], q0[2]), mk(q1[0], q1[1], q1[2]));

@@ -68,6 +68,11 @@ def lib():
             getattr(L, fn).argtypes = [_f]
         L.orc_dcd_pt_f.argtypes = [_f, _f, _f, _f, _f]
         L.orc_dcd_ee_f.argtypes = [_f, _f, _f, _f, _f]
+        L.orc_gt_pt_f.argtypes = [_f, _f, _f, _f, _f]
+        L.orc_gt_ee_f.argtypes = [_f, _f, _f, _f, _f]
+        L.orc_dcd2.restype = ctypes.c_int
+        L.orc_dcd2.argtypes = [_f, ctypes.c_int, _i, ctypes.c_int, _i, ctypes.c_int, _i, ctypes.c_int,
+                               ctypes.c_float, _i, _f, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_num_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -83,6 +88,8 @@ def ref_pin():
         R.ref_svd3.argtypes = [_f, _f, _f, _f]
         R.ref_dcd_pt_f.argtypes = [_f, _f, _f, _f, _f]
         R.ref_dcd_ee_f.argtypes = [_f, _f, _f, _f, _f]
+        R.ref_gt_pt_f.argtypes = [_f, _f, _f, _f, _f]
+        R.ref_gt_ee_f.argtypes = [_f, _f, _f, _f, _f]
         _ref = R
     return _ref
 
@@ -190,20 +197,40 @@ class Oracle:
         return {"pairs": pairs[:nc], "bary": bary[:nc], "normal": nrm[:nc], "point": pt[:nc], "gap": gap[:nc]}
 
 
-def dcd(x: np.ndarray, surf_verts, surf_tris, surf_edges, thickness: float, cap: Optional[int] = None):
-    """All contact pairs (int4) on float32 positions, in the oracle's order."""
+def dcd(x: np.ndarray, surf_verts, surf_tris, surf_edges, thickness: float, cap: Optional[int] = None,
+        semantics: int = 0, static_begin: Optional[int] = None):
+    """All contact pairs (int4) on float32 positions, in the oracle's order.  semantics 0: the GPU
+    backend's predicates; 1: the CPU backend's (static_begin = first static vertex)."""
     x = np.ascontiguousarray(x, np.float32)
     sv = np.ascontiguousarray(surf_verts, np.int32)
     st = np.ascontiguousarray(surf_tris, np.int32)
     se = np.ascontiguousarray(surf_edges, np.int32)
+    sb = len(x) if static_begin is None else int(static_begin)
     L = lib()
-    n = L.orc_dcd(_p(x, _f), len(x), _p(sv, _i), len(sv), _p(st, _i), len(st), _p(se, _i), len(se),
-                  float(thickness), None, None, 0)
+    args = (_p(x, _f), len(x), _p(sv, _i), len(sv), _p(st, _i), len(st), _p(se, _i), len(se), float(thickness))
+    n = L.orc_dcd2(*args, None, None, 0, int(semantics), sb)
     pairs = np.zeros((max(n, 1), 4), np.int32)
     dist = np.zeros(max(n, 1), np.float32)
-    L.orc_dcd(_p(x, _f), len(x), _p(sv, _i), len(sv), _p(st, _i), len(st), _p(se, _i), len(se),
-              float(thickness), _p(pairs, _i), _p(dist, _f), n)
+    L.orc_dcd2(*args, _p(pairs, _i), _p(dist, _f), n, int(semantics), sb)
     return pairs[:n], dist[:n]
+
+
+def gt_pt(p, t0, t1, t2, ref: bool = False) -> np.ndarray:
+    """The CPU backend's point-triangle closest points (11 floats as dcd_pt)."""
+    out = np.zeros(11, np.float32)
+    args = [np.ascontiguousarray(a, np.float32) for a in (p, t0, t1, t2)]
+    fn = ref_pin().ref_gt_pt_f if ref else lib().orc_gt_pt_f
+    fn(*[_p(a, _f) for a in args], _p(out, _f))
+    return out
+
+
+def gt_ee(p0, p1, q0, q1, ref: bool = False) -> np.ndarray:
+    """The CPU backend's segment-segment closest points (parameters in slots 2-3)."""
+    out = np.zeros(11, np.float32)
+    args = [np.ascontiguousarray(a, np.float32) for a in (p0, p1, q0, q1)]
+    fn = ref_pin().ref_gt_ee_f if ref else lib().orc_gt_ee_f
+    fn(*[_p(a, _f) for a in args], _p(out, _f))
+    return out
 
 
 def dcd_pt(p, t0, t1, t2, ref: bool = False) -> np.ndarray:

@@ -127,6 +127,182 @@ inline Result<R> dcd_ee(V3<R> P0, V3<R> P1, V3<R> Q0, V3<R> Q1) {
     return res;
 }
 
+// ---------------------------------------------------------------------------
+// Narrow phase of the reference's CPU backend (ProximalQuery::narrow_PT /
+// narrow_EE, src/contact/narrow_phase.cpp:376-469), which calls the closest-
+// point queries of David Eberly's Geometric Tools (src/mutils/distPT.h,
+// distEE.h; published in "Distance Between Point and Triangle in 3D" and
+// "Distance Between Two Line Segments in 3D", geometrictools.com).  Every
+// region is accepted.  Point-triangle: minimise |t0 + s e0 + t e1 - p|^2 over
+// the triangle by the sign of the unconstrained minimiser (s, t) and of
+// s + t - det; the closest point is t0 + s e0 + t e1, barycentric
+// (1 - s - t, s, t).  Segment-segment: minimise over [0,1]^2 by the signs of
+// b e - c d and a e - b d (or, for parallel segments, along the edges of the
+// square); parameters (s, t) are returned in bary[0..1] and bary[2] = -2 marks
+// an edge-edge result, as the GPU path's results do.  The operation order is
+// the reference's, so the accepted pair sets agree bit for bit.
+// ---------------------------------------------------------------------------
+template <class R>
+inline Result<R> gt_point_triangle(V3<R> point, V3<R> t0, V3<R> t1, V3<R> t2) {
+    const R zero = 0, one = 1, two = 2;
+    V3<R> diff = t0 - point, e0 = t1 - t0, e1 = t2 - t0;
+    const R a00 = dot(e0, e0), a01 = dot(e0, e1), a11 = dot(e1, e1);
+    const R b0 = dot(diff, e0), b1 = dot(diff, e1);
+    const R det = std::max(a00 * a11 - a01 * a01, zero);
+    R s = a01 * b1 - a11 * b0;
+    R t = a01 * b0 - a00 * b1;
+    // the minimiser clamped to an edge s = 0 / t = 0 from the sign of b
+    auto edge_t = [&](R& u) { u = b1 >= zero ? zero : (-b1 >= a11 ? one : -b1 / a11); };
+    auto edge_s = [&](R& u) { u = b0 >= zero ? zero : (-b0 >= a00 ? one : -b0 / a00); };
+    if (s + t <= det) {
+        if (s < zero) {
+            if (t < zero) {          // below both edges: vertex t0 region
+                if (b0 < zero) {
+                    t = zero;
+                    s = -b0 >= a00 ? one : -b0 / a00;
+                } else {
+                    s = zero;
+                    edge_t(t);
+                }
+            } else {                 // beyond edge s = 0
+                s = zero;
+                edge_t(t);
+            }
+        } else if (t < zero) {       // beyond edge t = 0
+            t = zero;
+            edge_s(s);
+        } else {                     // interior
+            s /= det;
+            t /= det;
+        }
+    } else {
+        if (s < zero) {              // beyond vertex t2
+            const R q0 = a01 + b0, q1 = a11 + b1;
+            if (q1 > q0) {
+                const R num = q1 - q0, den = a00 - two * a01 + a11;
+                if (num >= den) { s = one; t = zero; }
+                else { s = num / den; t = one - s; }
+            } else {
+                s = zero;
+                t = q1 <= zero ? one : (b1 >= zero ? zero : -b1 / a11);
+            }
+        } else if (t < zero) {       // beyond vertex t1
+            const R q0 = a01 + b1, q1 = a00 + b0;
+            if (q1 > q0) {
+                const R num = q1 - q0, den = a00 - two * a01 + a11;
+                if (num >= den) { t = one; s = zero; }
+                else { t = num / den; s = one - t; }
+            } else {
+                t = zero;
+                s = q1 <= zero ? one : (b0 >= zero ? zero : -b0 / a00);
+            }
+        } else {                     // beyond edge s + t = 1
+            const R num = a11 + b1 - a01 - b0;
+            if (num <= zero) { s = zero; t = one; }
+            else {
+                const R den = a00 - two * a01 + a11;
+                if (num >= den) { s = one; t = zero; }
+                else { s = num / den; t = one - s; }
+            }
+        }
+    }
+    Result<R> r{};
+    r.closest[0] = point;
+    r.closest[1] = (t0 + s * e0) + t * e1;
+    diff = r.closest[0] - r.closest[1];
+    r.sqrDistance = dot(diff, diff);
+    r.distance = std::sqrt(r.sqrDistance);
+    r.bary[0] = (one - s) - t;
+    r.bary[1] = s;
+    r.bary[2] = t;
+    return r;
+}
+
+template <class R>
+inline Result<R> gt_segment_segment(V3<R> P0, V3<R> P1, V3<R> Q0, V3<R> Q1) {
+    const R zero = 0, one = 1;
+    const V3<R> u = P1 - P0, v = Q1 - Q0, w = P0 - Q0;
+    const R a = dot(u, u), b = dot(u, v), c = dot(v, v), d = dot(u, w), e = dot(v, w);
+    const R det = a * c - b * b;
+    R s = zero, t = zero;
+    // s on [0, 1] for a fixed t edge: numerator n over a, clamped
+    auto clamp_s = [&](R n) { return n <= zero ? zero : (n >= a ? one : n / a); };
+    if (det > zero) {
+        const R bte = b * e, ctd = c * d;
+        if (bte <= ctd) {            // s <= 0
+            s = zero;
+            if (e <= zero) {
+                t = zero;
+                const R nd = -d;
+                if (nd >= a) s = one;
+                else if (nd > zero) s = nd / a;
+            } else if (e < c) {
+                t = e / c;
+            } else {
+                t = one;
+                const R bmd = b - d;
+                if (bmd >= a) s = one;
+                else if (bmd > zero) s = bmd / a;
+            }
+        } else {
+            s = bte - ctd;
+            if (s >= det) {          // s >= 1
+                s = one;
+                const R bpe = b + e;
+                if (bpe <= zero) {
+                    t = zero;
+                    const R nd = -d;
+                    if (nd <= zero) s = zero;
+                    else if (nd < a) s = nd / a;
+                } else if (bpe < c) {
+                    t = bpe / c;
+                } else {
+                    t = one;
+                    const R bmd = b - d;
+                    if (bmd <= zero) s = zero;
+                    else if (bmd < a) s = bmd / a;
+                }
+            } else {                 // 0 < s < 1
+                const R ate = a * e, btd = b * d;
+                if (ate <= btd) {
+                    t = zero;
+                    s = clamp_s(-d);
+                } else {
+                    t = ate - btd;
+                    if (t >= det) {
+                        t = one;
+                        s = clamp_s(b - d);
+                    } else {
+                        s /= det;
+                        t /= det;
+                    }
+                }
+            }
+        }
+    } else {                         // parallel segments
+        if (e <= zero) {
+            t = zero;
+            s = clamp_s(-d);
+        } else if (e >= c) {
+            t = one;
+            s = clamp_s(b - d);
+        } else {
+            s = zero;
+            t = e / c;
+        }
+    }
+    Result<R> r{};
+    r.bary[0] = s;
+    r.bary[1] = t;
+    r.bary[2] = R(-2);
+    r.closest[0] = P0 + s * u;
+    r.closest[1] = Q0 + t * v;
+    const V3<R> diff = r.closest[0] - r.closest[1];
+    r.sqrDistance = dot(diff, diff);
+    r.distance = std::sqrt(r.sqrDistance);
+    return r;
+}
+
 // AABB overlap with gap (lbvh.cu:43-49)
 template <class R> struct Box {
     V3<R> lo, up;

@@ -354,7 +354,7 @@ ADMM_DEV void grid_walk(const DevScene& s, const QueryGroup<G>& grp, bool vf, in
                         // same cell (not another of the bucket); larger edge index; once per pair:
                         // this cell is the first of the query's or of the element's range on every axis
                         ok = ek == kj && (vf || partner > e) && ((fj | __float_as_int(eup.w)) & 7) == 7 &&
-                             box_overlap(lo, up, elo, eup, gap);
+                             (s.cpu_contact || box_overlap(lo, up, elo, eup, gap));
                     }
                     grid_queue_push(grp, q, ok, partner, narrow);
                 }
@@ -367,7 +367,7 @@ ADMM_DEV void grid_walk(const DevScene& s, const QueryGroup<G>& grp, bool vf, in
                 if (t < n && g.mode[vf ? t : s.nst + t]) {
                     float4 eup;
                     const float4 elo = vf ? tri_box_lo(s, t, eup) : edge_box_lo(s, t, eup);
-                    ok = box_overlap(lo, up, elo, eup, gap);
+                    ok = s.cpu_contact || box_overlap(lo, up, elo, eup, gap);
                 }
                 grid_queue_push(grp, q, ok, t, narrow);
             }
@@ -383,7 +383,7 @@ ADMM_DEV void grid_walk(const DevScene& s, const QueryGroup<G>& grp, bool vf, in
             if (vf || (o != e && (small || o > e))) {
                 float4 oup;
                 const float4 olo = vf ? tri_box_lo(s, o, oup) : edge_box_lo(s, o, oup);
-                ok = box_overlap(lo, up, olo, oup, gap);  // the overlap rule is symmetric
+                ok = s.cpu_contact || box_overlap(lo, up, olo, oup, gap);  // the overlap rule is symmetric
             }
         }
         grid_queue_push(grp, q, ok, o, narrow);
@@ -476,23 +476,40 @@ ADMM_DEV bool surely_apart(float d2, float thickness, float4 a, float4 b, float4
 }
 
 // Narrow phase of vertex v against triangle f (region 0, 0 <= d < thickness).
+// Narrow phase of vertex v against triangle f: the GPU backend's (region 0,
+// 0 <= d < thickness) or, with cpu_contact, the CPU backend's (no pair of two
+// static elements, any closest point, d <= thickness).
 ADMM_DEV bool grid_hit_vf(const DevScene& s, int v, float4 P, int f, int4& ids, NpResult& r) {
     const int4 tri = s.st[f];
     if (v == tri.x || v == tri.y || v == tri.z) return false;
+    if (s.cpu_contact && v >= s.nd && tri.x >= s.nd) return false;
     ids = make_int4(v, tri.x, tri.y, tri.z);
     const float4 a = s.x[tri.x], b = s.x[tri.y], c = s.x[tri.z];
     if (surely_apart(fast_pt_dist2(P, a, b, c), s.thickness, P, a, b, c)) return false;
+    if (s.cpu_contact) {
+        closest_pt_all(P, a, b, c, r);
+        return r.dist <= s.thickness;
+    }
     return narrow_pt(P, a, b, c, r) && r.dist < s.thickness && r.dist >= 0.f;
 }
 
 // Narrow phase of edges e and o (no shared vertex), lower index first.
+// Narrow phase of edges e and o (no shared vertex), lower index first: the GPU
+// backend's (region 0) or, with cpu_contact, the CPU backend's (no pair of two
+// static edges, d < thickness unless both closest points are end points).
 ADMM_DEV bool grid_hit_ee(const DevScene& s, int e, int o, int4& ids, NpResult& r) {
     const int2 ed = s.se[e], od = s.se[o];
     if (ed.x == od.x || ed.x == od.y || ed.y == od.x || ed.y == od.y) return false;
     const int2 lo = o > e ? ed : od, hi = o > e ? od : ed;
+    if (s.cpu_contact && lo.x >= s.nd && hi.x >= s.nd) return false;
     ids = make_int4(lo.x, lo.y, hi.x, hi.y);
     const float4 p0 = s.x[lo.x], p1 = s.x[lo.y], q0 = s.x[hi.x], q1 = s.x[hi.y];
     if (surely_apart(fast_ee_dist2(p0, p1, q0, q1), s.thickness, p0, p1, q0, q1)) return false;
+    if (s.cpu_contact) {
+        closest_ee_all(p0, p1, q0, q1, r);
+        const bool corner = (r.bary[0] == 0.f || r.bary[0] == 1.f) && (r.bary[1] == 0.f || r.bary[1] == 1.f);
+        return r.dist < s.thickness && !corner;
+    }
     return narrow_ee(p0, p1, q0, q1, r) && r.dist < s.thickness && r.dist >= 0.f;
 }
 

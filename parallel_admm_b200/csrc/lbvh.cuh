@@ -284,6 +284,161 @@ ADMM_DEV bool narrow_ee(float4 P0, float4 P1, float4 Q0, float4 Q1, NpResult& r)
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// The CPU backend's closest points (ProximalQuery::narrow_PT / narrow_EE,
+// narrow_phase.cpp:376-469, through Eberly's queries of distPT.h / distEE.h):
+// every region, in the same operation order as the FP32 reference, so that the
+// accepted sets agree bit for bit.  Point-triangle: the minimiser of
+// |t0 + s e0 + t e1 - p|^2 on the triangle, chosen by the signs of s, t and
+// s + t - det; edge-edge: the minimiser over [0,1]^2 by the signs of
+// b e - c d and a e - b d, or along the square's edges for parallel segments.
+// ---------------------------------------------------------------------------
+ADMM_DEV float clamp_ratio(float n, float a) { return n <= 0.f ? 0.f : (n >= a ? 1.f : fdiv(n, a)); }
+
+ADMM_DEV void closest_pt_all(float4 P, float4 T0, float4 T1, float4 T2, NpResult& r) {
+    const float dx = fsub(T0.x, P.x), dy = fsub(T0.y, P.y), dz = fsub(T0.z, P.z);
+    const float e0x = fsub(T1.x, T0.x), e0y = fsub(T1.y, T0.y), e0z = fsub(T1.z, T0.z);
+    const float e1x = fsub(T2.x, T0.x), e1y = fsub(T2.y, T0.y), e1z = fsub(T2.z, T0.z);
+    const float a00 = ndot(e0x, e0y, e0z, e0x, e0y, e0z);
+    const float a01 = ndot(e0x, e0y, e0z, e1x, e1y, e1z);
+    const float a11 = ndot(e1x, e1y, e1z, e1x, e1y, e1z);
+    const float b0 = ndot(dx, dy, dz, e0x, e0y, e0z);
+    const float b1 = ndot(dx, dy, dz, e1x, e1y, e1z);
+    const float dd = fsub(fmul(a00, a11), fmul(a01, a01));
+    const float det = dd < 0.f ? 0.f : dd;
+    float s = fsub(fmul(a01, b1), fmul(a11, b0));
+    float t = fsub(fmul(a01, b0), fmul(a00, b1));
+    // the minimiser on an edge s = 0 (over t) or t = 0 (over s) from the sign of b
+    const float on_t = b1 >= 0.f ? 0.f : (-b1 >= a11 ? 1.f : fdiv(-b1, a11));
+    const float on_s = b0 >= 0.f ? 0.f : (-b0 >= a00 ? 1.f : fdiv(-b0, a00));
+    if (fadd(s, t) <= det) {
+        if (s < 0.f) {
+            if (t < 0.f && b0 < 0.f) {
+                t = 0.f;
+                s = -b0 >= a00 ? 1.f : fdiv(-b0, a00);
+            } else {
+                s = 0.f;
+                t = on_t;
+            }
+        } else if (t < 0.f) {
+            t = 0.f;
+            s = on_s;
+        } else {
+            s = fdiv(s, det);
+            t = fdiv(t, det);
+        }
+    } else {
+        const float den = fadd(fsub(a00, fmul(2.f, a01)), a11);
+        if (s < 0.f) {
+            const float q0 = fadd(a01, b0), q1 = fadd(a11, b1);
+            if (q1 > q0) {
+                const float num = fsub(q1, q0);
+                if (num >= den) { s = 1.f; t = 0.f; }
+                else { s = fdiv(num, den); t = fsub(1.f, s); }
+            } else {
+                s = 0.f;
+                t = q1 <= 0.f ? 1.f : (b1 >= 0.f ? 0.f : fdiv(-b1, a11));
+            }
+        } else if (t < 0.f) {
+            const float q0 = fadd(a01, b1), q1 = fadd(a00, b0);
+            if (q1 > q0) {
+                const float num = fsub(q1, q0);
+                if (num >= den) { t = 1.f; s = 0.f; }
+                else { t = fdiv(num, den); s = fsub(1.f, t); }
+            } else {
+                t = 0.f;
+                s = q1 <= 0.f ? 1.f : (b0 >= 0.f ? 0.f : fdiv(-b0, a00));
+            }
+        } else {
+            const float num = fsub(fsub(fadd(a11, b1), a01), b0);
+            if (num <= 0.f) { s = 0.f; t = 1.f; }
+            else if (num >= den) { s = 1.f; t = 0.f; }
+            else { s = fdiv(num, den); t = fsub(1.f, s); }
+        }
+    }
+    r.c0[0] = P.x; r.c0[1] = P.y; r.c0[2] = P.z;
+    r.c1[0] = fadd(fadd(T0.x, fmul(s, e0x)), fmul(t, e1x));
+    r.c1[1] = fadd(fadd(T0.y, fmul(s, e0y)), fmul(t, e1y));
+    r.c1[2] = fadd(fadd(T0.z, fmul(s, e0z)), fmul(t, e1z));
+    const float qx = fsub(r.c0[0], r.c1[0]), qy = fsub(r.c0[1], r.c1[1]), qz = fsub(r.c0[2], r.c1[2]);
+    r.dist = fsqrt(ndot(qx, qy, qz, qx, qy, qz));
+    r.bary[0] = fsub(fsub(1.f, s), t);
+    r.bary[1] = s;
+    r.bary[2] = t;
+}
+
+ADMM_DEV void closest_ee_all(float4 P0, float4 P1, float4 Q0, float4 Q1, NpResult& r) {
+    const float ux = fsub(P1.x, P0.x), uy = fsub(P1.y, P0.y), uz = fsub(P1.z, P0.z);
+    const float vx = fsub(Q1.x, Q0.x), vy = fsub(Q1.y, Q0.y), vz = fsub(Q1.z, Q0.z);
+    const float wx = fsub(P0.x, Q0.x), wy = fsub(P0.y, Q0.y), wz = fsub(P0.z, Q0.z);
+    const float a = ndot(ux, uy, uz, ux, uy, uz);
+    const float b = ndot(ux, uy, uz, vx, vy, vz);
+    const float c = ndot(vx, vy, vz, vx, vy, vz);
+    const float d = ndot(ux, uy, uz, wx, wy, wz);
+    const float e = ndot(vx, vy, vz, wx, wy, wz);
+    const float det = fsub(fmul(a, c), fmul(b, b));
+    float s = 0.f, t = 0.f;
+    if (det > 0.f) {
+        const float bte = fmul(b, e), ctd = fmul(c, d);
+        if (bte <= ctd) {
+            if (e <= 0.f) {
+                const float nd = -d;
+                s = nd >= a ? 1.f : (nd > 0.f ? fdiv(nd, a) : 0.f);
+            } else if (e < c) {
+                t = fdiv(e, c);
+            } else {
+                t = 1.f;
+                const float bmd = fsub(b, d);
+                s = bmd >= a ? 1.f : (bmd > 0.f ? fdiv(bmd, a) : 0.f);
+            }
+        } else {
+            s = fsub(bte, ctd);
+            if (s >= det) {
+                const float bpe = fadd(b, e);
+                if (bpe <= 0.f) {
+                    const float nd = -d;
+                    s = nd <= 0.f ? 0.f : (nd < a ? fdiv(nd, a) : 1.f);
+                } else if (bpe < c) {
+                    s = 1.f;
+                    t = fdiv(bpe, c);
+                } else {
+                    t = 1.f;
+                    const float bmd = fsub(b, d);
+                    s = bmd <= 0.f ? 0.f : (bmd < a ? fdiv(bmd, a) : 1.f);
+                }
+            } else {
+                const float ate = fmul(a, e), btd = fmul(b, d);
+                if (ate <= btd) {
+                    s = clamp_ratio(-d, a);
+                } else {
+                    t = fsub(ate, btd);
+                    if (t >= det) {
+                        t = 1.f;
+                        s = clamp_ratio(fsub(b, d), a);
+                    } else {
+                        s = fdiv(s, det);
+                        t = fdiv(t, det);
+                    }
+                }
+            }
+        }
+    } else if (e <= 0.f) {
+        s = clamp_ratio(-d, a);
+    } else if (e >= c) {
+        t = 1.f;
+        s = clamp_ratio(fsub(b, d), a);
+    } else {
+        t = fdiv(e, c);
+    }
+    r.bary[0] = s;
+    r.bary[1] = t;
+    r.bary[2] = -10.f;
+    r.c0[0] = fadd(P0.x, fmul(s, ux)); r.c0[1] = fadd(P0.y, fmul(s, uy)); r.c0[2] = fadd(P0.z, fmul(s, uz));
+    r.c1[0] = fadd(Q0.x, fmul(t, vx)); r.c1[1] = fadd(Q0.y, fmul(t, vy)); r.c1[2] = fadd(Q0.z, fmul(t, vz));
+    const float qx = fsub(r.c0[0], r.c1[0]), qy = fsub(r.c0[1], r.c1[1]), qz = fsub(r.c0[2], r.c1[2]);
+    r.dist = fsqrt(ndot(qx, qy, qz, qx, qy, qz));
+}
+
 ADMM_DEV bool box_overlap(float4 llo, float4 lup, float4 rlo, float4 rup, float gap) {
     if ((rlo.x - lup.x) >= gap || (llo.x - rup.x) >= gap) return false;
     if ((rlo.y - lup.y) >= gap || (llo.y - rup.y) >= gap) return false;

@@ -82,6 +82,7 @@ struct DevScene {
     int tri_sr = 0, tet_sr = 0, bend_sr = 0, pin_sr = 0;
     float dt = 0, dt_inv = 0, g = 0, mu = 0, eps = 0, gam = 0, thickness = 0;
     int contact = 0;
+    int cpu_contact = 0;  // contact predicates of the CPU backend (ProximalQuery)
     // vertex state (float4 rows, w unused)
     float4 *x = nullptr, *x0 = nullptr, *v = nullptr, *p = nullptr, *mxt = nullptr;
     float4 *b = nullptr, *uc = nullptr, *xprev = nullptr, *jac[2] = {nullptr, nullptr};

@@ -64,6 +64,7 @@ class SolverParams:
     global_solver: int = 0  # 0 Jacobi (reference), 1 PCG with diag(A), 2 PCG with learned blocks
     pcg_iter: int = 0  # 0 = jacobi_iter // 2
     query_lanes: int = 0  # lanes per grid DCD query: 0 chosen from the query count, or 8, 16, 32
+    contact_semantics: int = 0  # contact predicates: 0 the GPU backend's, 1 the CPU backend's
 
 
 @dataclasses.dataclass

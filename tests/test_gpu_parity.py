@@ -596,3 +596,48 @@ def test_batch_with_per_body_friction_parity():
         assert err <= TOL_STEP * (k + 1), (k, err, sg["n_contacts"], so["n_contacts"])
         seen = sg["n_contacts"]
     assert seen > 0
+
+
+@pytest.mark.parametrize("lanes", [8, 32])
+@pytest.mark.parametrize("case", ["cloth_fold", "cube_squeezed", "cloth_flat_on_box", "layers_stack"])
+def test_dcd_pairs_bitexact_cpu_semantics(case, lanes):
+    """contact_semantics 1 (the CPU backend's ProximalQuery predicates): the device pair set equals
+    the oracle's, whose closest points are pinned to the reference's distPT.h / distEE.h."""
+    from oracle import oracle as O
+    sc, x = _dcd_case(case)
+    sc.params.contact_semantics = 1
+    sc.params.query_lanes = lanes
+    h = B.Handle(sc)
+    n = h.detect(x)
+    ref_pairs, _ = O.dcd(x, sc.surf_verts, sc.surf_tris, sc.surf_edges, sc.params.thickness,
+                         semantics=1, static_begin=sc.n_dyn)
+    assert n == len(ref_pairs) and n > 0
+    got = h.contacts()
+    assert sorted(map(tuple, got["pairs"].tolist())) == sorted(map(tuple, ref_pairs.tolist()))
+
+
+def test_cpu_semantics_contact_step_parity():
+    """The CPU backend's contact predicates through conversion and the contact projection: the
+    same pairs as the oracle, converted fields and contact velocities within the tolerances of
+    the GPU predicates' test."""
+    sc, x = _crumpled_cloth()
+    sc.params.contact_semantics = 1
+    h, o = _setup(sc)
+    x64 = x.astype(np.float64)
+    rng = np.random.default_rng(12)
+    uc = rng.normal(scale=1e-4, size=(sc.n_dyn, 3))
+    for tgt in (h, o):
+        tgt.write(B.BUF_X, x64)
+        tgt.write(B.BUF_UC, uc)
+    n = h.detect()
+    assert n == o.detect() and n > 0
+    gc, oc = h.contacts(), o.contacts()
+    gi = {tuple(p): i for i, p in enumerate(gc["pairs"].tolist())}
+    perm = np.array([gi[tuple(p)] for p in oc["pairs"].tolist()])
+    assert np.abs(gc["bary"][perm] - oc["bary"]).max() <= 1e-5
+    assert np.abs(gc["normal"][perm] - oc["normal"]).max() <= 1e-4
+    assert np.abs(gc["gap"][perm] - oc["gap"]).max() <= 1e-6
+    h.contact_step()
+    o.contact_step()
+    pg, po = h.read(B.BUF_P), o.read(B.BUF_P)
+    assert _rel(pg[:sc.n_dyn], po[:sc.n_dyn]) <= 1e-4
