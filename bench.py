@@ -409,6 +409,8 @@ def main():
                "sample": f"{n} substeps, one at every {args.cpu_stride}th frame of frames 0..{args.steps - 1}, "
                          f"each from the GPU run's state; {secs:.1f} s of CPU time (oracle FP32, OpenMP), "
                          f"mean {it_mean:.1f} ADMM iterations per step"}
+    tn, gm = h.tuning(), h.global_mode()
+    tuned = {"jacobi_lanes": tn["jacobi_lanes"], "rhs_lanes": tn["rhs_lanes"], "global_mode": gm["mode"]}
     line = {
         "metric": metric_name(args.tol, sc.params.admm_max_iter, args.global_solver,
                               args.pcg_iter or max(1, sc.params.jacobi_iter // 2)),
@@ -420,7 +422,8 @@ def main():
                    "contacts_mean": float(np.mean(contacts)), "contacts_peak": int(peak),
                    "residual_tol": args.tol, "admm_iter_cap": sc.params.admm_max_iter,
                    "admm_iters_mean": float(np.mean(iters)),
-                   "converged_fraction": float(np.mean(conv)) if args.tol > 0 else None},
+                   "converged_fraction": float(np.mean(conv)) if args.tol > 0 else None,
+                   "tuned": tuned},
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": args.probe, "achieved": achieved, "peak": peak_gbs,

@@ -697,18 +697,20 @@ int time_global(AdmmB200* h, int mode, float* ms) {
 }
 
 int upload_ell(AdmmB200* h, const HostCsr& c, int rows, int lanes, SlicedEll& out, HostEll* keep = nullptr) {
-    HostEll e = csr_to_sliced_ell(c, rows, lanes);
-    int *p = nullptr, *cc = nullptr;
+    HostEll e = csr_to_sliced_ell(c, rows, lanes, true);
+    int *p = nullptr, *cc = nullptr, *rid = nullptr;
     float* v = nullptr;
     TRY(dupload(h, &p, e.ptr.data(), e.ptr.size()));
     TRY(dupload(h, &cc, e.col.data(), e.col.size()));
     TRY(dupload(h, &v, e.val.data(), e.val.size()));
+    if (!e.rowid.empty()) TRY(dupload(h, &rid, e.rowid.data(), e.rowid.size()));
     out.rows = rows;
     out.nslices = e.nslices;
     out.lanes = lanes;
     out.ptr = p;
     out.col = cc;
     out.val = v;
+    out.rowid = rid;
     if (keep) *keep = std::move(e);
     return ADMM_OK;
 }
@@ -717,6 +719,7 @@ void free_ell(AdmmB200* h, SlicedEll& m) {
     dfree(h, const_cast<int*>(m.ptr));
     dfree(h, const_cast<int*>(m.col));
     dfree(h, const_cast<float*>(m.val));
+    dfree(h, const_cast<int*>(m.rowid));
     m = SlicedEll{};
 }
 

@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s, int spli
 template <int T, bool CG = false>
 ADMM_DEV float4 ell_row_sum(const SlicedEll& M, const float4* __restrict__ v, int w, int lane, int& row) {
     constexpr int S = 32 / T;
-    row = w * S + (lane % S);
+    row = M.rowid ? __ldg(&M.rowid[w * S + (lane % S)]) : w * S + (lane % S);
     const int b = M.ptr[w], e = M.ptr[w + 1];
     float ax = 0.f, ay = 0.f, az = 0.f;
 #pragma unroll 4
@@ -325,7 +325,7 @@ constexpr int kPrefetch = 8;
 template <int T>
 ADMM_DEV float4 ell_row_sum_pf(const SlicedEll& M, const float4* __restrict__ v, int w, int lane, int& row) {
     constexpr int S = 32 / T;
-    row = w * S + (lane % S);
+    row = M.rowid ? __ldg(&M.rowid[w * S + (lane % S)]) : w * S + (lane % S);
     const int b = M.ptr[w], e = M.ptr[w + 1];
     int cc[kPrefetch];
     float vv[kPrefetch];

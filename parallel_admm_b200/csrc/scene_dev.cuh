@@ -7,7 +7,9 @@ namespace admm {
 constexpr int kStackDepth = 64;     // BVH traversal stack (lbvh.cu:1698 uses 64)
 
 // Sliced ELL with `lanes` (T) threads per row: slices of 32/T rows, one warp per
-// slice; entry k of local row lr at ptr[s] + (k/T)*32 + (k%T)*(32/T) + lr.
+// slice; entry k of local row lr at ptr[s] + (k/T)*32 + (k%T)*(32/T) + lr.  Slot
+// lr of slice s holds row rowid[s*32/T + lr] (rows reordered by length within
+// windows of 32), or row s*32/T + lr without rowid.
 struct SlicedEll {
     int rows = 0;
     int nslices = 0;
@@ -15,6 +17,7 @@ struct SlicedEll {
     const int* ptr = nullptr;    // [nslices+1] offsets (multiples of kSlice)
     const int* col = nullptr;
     const float* val = nullptr;
+    const int* rowid = nullptr;  // [nslices * 32/T] row of each slot (null: slot = row)
 };
 
 struct BvhDev {

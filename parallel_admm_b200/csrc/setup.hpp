@@ -18,6 +18,7 @@ struct HostEll {
     int rows = 0, nslices = 0, lanes = 1;
     std::vector<int> ptr, col;
     std::vector<float> val;
+    std::vector<int> rowid;  // [nslices * S] row of each slot (empty: slot = row)
     int64_t nnz = 0;  // true entries (without padding)
 };
 
@@ -32,16 +33,35 @@ struct HostCsr {
 // reads 32 consecutive entries.  Padding repeats the row's own column with a
 // zero value (branch-free in the kernel).  T = 1 is the classic sliced ELL of
 // Monakov et al. (2010) with slice height 32.
-inline HostEll csr_to_sliced_ell(const HostCsr& c, int rows, int T) {
+// permute: within each window of 32 consecutive rows the rows are placed in the
+// slots in order of decreasing length (ties by index), so that rows of similar
+// length share a slice and the padding shrinks (the vertices of a tet lattice
+// alternate between 6 and 18 neighbours, which pads every unpermuted slice to
+// 18); rowid[slot] gives the row, rows for the empty slots past the end.  A
+// window never straddles a multiple of 32, so row ranges that start at such
+// multiples own exactly their slices.  Each row keeps its entries, their order
+// and lane layout, so its sum is the same as without the permutation.
+inline HostEll csr_to_sliced_ell(const HostCsr& c, int rows, int T, bool permute = false) {
     HostEll e;
     const int S = 32 / T;
     e.rows = rows;
     e.lanes = T;
     e.nslices = (rows + S - 1) / S;
+    std::vector<int> order((size_t)e.nslices * S, rows);
+    for (int r = 0; r < rows; r++) order[r] = r;
+    if (permute) {
+        auto len = [&](int r) { return c.start[r + 1] - c.start[r]; };
+        for (int w0 = 0; w0 < rows; w0 += 32) {
+            const int w1 = std::min(rows, w0 + 32);
+            std::stable_sort(order.begin() + w0, order.begin() + w1, [&](int a, int b) { return len(a) > len(b); });
+        }
+        e.rowid = order;
+    }
     e.ptr.assign(e.nslices + 1, 0);
     for (int s = 0; s < e.nslices; s++) {
         int w = 0;
-        for (int r = s * S; r < std::min(rows, (s + 1) * S); r++) w = std::max(w, c.start[r + 1] - c.start[r]);
+        for (int k = s * S; k < (s + 1) * S; k++)
+            if (order[k] < rows) w = std::max(w, c.start[order[k] + 1] - c.start[order[k]]);
         w = (w + T - 1) / T * T;
         e.ptr[s + 1] = e.ptr[s] + w * S;
     }
@@ -50,7 +70,7 @@ inline HostEll csr_to_sliced_ell(const HostCsr& c, int rows, int T) {
     for (int s = 0; s < e.nslices; s++) {
         const int w = (e.ptr[s + 1] - e.ptr[s]) / S;
         for (int lr = 0; lr < S; lr++) {
-            const int r = s * S + lr;
+            const int r = order[s * S + lr];
             const int len = r < rows ? c.start[r + 1] - c.start[r] : 0;
             for (int k = 0; k < w; k++) {
                 const int idx = e.ptr[s] + (k / T) * 32 + (k % T) * S + lr;
