@@ -294,7 +294,7 @@ void launch_grid_query(AdmmB200* h, bool write, int nq) {
     DevScene& s = h->s;
     const int g = blocks((int)std::min<int64_t>((int64_t)nq * h->query_lanes, INT32_MAX), kQueryThreads);
     switch (h->query_lanes * 2 + (write ? 1 : 0)) {
-        case 16: LAUNCH((k_grid_query<false, 8>), g, kQueryThreads, s); break;
+        case 16: LAUNCH(k_grid_count8, g, kQueryThreads, s); break;
         case 17: LAUNCH_P(ADMM_KERNEL_DCD_VF, (k_grid_query<true, 8>), g, kQueryThreads, s); break;
         case 32: LAUNCH((k_grid_query<false, 16>), g, kQueryThreads, s); break;
         case 33: LAUNCH_P(ADMM_KERNEL_DCD_VF, (k_grid_query<true, 16>), g, kQueryThreads, s); break;
