@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "admm_b200.h"
+#include "umma.cuh"
 
 namespace {
 
@@ -65,6 +66,86 @@ __global__ void __launch_bounds__(256) k_dense_fwd(const float* __restrict__ X, 
     Z[(size_t)r * N + c] = acc;
     if (act == 1) Y[(size_t)r * N + c] = fmaxf(acc, 0.f);
     else if (act == 2) Y[(size_t)r * N + c] = res[(size_t)r * N + c] + fmaxf(acc, 0.f);
+}
+
+// The same layer on the tensor cores (tcgen05, kind::tf32, FP32 accumulation in
+// tensor memory) for N = 64 outputs: one CTA of 4 warps per 128 rows.  The
+// rows of X and the weights (rounded to BF16 first when bf16 is set) are
+// rounded to TF32 and staged in shared memory in the canonical K-major layout,
+// K padded with zeros to KP (a multiple of 8); thread 0 issues KP / 8 MMAs of
+// 128 x 64 x 8 into 64 TMEM columns and commits them to an mbarrier; each warp
+// then reads its 32 rows of the accumulator and applies bias and activation.
+// The wait for the MMAs is bounded: a wait that gives up sets err[0] and the
+// CTA releases its TMEM and leaves without writing.
+constexpr int kTcRows = 128, kTcN = 64;
+
+__global__ void __launch_bounds__(128) k_dense_fwd_tc(const float* __restrict__ X, int R, int K, int KP,
+                                                      const float* __restrict__ W, const float* __restrict__ b,
+                                                      float* __restrict__ Z, float* __restrict__ Y,
+                                                      const float* __restrict__ res, int act, int bf16,
+                                                      int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    const int C = KP / 4;  // 16-byte K chunks per row
+    unsigned char* As = tc_smem;
+    unsigned char* Bs = tc_smem + (size_t)kTcRows * KP * 4;
+    const int row0 = blockIdx.x * kTcRows;
+    for (int i = threadIdx.x; i < kTcRows * KP; i += blockDim.x) {
+        const int m = i / KP, k = i % KP;
+        const float v = (row0 + m < R && k < K) ? X[(size_t)(row0 + m) * K + k] : 0.f;
+        *(float*)(As + umma::core_offset(m, k >> 2, C) + (k & 3) * 4) = umma::tf32_round(v);
+    }
+    for (int i = threadIdx.x; i < kTcN * KP; i += blockDim.x) {
+        const int n = i / KP, k = i % KP;
+        const float v = k < K ? wval(W, n * K + k, bf16) : 0.f;
+        *(float*)(Bs + umma::core_offset(n, k >> 2, C) + (k & 3) * 4) = umma::tf32_round(v);
+    }
+    umma::fence_operands();
+    if (threadIdx.x == 0) umma::mbar_init(&mbar, 1);
+    if (threadIdx.x < 32) umma::tmem_alloc(&tmem_base, kTcN);
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t td = tmem_base;
+    if (threadIdx.x == 0) {
+        const uint32_t idesc = umma::idesc_tf32(kTcRows, kTcN);
+        const uint32_t a0 = umma::smem_u32(As), b0 = umma::smem_u32(Bs);
+        for (int k = 0; k < KP / 8; k++)  // 8 TF32 values of K = two 16-byte chunks per MMA
+            umma::mma_tf32(td, umma::smem_desc(a0 + 256u * k, C), umma::smem_desc(b0 + 256u * k, C), idesc, k > 0);
+        umma::commit(&mbar);
+    }
+    const bool ok = umma::mbar_wait(&mbar, 0, 1 << 22);
+    umma::fence_after();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = row0 + warp * 32 + lane;
+    if (ok) {
+        const uint32_t tw = td + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int c0 = 0; c0 < kTcN; c0 += 16) {
+            uint32_t r[16];
+            umma::tmem_load16(tw + c0, r);
+            umma::tmem_wait16(r);
+            if (row < R) {
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const int c = c0 + j;
+                    const float z = __uint_as_float(r[j]) + b[c];
+                    Z[(size_t)row * kTcN + c] = z;
+                    if (act == 1) Y[(size_t)row * kTcN + c] = fmaxf(z, 0.f);
+                    else if (act == 2) Y[(size_t)row * kTcN + c] = res[(size_t)row * kTcN + c] + fmaxf(z, 0.f);
+                }
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+    }
+    umma::fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        umma::fence_after();
+        umma::tmem_dealloc(td, kTcN);
+    }
 }
 
 // dX[R x K] = dZ[R x N] W  (W [N x K]).  Block: 4 rows x 256/4 threads over k.
@@ -330,6 +411,7 @@ struct AdmmGnn {
     float *gh = nullptr, *gh2 = nullptr, *gz = nullptr, *ginp = nullptr, *gnin = nullptr, *go = nullptr, *gB = nullptr;
     float *part = nullptr, *r = nullptr, *zv = nullptr, *res = nullptr, *gzv = nullptr;
     double *dots = nullptr, *scal = nullptr;
+    int* derr = nullptr;    // set by a tensor-core layer whose bounded wait gave up
     cudaStream_t st = nullptr;
     std::string err;
 };
@@ -372,8 +454,17 @@ int galloc(AdmmGnn* g, T** p, size_t count, bool graph) {
         if (r_) return r_;       \
     } while (0)
 
+// With BF16 weights the 64-output layers run on the tensor cores, the others
+// (and every layer with FP32 weights) on the SIMT kernel.
 void dense_fwd(AdmmGnn* g, const float* X, int R, int K, int wo, int bo, int N, float* Z, float* Y, const float* res,
                int act) {
+    if (g->bf16 && N == kTcN && R > 0) {
+        const int KP = (K + 7) / 8 * 8;
+        const size_t sm = sizeof(float) * (size_t)(kTcRows + kTcN) * KP;
+        k_dense_fwd_tc<<<nblk(R, kTcRows), 128, sm, g->st>>>(X, R, K, KP, g->theta + wo, g->theta + bo, Z, Y, res, act,
+                                                            g->bf16, g->derr);
+        return;
+    }
     const size_t sm = sizeof(float) * (size_t)(N * K + 4 * K);
     k_dense_fwd<<<nblk(R, 4), 256, sm, g->st>>>(X, R, K, g->theta + wo, g->theta + bo, N, Z, Y, res, act, g->bf16);
 }
@@ -402,6 +493,16 @@ void forward(AdmmGnn* g) {
     k_blocks<<<nblk(g->n, 256), 256, 0, g->st>>>(g->o, g->adiag, g->n, g->B);
 }
 
+// ADMM_ERR_TIMEOUT once a tensor-core layer gave up waiting for its MMAs (the
+// flag is cleared for the next call).
+int tc_status(AdmmGnn* g) {
+    int e = 0;
+    if (cudaMemcpy(&e, g->derr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ADMM_ERR_CUDA;
+    if (!e) return ADMM_OK;
+    cudaMemset(g->derr, 0, sizeof(int));
+    return ADMM_ERR_TIMEOUT;
+}
+
 }  // namespace
 
 extern "C" {
@@ -415,7 +516,8 @@ int admm_gnn_create(int bf16, AdmmGnn** out) {
     g->P = offsets().total;
     int rc;
     if ((rc = galloc(g, &g->theta, g->P, false)) || (rc = galloc(g, &g->grad, g->P, false)) ||
-        (rc = galloc(g, &g->m, g->P, false)) || (rc = galloc(g, &g->v, g->P, false))) {
+        (rc = galloc(g, &g->m, g->P, false)) || (rc = galloc(g, &g->v, g->P, false)) ||
+        (rc = galloc(g, &g->derr, 1, false))) {
         admm_gnn_destroy(g);
         return rc;
     }
@@ -425,6 +527,7 @@ int admm_gnn_create(int bf16, AdmmGnn** out) {
     }
     cudaFuncSetAttribute(k_dense_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     cudaFuncSetAttribute(k_dense_dx, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(k_dense_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     *out = g;
     return ADMM_OK;
 }
@@ -518,7 +621,8 @@ int admm_gnn_forward(AdmmGnn* g, float* blocks9) {
     if (blocks9 && cudaMemcpyAsync(blocks9, g->B, sizeof(float) * 9 * (size_t)g->n, cudaMemcpyDeviceToHost, g->st) != cudaSuccess)
         return ADMM_ERR_CUDA;
     if (cudaStreamSynchronize(g->st) != cudaSuccess) return ADMM_ERR_CUDA;
-    return cudaGetLastError() == cudaSuccess ? ADMM_OK : ADMM_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return ADMM_ERR_CUDA;
+    return tc_status(g);
 }
 
 // Loss mean_k |A B r_k - r_k|^2 / |r_k|^2 over K residual samples (host, K x n x 3)
@@ -568,7 +672,7 @@ int admm_gnn_loss_grad(AdmmGnn* g, const float* R, int K, double* loss, float* g
     if (grad) cudaMemcpyAsync(grad, g->grad, sizeof(float) * g->P, cudaMemcpyDeviceToHost, g->st);
     if (cudaStreamSynchronize(g->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ADMM_ERR_CUDA;
     if (loss) *loss = total;
-    return ADMM_OK;
+    return tc_status(g);
 }
 
 // One Adam step on the gradient of the last admm_gnn_loss_grad.

@@ -38,6 +38,38 @@ def test_gradient_matches_the_restatement():
     net.close()
 
 
+def _bf16(a):
+    """Round float32 values to the nearest BF16 (ties to even), kept as float32."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32)
+
+
+def test_tensor_core_layers_match_the_restatement():
+    """With BF16 weights the 64-output layers run on the tensor cores (tcgen05, TF32 operands,
+    FP32 accumulation in tensor memory): the blocks agree with the FP64 restatement evaluated
+    with the same BF16-rounded weights, within the TF32 rounding of the activations."""
+    sc, h, sysm, x, ef = _cube_system(6, seed=4)
+    rng = np.random.default_rng(5)
+    theta = (G.init_params(7) + rng.normal(scale=0.05, size=G.n_params())).astype(np.float32)
+    net = gnn.LearnedPreconditioner(bf16=True)
+    net.set_params(theta)
+    Bg = net.blocks(sysm, x, ef).reshape(-1, 3, 3)
+    net.close()
+    # the restatement with the weights (not the biases) rounded to BF16
+    parts, k = [], 0
+    for shp in G.param_shapes():
+        n = int(np.prod(shp))
+        blk = theta[k:k + n]
+        parts.append(_bf16(blk) if len(shp) == 2 else blk)
+        k += n
+    th = np.concatenate(parts).astype(np.float64)
+    Bo, _ = G.forward(th, x.astype(np.float64), ef.astype(np.float64), sysm.start, sysm.col,
+                      sysm.diag.astype(np.float64))
+    err = np.abs(Bg - Bo).max() / np.abs(Bo).max()
+    assert err <= 1e-2, err
+
+
 def test_bf16_weights_stay_close():
     sc, h, sysm, x, ef = _cube_system(5, seed=1)
     rng = np.random.default_rng(2)
