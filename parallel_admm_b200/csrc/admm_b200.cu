@@ -43,6 +43,7 @@ struct AdmmB200 {
     int tet_blocks = 0, tri_blocks = 0, bend_blocks = 0, pin_blocks = 0;
     int contact_grid = 1;
     int group_grid = 1;             // blocks of the kernels that walk the touched list in lane groups
+    int pass_grid = 1;              // blocks of the fused projection passes (a warp per contact)
     int warp_grid = 1;              // blocks of the kernels that walk it one warp per vertex
     int* hist = nullptr;       // radix histograms
     int sort_max = 0;
@@ -390,10 +391,19 @@ int enqueue_contact(AdmmB200* h, bool dual) {
     const int split = blocks(s.nd, kVertThreads);
     if (dual) LAUNCH(k_contact_p<true>, split + h->group_grid, kVertThreads, s, split);
     else LAUNCH(k_contact_p<false>, split + h->group_grid, kVertThreads, s, split);
-    for (int g = 0; g < h->gs_iter; g++) {
-        LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
-        LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, h->group_grid, kContactThreads, s);
-    }
+    const int G = h->gs_iter;
+    if (G <= 0) return ADMM_OK;
+    // pass 1 projects from s.p into s.du; pass g = 2..G rebuilds p of pass g-1
+    // (P[g-1]) from P[g-2] and D[g-1] and projects into D[g]; the last gather
+    // writes P[G] into s.p.  P[j] = s.p for even j, s.p2 for odd j; D[j] = s.du
+    // for odd j, s.du2 for even j.
+    auto P = [&](int j) { return (j & 1) ? s.p2 : s.p; };
+    auto D = [&](int j) { return (j & 1) ? s.du : s.du2; };
+    LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
+    for (int g = 2; g <= G; g++)
+        LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_pass, h->pass_grid, kContactThreads, s, P(g - 2), P(g - 1),
+                 D(g - 1), D(g));
+    LAUNCH_P(ADMM_KERNEL_CONTACT_GATHER, k_contact_gather, h->group_grid, kContactThreads, s, P(G - 1), D(G));
     return ADMM_OK;
 }
 
@@ -1297,6 +1307,8 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.ginc, 4 * (size_t)s.cap));
     TRY(dalloc(h, &s.vtmp, 4 * (size_t)s.cap));
     TRY(dalloc(h, &s.du, s.cap));
+    TRY(dalloc(h, &s.du2, s.cap));
+    TRY(dalloc(h, &s.p2, n));
     TRY(dalloc(h, &s.vcnt, n));
     TRY(dalloc(h, &s.vfill, n));
     TRY(dalloc(h, &s.vstart, n + 1));
@@ -1320,6 +1332,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.done, 4));
     h->contact_grid = std::max(1, std::min(blocks(s.cap, kContactThreads), 2 * 148));
     h->group_grid = std::max(1, std::min(blocks(std::min(n, 4 * s.cap) * kGatherLanes, kContactThreads), 8 * 148));
+    h->pass_grid = std::max(1, std::min(blocks(s.cap * 32, kContactThreads), 8 * 148));
     h->warp_grid = std::max(1, std::min(blocks(std::min(n, 4 * s.cap) * 32, kContactThreads), 8 * 148));
     TRY(dalloc(h, &s.tpos, n));
     TRY(dalloc(h, &s.tv, n));

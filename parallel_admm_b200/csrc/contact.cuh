@@ -172,11 +172,10 @@ ADMM_DEV float4 friction_cone_du(const DevScene& s, int c, float ux, float uy, f
     return f4(uN * n.x + tx - ux, uN * n.y + ty - uy, uN * n.z + tz - uz);
 }
 
-// u_c = sum_k bary_k p_k + K_c for contact c, from the p values in `p`.
-ADMM_DEV void contact_u(const DevScene& s, int c, const float4* __restrict__ p, float& ux, float& uy, float& uz) {
-    const int4 q = s.pairs[c];
+// u_c = sum_k bary_k p_k + K_c for contact c from the p values of its four vertices.
+ADMM_DEV void contact_u_of(const DevScene& s, int c, float4 p0, float4 p1, float4 p2, float4 p3, float& ux,
+                           float& uy, float& uz) {
     const float4 b = s.bary[c];
-    const float4 p0 = p[q.x], p1 = p[q.y], p2 = p[q.z], p3 = p[q.w];
     const float4 kc = s.kc[c];
     ux = b.x * p0.x + b.y * p1.x + b.z * p2.x + b.w * p3.x;
     uy = b.x * p0.y + b.y * p1.y + b.z * p2.y + b.w * p3.y;
@@ -184,6 +183,12 @@ ADMM_DEV void contact_u(const DevScene& s, int c, const float4* __restrict__ p, 
     ux = ux + kc.x;
     uy = uy + kc.y;
     uz = uz + kc.z;
+}
+
+// u_c from the p values in `p`.
+ADMM_DEV void contact_u(const DevScene& s, int c, const float4* __restrict__ p, float& ux, float& uy, float& uz) {
+    const int4 q = s.pairs[c];
+    contact_u_of(s, c, p[q.x], p[q.y], p[q.z], p[q.w], ux, uy, uz);
 }
 
 __global__ void __launch_bounds__(kContactThreads) k_contact_du(DevScene s) {
@@ -199,10 +204,11 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_du(DevScene s) {
     }
 }
 
-// p_i += sum_c Gamma_c,i du_c over the incidence list of vertex i (update_p,
-// contact_solver.cu:381-399), kGatherLanes lanes per vertex with contacts
-// (grid-stride over the touched list; static vertices skipped).
-__global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s) {
+// p_i = p_src_i + sum_c Gamma_c,i du_c over the incidence list of vertex i
+// (update_p, contact_solver.cu:381-399) into s.p, kGatherLanes lanes per vertex
+// with contacts (grid-stride over the touched list; static vertices skipped).
+__global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s, const float4* __restrict__ p_src,
+                                                                   const float4* __restrict__ du) {
     ADMM_PDL_PROLOGUE();
     const int sub = threadIdx.x % kGatherLanes;
     const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kGatherLanes - 1));
@@ -212,13 +218,63 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s) 
     for (int t = g0; t < ntv; t += gs) {  // uniform per group
         const int i = s.tv[t];
         if (i >= s.nd) continue;
-        const float4 acc = gather_group(s, s.du, s.vstart[i], s.vstart[i + 1], sub, gmask);
+        const float4 acc = gather_group(s, du, s.vstart[i], s.vstart[i + 1], sub, gmask);
         if (sub == 0) {
-            float4 p = s.p[i];
+            float4 p = p_src[i];
             p.x += acc.x;
             p.y += acc.y;
             p.z += acc.z;
             s.p[i] = p;
+        }
+    }
+}
+
+// One projection pass fused with the gather of the previous one, a warp per
+// contact: the four lane groups of 8 rebuild p of the contact's four vertices
+// from p_old and the previous pass's du_old (the same sums, in the same order,
+// as k_contact_gather), the first contact of each vertex's incidence list
+// stores that p into p_new for the next pass, and lane 0 projects the contact
+// (du_new, r_c += du) from those p.  Static vertices keep p in s.p.  Replaces
+// a gather + projection pair of launches with one launch and one round trip.
+__global__ void __launch_bounds__(kContactThreads) k_contact_pass(DevScene s, const float4* __restrict__ p_old,
+                                                                 float4* __restrict__ p_new,
+                                                                 const float4* __restrict__ du_old,
+                                                                 float4* __restrict__ du_new) {
+    ADMM_PDL_PROLOGUE();
+    const int lane = threadIdx.x & 31, grp = lane >> 3, sub = lane & 7;
+    const unsigned gmask = 0xffu << (lane & ~7);
+    const int nc = ccount(s);
+    const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, ws = (gridDim.x * blockDim.x) >> 5;
+    for (int c = w0; c < nc; c += ws) {  // uniform per warp
+        const int4 q = s.pairs[c];
+        const int v = grp == 0 ? q.x : grp == 1 ? q.y : grp == 2 ? q.z : q.w;
+        float4 pv;
+        if (v >= s.nd) {  // uniform per group
+            pv = s.p[v];
+        } else {
+            const int b = s.vstart[v];
+            const float4 acc = gather_group(s, du_old, b, s.vstart[v + 1], sub, gmask);
+            pv = p_old[v];
+            pv.x += acc.x;
+            pv.y += acc.y;
+            pv.z += acc.z;
+            if (sub == 0 && __float_as_int(s.ginc[b].x) == c) p_new[v] = pv;
+        }
+        const float4 p0 = f4(__shfl_sync(0xffffffffu, pv.x, 0), __shfl_sync(0xffffffffu, pv.y, 0),
+                             __shfl_sync(0xffffffffu, pv.z, 0));
+        const float4 p1 = f4(__shfl_sync(0xffffffffu, pv.x, 8), __shfl_sync(0xffffffffu, pv.y, 8),
+                             __shfl_sync(0xffffffffu, pv.z, 8));
+        const float4 p2 = f4(__shfl_sync(0xffffffffu, pv.x, 16), __shfl_sync(0xffffffffu, pv.y, 16),
+                             __shfl_sync(0xffffffffu, pv.z, 16));
+        const float4 p3 = f4(__shfl_sync(0xffffffffu, pv.x, 24), __shfl_sync(0xffffffffu, pv.y, 24),
+                             __shfl_sync(0xffffffffu, pv.z, 24));
+        if (lane == 0) {
+            float ux, uy, uz;
+            contact_u_of(s, c, p0, p1, p2, p3, ux, uy, uz);
+            const float4 r = s.rc[c];
+            const float4 d = friction_cone_du(s, c, ux, uy, uz, r);
+            du_new[c] = d;
+            s.rc[c] = f4(r.x + d.x, r.y + d.y, r.z + d.z);
         }
     }
 }

@@ -128,6 +128,8 @@ struct DevScene {
     float* cmu = nullptr;                 // [cap] friction coefficient per contact
     const float* vmu = nullptr;           // [n] per-vertex coefficient, or null
     float4* du = nullptr;
+    float4* du2 = nullptr;  // [cap] second buffer of the fused projection passes
+    float4* p2 = nullptr;   // [n] second buffer of p in the fused projection passes
     int* vcnt = nullptr;                  // [n] contacts per vertex
     int* vfill = nullptr;                 // [n]
     int* vstart = nullptr;                // [n+1]
