@@ -78,7 +78,8 @@ def make_scene(args, rank=0):
     c = CONFIGS[args.config]
     kw = dict(c["kw"])
     if c.get("per_rank_seed"):
-        kw["seed"] = kw.get("seed", 0) + rank
+        from parallel_admm_b200 import replicas as R
+        kw["seed"] = R.rank_seed(kw.get("seed", 0), rank)
     sc = getattr(scene, c["fn"])(**kw)
     sc.params.jacobi_mode = args.jacobi_mode
     sc.params.ell_lanes = args.ell_lanes
@@ -292,6 +293,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     from parallel_admm_b200 import backend as B
+    from parallel_admm_b200 import replicas as R
 
     sc = make_scene(args, rank)
     h = B.Handle(sc, device=local, residual_tol=args.tol)
@@ -339,12 +341,9 @@ def main():
     clocks = clk.summary()
     probe_ms, probe_n = h.probe_time()
     total_ms = float(np.sum(dev_ms))
-    t = torch.tensor([total_ms], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_total_ms = float(t.item())
+    max_total_ms = R.max_over_ranks(total_ms, f"cuda:{local}")
     ms_per_step = max_total_ms / args.steps
-    value = world * args.steps / (max_total_ms / 1e3)
+    value = R.job_throughput(args.steps, world, max_total_ms / 1e3)
 
     # end to end through the public C ABI: pinned host buffers in, one substep, host buffers out
     h.reset()
@@ -361,10 +360,7 @@ def main():
         e2e_s += time.perf_counter() - t0
         x_in[:] = x_out
         v_in[:] = v_out
-    te = torch.tensor([e2e_s], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / float(te.item())
+    e2e_value = R.job_throughput(args.steps, world, R.max_over_ranks(e2e_s, f"cuda:{local}"))
     bytes_io = 2 * sc.n_vert * 3 * 4
 
     # Device time per phase inside the step graph (events at phase changes, so the launch gaps
