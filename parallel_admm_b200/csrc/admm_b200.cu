@@ -748,21 +748,47 @@ struct TuneKey {
 std::mutex g_tune_mu;
 std::vector<std::pair<TuneKey, std::pair<int, float>>> g_tune_cache;
 
+// Device time of one Jacobi sweep (which = 0) or RHS launch (1) at the current
+// lane count, as the step graph runs them: a graph of kTuneLaunches dependent
+// launches (sweeps ping-pong between the two iterate buffers) with programmatic
+// dependent launch between them, run once to warm up and then kTuneReps times;
+// the fastest repetition counts.  Ten stream launches timed once ranked lane
+// counts that lie within a few per cent of each other in the wrong order.
 int time_ell(AdmmB200* h, int which, float* ms_per_launch) {
+    constexpr int kTuneLaunches = 40, kTuneReps = 3;
     DevScene& s = h->s;
-    if (which == 0) launch_jacobi(h, s.x, s.jac[0]);
-    else launch_rhs(h, false);
-    CK(cudaEventRecord(h->ev0, h->stream));
-    for (int r = 0; r < 10; r++) {
-        if (which == 0) launch_jacobi(h, s.x, s.jac[0]);
+    const cudaStream_t keep = h->cstream;
+    const int counter = h->launch_counter;
+    h->cstream = h->stream;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int r = 0; r < kTuneLaunches; r++) {
+        if (which == 0) launch_jacobi(h, r == 0 ? s.x : s.jac[(r + 1) & 1], s.jac[r & 1]);
         else launch_rhs(h, false);
     }
-    CK(cudaEventRecord(h->ev1, h->stream));
-    CK(cudaEventSynchronize(h->ev1));
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+    h->cstream = keep;
+    h->launch_counter = counter;
+    CK(ce);
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    CK(ie);
+    float best = 1e30f;
+    cudaError_t e = cudaGraphLaunch(ge, h->stream);
+    for (int k = 0; k < kTuneReps && e == cudaSuccess; k++) {
+        e = cudaEventRecord(h->ev0, h->stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(ge, h->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(h->ev1, h->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(h->ev1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        if (e == cudaSuccess) best = std::min(best, ms);
+    }
+    cudaGraphExecDestroy(ge);
+    CK(e);
     CK(cudaGetLastError());
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-    *ms_per_launch = ms / 10.f;
+    *ms_per_launch = best / (float)kTuneLaunches;
     return ADMM_OK;
 }
 

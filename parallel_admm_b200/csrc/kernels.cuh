@@ -302,77 +302,99 @@ ADMM_DEV float4 ell_row_sum(const SlicedEll& M, const float4* __restrict__ v, in
 // SAVE_PREV also keeps x before the solve (for the dual residual).
 // ---------------------------------------------------------------------------
 // b_i from the row sum acc = (h^2 D^T W^2 (z - Ue))_i.
-template <bool SAVE_PREV>
-ADMM_DEV void rhs_row(const DevScene& s, int i, float4 acc) {
-    const float4 m = s.mxt[i];
+ADMM_DEV float4 rhs_value(const DevScene& s, float4 acc, float4 m, float4 p, float4 x0, float4 uc, float wc) {
     float4 bi = f4(m.x + acc.x, m.y + acc.y, m.z + acc.z);
     if (s.contact) {
-        const float4 p = s.p[i], x0 = s.x0[i], uc = s.uc[i];
-        const float wc = s.dt2wc[i];
         bi.x = bi.x + wc * ((p.x * s.dt + x0.x) - uc.x);
         bi.y = bi.y + wc * ((p.y * s.dt + x0.y) - uc.y);
         bi.z = bi.z + wc * ((p.z * s.dt + x0.z) - uc.z);
     }
-    s.b[i] = bi;
+    return bi;
+}
+
+template <bool SAVE_PREV>
+ADMM_DEV void rhs_row(const DevScene& s, int i, float4 acc) {
+    const float4 z = f4(0.f, 0.f, 0.f);
+    const bool c = s.contact;
+    s.b[i] = rhs_value(s, acc, s.mxt[i], c ? s.p[i] : z, c ? s.x0[i] : z, c ? s.uc[i] : z, c ? s.dt2wc[i] : 0.f);
     if (SAVE_PREV) s.xprev[i] = s.x[i];
 }
 
-// ell_row_sum with the matrix entries of the lane's first kPrefetch steps loaded
-// before the programmatic-dependency wait (the matrix is constant), the gathered
-// vector after it.  Same operations in the same order as ell_row_sum.
+// ell_row_sum in two parts around the programmatic-dependency wait: load()
+// reads the lane's row index and the matrix entries of its first kPrefetch
+// steps (the matrix is constant, so before the wait), sum() the gathered vector
+// and the rest of the row (after it).  Between the two a kernel loads its own
+// per-row operands, so that they travel in parallel with the gathers instead of
+// after the row sum.  Same operations in the same order as ell_row_sum.
 constexpr int kPrefetch = 8;
 
 template <int T>
-ADMM_DEV float4 ell_row_sum_pf(const SlicedEll& M, const float4* __restrict__ v, int w, int lane, int& row) {
-    constexpr int S = 32 / T;
-    row = M.rowid ? __ldg(&M.rowid[w * S + (lane % S)]) : w * S + (lane % S);
-    const int b = M.ptr[w], e = M.ptr[w + 1];
+struct EllRowPf {
+    static constexpr int S = 32 / T;
+    int row, b, e;
     int cc[kPrefetch];
     float vv[kPrefetch];
+
+    ADMM_DEV void load(const SlicedEll& M, int w, int lane) {
+        row = M.rowid ? __ldg(&M.rowid[w * S + (lane % S)]) : w * S + (lane % S);
+        b = M.ptr[w];
+        e = M.ptr[w + 1];
 #pragma unroll
-    for (int j = 0; j < kPrefetch; j++) {
-        const int k = b + lane + 32 * j;
-        cc[j] = k < e ? __ldg(&M.col[k]) : 0;
-        vv[j] = k < e ? __ldg(&M.val[k]) : 0.f;
-    }
-    ADMM_PDL_WAIT();
-    float ax = 0.f, ay = 0.f, az = 0.f;
-#pragma unroll
-    for (int j = 0; j < kPrefetch; j++) {
-        if (b + lane + 32 * j < e) {
-            const float4 q = v[cc[j]];
-            ax = fmaf(vv[j], q.x, ax);
-            ay = fmaf(vv[j], q.y, ay);
-            az = fmaf(vv[j], q.z, az);
+        for (int j = 0; j < kPrefetch; j++) {
+            const int k = b + lane + 32 * j;
+            cc[j] = k < e ? __ldg(&M.col[k]) : 0;
+            vv[j] = k < e ? __ldg(&M.val[k]) : 0.f;
         }
     }
-    for (int k = b + lane + 32 * kPrefetch; k < e; k += 32) {
-        const int c = __ldg(&M.col[k]);
-        const float a = __ldg(&M.val[k]);
-        const float4 q = v[c];
-        ax = fmaf(a, q.x, ax);
-        ay = fmaf(a, q.y, ay);
-        az = fmaf(a, q.z, az);
-    }
+
+    ADMM_DEV float4 sum(const SlicedEll& M, const float4* __restrict__ v, int lane) const {
+        float ax = 0.f, ay = 0.f, az = 0.f;
 #pragma unroll
-    for (int o = S; o < 32; o <<= 1) {
-        ax += __shfl_xor_sync(0xffffffffu, ax, o);
-        ay += __shfl_xor_sync(0xffffffffu, ay, o);
-        az += __shfl_xor_sync(0xffffffffu, az, o);
+        for (int j = 0; j < kPrefetch; j++) {
+            if (b + lane + 32 * j < e) {
+                const float4 q = v[cc[j]];
+                ax = fmaf(vv[j], q.x, ax);
+                ay = fmaf(vv[j], q.y, ay);
+                az = fmaf(vv[j], q.z, az);
+            }
+        }
+        for (int k = b + lane + 32 * kPrefetch; k < e; k += 32) {
+            const int c = __ldg(&M.col[k]);
+            const float a = __ldg(&M.val[k]);
+            const float4 q = v[c];
+            ax = fmaf(a, q.x, ax);
+            ay = fmaf(a, q.y, ay);
+            az = fmaf(a, q.z, az);
+        }
+#pragma unroll
+        for (int o = S; o < 32; o <<= 1) {
+            ax += __shfl_xor_sync(0xffffffffu, ax, o);
+            ay += __shfl_xor_sync(0xffffffffu, ay, o);
+            az += __shfl_xor_sync(0xffffffffu, az, o);
+        }
+        return f4(ax, ay, az);
     }
-    return f4(ax, ay, az);
-}
+};
 
 template <int T, bool SAVE_PREV>
 __global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
-    ADMM_PDL_PROLOGUE();
+    ADMM_PDL_TRIGGER();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= s.R.nslices) return;
-    int i;
-    const float4 acc = ell_row_sum<T>(s.R, s.y, w, lane, i);
-    if (lane >= 32 / T || i >= s.nd) return;
-    rhs_row<SAVE_PREV>(s, i, acc);
+    EllRowPf<T> r;
+    r.load(s.R, w, lane);
+    const int i = r.row;
+    const bool own = i < s.nd, c = own && s.contact;
+    const float wc = c ? __ldg(&s.dt2wc[i]) : 0.f;
+    ADMM_PDL_WAIT();
+    const float4 z = f4(0.f, 0.f, 0.f);
+    const float4 m = own ? s.mxt[i] : z, p = c ? s.p[i] : z, x0 = c ? s.x0[i] : z, uc = c ? s.uc[i] : z;
+    const float4 xi = SAVE_PREV && own ? s.x[i] : z;
+    const float4 acc = r.sum(s.R, s.y, lane);
+    if (lane >= 32 / T || !own) return;
+    s.b[i] = rhs_value(s, acc, m, p, x0, uc, wc);
+    if (SAVE_PREV) s.xprev[i] = xi;
 }
 
 // dst_i = (b_i - acc) / a_ii
@@ -394,10 +416,16 @@ __global__ void __launch_bounds__(kVertThreads) k_jacobi(DevScene s, const float
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= s.A.nslices) return;
-    int i;
-    const float4 acc = ell_row_sum_pf<T>(s.A, src, w, lane, i);
-    if (lane >= 32 / T || i >= s.nd) return;
-    jacobi_row(s, i, acc, dst);
+    EllRowPf<T> r;
+    r.load(s.A, w, lane);
+    const int i = r.row;
+    const bool own = i < s.nd;
+    const float d = own ? __ldg(&s.a_diag[i]) : 1.f;  // A is constant: before the wait
+    ADMM_PDL_WAIT();
+    const float4 bi = own ? s.b[i] : f4(0.f, 0.f, 0.f);
+    const float4 acc = r.sum(s.A, src, lane);
+    if (lane >= 32 / T || !own) return;
+    dst[i] = f4((bi.x - acc.x) / d, (bi.y - acc.y) / d, (bi.z - acc.z) / d);
 }
 
 // ---------------------------------------------------------------------------
