@@ -1358,9 +1358,10 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     TRY(dalloc(h, &s.done, 4));
     h->contact_grid = std::max(1, std::min(blocks(s.cap, kContactThreads), 2 * 148));
     h->group_grid = std::max(1, std::min(blocks(std::min(n, 4 * s.cap) * kGatherLanes, kContactThreads), 8 * 148));
-    // four blocks per SM: a warp per contact over a grid-stride loop; with a few hundred contacts
-    // most blocks only start and exit, and 8 * 148 of them cost a quarter more per launch
-    h->pass_grid = std::max(1, std::min(blocks(s.cap * 32, kContactThreads), 4 * 148));
+    // one wave of three blocks per SM (the pass holds 74 registers per thread): a warp per contact
+    // over a grid-stride loop; with a few hundred contacts most blocks only start and exit, and
+    // 8 * 148 of them cost a quarter more per launch than 4 * 148
+    h->pass_grid = std::max(1, std::min(blocks(s.cap * 32, kContactThreads), 3 * 148));
     h->warp_grid = std::max(1, std::min(blocks(std::min(n, 4 * s.cap) * 32, kContactThreads), 8 * 148));
     TRY(dalloc(h, &s.tpos, n));
     TRY(dalloc(h, &s.tv, n));

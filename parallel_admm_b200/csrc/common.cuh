@@ -18,6 +18,15 @@
 #define ADMM_PDL_TRIGGER() asm volatile("griddepcontrol.launch_dependents;" ::: "memory")
 #define ADMM_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
 
+// Wait first, then let the next kernel launch: the next kernel then starts only
+// after this kernel's predecessor has completed, so before its own wait it may
+// read (through L2) anything that the kernels before this one wrote.
+#define ADMM_PDL_WAIT_THEN_TRIGGER()                                 \
+    do {                                                             \
+        asm volatile("griddepcontrol.wait;" ::: "memory");           \
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); \
+    } while (0)
+
 #define ADMM_PDL_PROLOGUE()                                          \
     do {                                                             \
         asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); \

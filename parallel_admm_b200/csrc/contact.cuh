@@ -151,16 +151,16 @@ ADMM_DEV float4 gather_group(const DevScene& s, const float4* __restrict__ v, in
     return f4(ax, ay, az);
 }
 
-// Projection of u = sum_k bary_k p_k + K_c onto the friction cone for contact c
-// with accumulated correction r: returns du (the caller sets r_c = r + du).
-ADMM_DEV float4 friction_cone_du(const DevScene& s, int c, float ux, float uy, float uz, float4 r) {
-    const float4 n = s.nrm[c];
+// Projection of u = sum_k bary_k p_k + K_c onto the friction cone of normal n
+// and coefficient mu with accumulated correction r: returns du (the caller sets
+// r_c = r + du).
+ADMM_DEV float4 cone_du(float4 n, float mu, float ux, float uy, float uz, float4 r) {
     const float sx = ux - r.x, sy = uy - r.y, sz = uz - r.z;
     float uN = n.x * sx + n.y * sy + n.z * sz;
     float tx = sx - uN * n.x, ty = sy - uN * n.y, tz = sz - uN * n.z;
     if (uN < 0.f) {
         const float tau = sqrtf(tx * tx + ty * ty + tz * tz);
-        const float alpha = -s.cmu[c] * uN;
+        const float alpha = -mu * uN;
         uN = 0.f;
         if (tau <= alpha) {
             tx = ty = tz = 0.f;
@@ -172,11 +172,9 @@ ADMM_DEV float4 friction_cone_du(const DevScene& s, int c, float ux, float uy, f
     return f4(uN * n.x + tx - ux, uN * n.y + ty - uy, uN * n.z + tz - uz);
 }
 
-// u_c = sum_k bary_k p_k + K_c for contact c from the p values of its four vertices.
-ADMM_DEV void contact_u_of(const DevScene& s, int c, float4 p0, float4 p1, float4 p2, float4 p3, float& ux,
-                           float& uy, float& uz) {
-    const float4 b = s.bary[c];
-    const float4 kc = s.kc[c];
+// u = sum_k bary_k p_k + K_c from the p values of the contact's four vertices.
+ADMM_DEV void contact_u_bk(float4 b, float4 kc, float4 p0, float4 p1, float4 p2, float4 p3, float& ux, float& uy,
+                           float& uz) {
     ux = b.x * p0.x + b.y * p1.x + b.z * p2.x + b.w * p3.x;
     uy = b.x * p0.y + b.y * p1.y + b.z * p2.y + b.w * p3.y;
     uz = b.x * p0.z + b.y * p1.z + b.z * p2.z + b.w * p3.z;
@@ -185,20 +183,42 @@ ADMM_DEV void contact_u_of(const DevScene& s, int c, float4 p0, float4 p1, float
     uz = uz + kc.z;
 }
 
-// u_c from the p values in `p`.
-ADMM_DEV void contact_u(const DevScene& s, int c, const float4* __restrict__ p, float& ux, float& uy, float& uz) {
-    const int4 q = s.pairs[c];
-    contact_u_of(s, c, p[q.x], p[q.y], p[q.z], p[q.w], ux, uy, uz);
+// What only a detection writes about contact c (vertices, barycentric weights,
+// K_c, normal, friction coefficient), read through L2 (ld.global.cg): the
+// projection kernels load it before their dependency wait, when no line that
+// L1 may hold from before the detection must be read.
+struct ContactRec {
+    int4 q;
+    float4 b, kc, n;
+    float mu;
+};
+
+ADMM_DEV ContactRec contact_rec(const DevScene& s, int c) {
+    ContactRec r;
+    r.q = __ldcg(&s.pairs[c]);
+    r.b = __ldcg(&s.bary[c]);
+    r.kc = __ldcg(&s.kc[c]);
+    r.n = __ldcg(&s.nrm[c]);
+    r.mu = __ldcg(&s.cmu[c]);
+    return r;
 }
 
+// First projection of an ADMM iteration, a thread per contact, from s.p into
+// s.du (get_delta_u_kernel, contact_solver.cu:337-379).  k_contact_p before it
+// waits before it triggers, so the detection has completed when this kernel
+// starts: the contact records are loaded before the wait, only p and r_c after.
 __global__ void __launch_bounds__(kContactThreads) k_contact_du(DevScene s) {
-    ADMM_PDL_PROLOGUE();
-    const int nc = ccount(s);
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-        float ux, uy, uz;
-        contact_u(s, c, s.p, ux, uy, uz);
+    const int c0 = blockIdx.x * blockDim.x + threadIdx.x, cs = gridDim.x * blockDim.x;
+    const int nc = __ldcg(s.nc);
+    ContactRec R0 = {};
+    if (c0 < nc) R0 = contact_rec(s, c0);
+    ADMM_PDL_WAIT_THEN_TRIGGER();
+    for (int c = c0; c < nc; c += cs) {
+        const ContactRec R = c == c0 ? R0 : contact_rec(s, c);
         const float4 r = s.rc[c];
-        const float4 d = friction_cone_du(s, c, ux, uy, uz, r);
+        float ux, uy, uz;
+        contact_u_bk(R.b, R.kc, s.p[R.q.x], s.p[R.q.y], s.p[R.q.z], s.p[R.q.w], ux, uy, uz);
+        const float4 d = cone_du(R.n, R.mu, ux, uy, uz, r);
         s.du[c] = d;
         s.rc[c] = f4(r.x + d.x, r.y + d.y, r.z + d.z);
     }
@@ -207,25 +227,148 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_du(DevScene s) {
 // p_i = p_src_i + sum_c Gamma_c,i du_c over the incidence list of vertex i
 // (update_p, contact_solver.cu:381-399) into s.p, kGatherLanes lanes per vertex
 // with contacts (grid-stride over the touched list; static vertices skipped).
+// The pass before it waits before it triggers: the touched list, the list
+// bounds and the first two incidence entries of each lane (detection data) are
+// loaded before the wait.
 __global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s, const float4* __restrict__ p_src,
                                                                    const float4* __restrict__ du) {
-    ADMM_PDL_PROLOGUE();
+    ADMM_PDL_TRIGGER();
     const int sub = threadIdx.x % kGatherLanes;
     const unsigned gmask = 0xffu << (threadIdx.x & 31 & ~(kGatherLanes - 1));
-    const int ntv = *s.ntv;
+    const int ntv = __ldcg(s.ntv);
     const int g0 = (blockIdx.x * blockDim.x + threadIdx.x) / kGatherLanes;
     const int gs = gridDim.x * blockDim.x / kGatherLanes;
+    int i0 = -1, b0 = 0, e0 = 0;
+    float2 gi0[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    if (g0 < ntv) {
+        i0 = __ldcg(&s.tv[g0]);
+        if (i0 < s.nd) {
+            b0 = __ldcg(&s.vstart[i0]);
+            e0 = __ldcg(&s.vstart[i0 + 1]);
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+                if (b0 + sub + j * kGatherLanes < e0) gi0[j] = __ldcg(&s.ginc[b0 + sub + j * kGatherLanes]);
+        }
+    }
+    ADMM_PDL_WAIT();
     for (int t = g0; t < ntv; t += gs) {  // uniform per group
-        const int i = s.tv[t];
+        const bool first = t == g0;
+        const int i = first ? i0 : s.tv[t];
         if (i >= s.nd) continue;
-        const float4 acc = gather_group(s, du, s.vstart[i], s.vstart[i + 1], sub, gmask);
+        const int b = first ? b0 : s.vstart[i], e = first ? e0 : s.vstart[i + 1];
+        float4 p = p_src[i];
+        float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int k = b + sub + j * kGatherLanes;
+            if (k < e) {
+                const float2 gi = first ? gi0[j] : s.ginc[k];
+                const float4 d = du[__float_as_int(gi.x)];
+                ax = fmaf(d.x, gi.y, ax);
+                ay = fmaf(d.y, gi.y, ay);
+                az = fmaf(d.z, gi.y, az);
+            }
+        }
+        for (int k = b + sub + 2 * kGatherLanes; k < e; k += kGatherLanes) {
+            const float2 gi = s.ginc[k];
+            const float4 d = du[__float_as_int(gi.x)];
+            ax = fmaf(d.x, gi.y, ax);
+            ay = fmaf(d.y, gi.y, ay);
+            az = fmaf(d.z, gi.y, az);
+        }
+#pragma unroll
+        for (int o = kGatherLanes / 2; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(gmask, ax, o, kGatherLanes);
+            ay += __shfl_xor_sync(gmask, ay, o, kGatherLanes);
+            az += __shfl_xor_sync(gmask, az, o, kGatherLanes);
+        }
         if (sub == 0) {
-            float4 p = p_src[i];
-            p.x += acc.x;
-            p.y += acc.y;
-            p.z += acc.z;
+            p.x += ax;
+            p.y += ay;
+            p.z += az;
             s.p[i] = p;
         }
+    }
+}
+
+// What a projection pass reads of the detection for one contact and one lane
+// group (one of the contact's four vertices): the contact record, the vertex,
+// its incidence-list bounds and the lane's first entry, or p of a static
+// vertex (set before the contact step).  All through L2 (see ContactRec).
+struct PassRec {
+    ContactRec r;
+    int v, b, e;
+    float2 gi;
+    float4 pst;
+};
+
+ADMM_DEV PassRec pass_rec(const DevScene& s, int c, int grp, int sub) {
+    PassRec P;
+    P.r = contact_rec(s, c);
+    P.v = grp == 0 ? P.r.q.x : grp == 1 ? P.r.q.y : grp == 2 ? P.r.q.z : P.r.q.w;
+    P.b = P.e = 0;
+    P.gi = make_float2(0.f, 0.f);
+    P.pst = f4(0.f, 0.f, 0.f);
+    if (P.v >= s.nd) {
+        P.pst = __ldcg(&s.p[P.v]);
+    } else {
+        P.b = __ldcg(&s.vstart[P.v]);
+        P.e = __ldcg(&s.vstart[P.v + 1]);
+        if (P.b + sub < P.e) P.gi = __ldcg(&s.ginc[P.b + sub]);
+    }
+    return P;
+}
+
+// The pass for contact c, from its PassRec P.
+ADMM_DEV void pass_contact(const DevScene& s, int c, const PassRec& P, int lane, int sub, unsigned gmask,
+                           const float4* __restrict__ p_old, float4* __restrict__ p_new,
+                           const float4* __restrict__ du_old, float4* __restrict__ du_new) {
+    const float4 r = lane == 0 ? s.rc[c] : f4(0.f, 0.f, 0.f);  // issued beside the gathers
+    float4 pv;
+    if (P.v >= s.nd) {  // uniform per group
+        pv = P.pst;
+    } else {
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        const float4 po = p_old[P.v];
+        if (P.b + sub < P.e) {
+            const float4 d = du_old[__float_as_int(P.gi.x)];
+            ax = fmaf(d.x, P.gi.y, ax);
+            ay = fmaf(d.y, P.gi.y, ay);
+            az = fmaf(d.z, P.gi.y, az);
+        }
+        for (int k = P.b + sub + kGatherLanes; k < P.e; k += kGatherLanes) {
+            const float2 gi = s.ginc[k];
+            const float4 d = du_old[__float_as_int(gi.x)];
+            ax = fmaf(d.x, gi.y, ax);
+            ay = fmaf(d.y, gi.y, ay);
+            az = fmaf(d.z, gi.y, az);
+        }
+#pragma unroll
+        for (int o = kGatherLanes / 2; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(gmask, ax, o, kGatherLanes);
+            ay += __shfl_xor_sync(gmask, ay, o, kGatherLanes);
+            az += __shfl_xor_sync(gmask, az, o, kGatherLanes);
+        }
+        pv = po;
+        pv.x += ax;
+        pv.y += ay;
+        pv.z += az;
+        if (sub == 0 && __float_as_int(P.gi.x) == c) p_new[P.v] = pv;
+    }
+    const float4 p0 = f4(__shfl_sync(0xffffffffu, pv.x, 0), __shfl_sync(0xffffffffu, pv.y, 0),
+                         __shfl_sync(0xffffffffu, pv.z, 0));
+    const float4 p1 = f4(__shfl_sync(0xffffffffu, pv.x, 8), __shfl_sync(0xffffffffu, pv.y, 8),
+                         __shfl_sync(0xffffffffu, pv.z, 8));
+    const float4 p2 = f4(__shfl_sync(0xffffffffu, pv.x, 16), __shfl_sync(0xffffffffu, pv.y, 16),
+                         __shfl_sync(0xffffffffu, pv.z, 16));
+    const float4 p3 = f4(__shfl_sync(0xffffffffu, pv.x, 24), __shfl_sync(0xffffffffu, pv.y, 24),
+                         __shfl_sync(0xffffffffu, pv.z, 24));
+    if (lane == 0) {
+        float ux, uy, uz;
+        contact_u_bk(P.r.b, P.r.kc, p0, p1, p2, p3, ux, uy, uz);
+        const float4 d = cone_du(P.r.n, P.r.mu, ux, uy, uz, r);
+        du_new[c] = d;
+        s.rc[c] = f4(r.x + d.x, r.y + d.y, r.z + d.z);
     }
 }
 
@@ -236,47 +379,23 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s, 
 // stores that p into p_new for the next pass, and lane 0 projects the contact
 // (du_new, r_c += du) from those p.  Static vertices keep p in s.p.  Replaces
 // a gather + projection pair of launches with one launch and one round trip.
+// The kernel before it (k_contact_du or the previous pass) waits before it
+// triggers, so the detection data of the warp's first contact (PassRec) is
+// loaded before the wait; after it only du_old, p_old and r_c.
 __global__ void __launch_bounds__(kContactThreads) k_contact_pass(DevScene s, const float4* __restrict__ p_old,
-                                                                 float4* __restrict__ p_new,
+                                                                    float4* __restrict__ p_new,
                                                                  const float4* __restrict__ du_old,
                                                                  float4* __restrict__ du_new) {
-    ADMM_PDL_PROLOGUE();
     const int lane = threadIdx.x & 31, grp = lane >> 3, sub = lane & 7;
     const unsigned gmask = 0xffu << (lane & ~7);
-    const int nc = ccount(s);
+    const int nc = __ldcg(s.nc);
     const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, ws = (gridDim.x * blockDim.x) >> 5;
-    for (int c = w0; c < nc; c += ws) {  // uniform per warp
-        const int4 q = s.pairs[c];
-        const int v = grp == 0 ? q.x : grp == 1 ? q.y : grp == 2 ? q.z : q.w;
-        float4 pv;
-        if (v >= s.nd) {  // uniform per group
-            pv = s.p[v];
-        } else {
-            const int b = s.vstart[v];
-            const float4 acc = gather_group(s, du_old, b, s.vstart[v + 1], sub, gmask);
-            pv = p_old[v];
-            pv.x += acc.x;
-            pv.y += acc.y;
-            pv.z += acc.z;
-            if (sub == 0 && __float_as_int(s.ginc[b].x) == c) p_new[v] = pv;
-        }
-        const float4 p0 = f4(__shfl_sync(0xffffffffu, pv.x, 0), __shfl_sync(0xffffffffu, pv.y, 0),
-                             __shfl_sync(0xffffffffu, pv.z, 0));
-        const float4 p1 = f4(__shfl_sync(0xffffffffu, pv.x, 8), __shfl_sync(0xffffffffu, pv.y, 8),
-                             __shfl_sync(0xffffffffu, pv.z, 8));
-        const float4 p2 = f4(__shfl_sync(0xffffffffu, pv.x, 16), __shfl_sync(0xffffffffu, pv.y, 16),
-                             __shfl_sync(0xffffffffu, pv.z, 16));
-        const float4 p3 = f4(__shfl_sync(0xffffffffu, pv.x, 24), __shfl_sync(0xffffffffu, pv.y, 24),
-                             __shfl_sync(0xffffffffu, pv.z, 24));
-        if (lane == 0) {
-            float ux, uy, uz;
-            contact_u_of(s, c, p0, p1, p2, p3, ux, uy, uz);
-            const float4 r = s.rc[c];
-            const float4 d = friction_cone_du(s, c, ux, uy, uz, r);
-            du_new[c] = d;
-            s.rc[c] = f4(r.x + d.x, r.y + d.y, r.z + d.z);
-        }
-    }
+    PassRec P0 = {};
+    if (w0 < nc) P0 = pass_rec(s, w0, grp, sub);
+    ADMM_PDL_WAIT_THEN_TRIGGER();
+    if (w0 < nc) pass_contact(s, w0, P0, lane, sub, gmask, p_old, p_new, du_old, du_new);
+    for (int c = w0 + ws; c < nc; c += ws)  // uniform per warp
+        pass_contact(s, c, pass_rec(s, c, grp, sub), lane, sub, gmask, p_old, p_new, du_old, du_new);
 }
 
 }  // namespace admm

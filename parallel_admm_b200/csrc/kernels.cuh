@@ -239,9 +239,11 @@ ADMM_DEV float4 contact_p_base(const DevScene& s, int i) {
     return f4(((x.x - x0.x) + uc.x) * s.dt_inv, ((x.y - x0.y) + uc.y) * s.dt_inv, ((x.z - x0.z) + uc.z) * s.dt_inv);
 }
 
+// Waits before it triggers (so does every kernel of the projection passes after
+// it): each pass may load the detection's contact data before its own wait.
 template <bool DUALC>
 __global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s, int split) {
-    ADMM_PDL_PROLOGUE();
+    ADMM_PDL_WAIT_THEN_TRIGGER();
     if ((int)blockIdx.x < split) {
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i < s.nd && s.vstart[i] == s.vstart[i + 1]) s.p[i] = contact_p_base<DUALC>(s, i);
