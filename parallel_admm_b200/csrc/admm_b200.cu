@@ -1331,6 +1331,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         s.vmu = vm;
     }
     TRY(dalloc(h, &s.ginc, 4 * (size_t)s.cap));
+    TRY(dalloc(h, &s.cinc, 4 * (size_t)s.cap));
     TRY(dalloc(h, &s.vtmp, 4 * (size_t)s.cap));
     TRY(dalloc(h, &s.du, s.cap));
     TRY(dalloc(h, &s.du2, s.cap));
@@ -1365,6 +1366,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     h->warp_grid = std::max(1, std::min(blocks(std::min(n, 4 * s.cap) * 32, kContactThreads), 8 * 148));
     TRY(dalloc(h, &s.tpos, n));
     TRY(dalloc(h, &s.tv, n));
+    TRY(dalloc(h, &s.tvr, n));
     TRY(dalloc(h, &s.ntv, 1));
 
     h->tet_blocks = s.ntet ? blocks(s.ntet, kLocalThreads) : 0;

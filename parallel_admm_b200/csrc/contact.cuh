@@ -52,11 +52,17 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_fill(DevScene s) {
 constexpr int kRankSortRegs = 64;
 
 // The vertices with contacts, ascending: tv[tpos[i]] = i for vcnt[i] > 0
-// (tpos = exclusive scan of vcnt != 0, *ntv = their number).
+// (tpos = exclusive scan of vcnt != 0, *ntv = their number), and beside it the
+// vertex with its incidence-list bounds (tvr), which the gather loads in one
+// round trip.
 __global__ void __launch_bounds__(kContactThreads) k_contact_touched(DevScene s) {
     ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < s.n && s.vcnt[i] > 0) s.tv[s.tpos[i]] = i;
+    if (i < s.n && s.vcnt[i] > 0) {
+        const int t = s.tpos[i];
+        s.tv[t] = i;
+        s.tvr[t] = make_int4(i, s.vstart[i], s.vstart[i + 1], 0);
+    }
 }
 
 // One warp per vertex with contacts (grid-stride over the touched list).
@@ -111,6 +117,9 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_scc(DevScene s) {
         float mu = s.mu;
         if (s.vmu) mu = s.vmu[q.x < s.nd ? q.x : q.y < s.nd ? q.y : q.z < s.nd ? q.z : q.w];
         s.cmu[c] = mu;
+        const int v[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) s.cinc[4 * c + k] = make_int4(v[k], s.vstart[v[k]], s.vstart[v[k] + 1], 0);
     }
 }
 
@@ -240,11 +249,12 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s, 
     const int gs = gridDim.x * blockDim.x / kGatherLanes;
     int i0 = -1, b0 = 0, e0 = 0;
     float2 gi0[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    if (g0 < ntv) {
-        i0 = __ldcg(&s.tv[g0]);
-        if (i0 < s.nd) {
-            b0 = __ldcg(&s.vstart[i0]);
-            e0 = __ldcg(&s.vstart[i0 + 1]);
+    if (g0 < s.n) {  // tvr has n entries: loaded beside ntv, used below ntv only
+        const int4 r = __ldcg(&s.tvr[g0]);
+        if (g0 < ntv && r.x < s.nd) {
+            i0 = r.x;
+            b0 = r.y;
+            e0 = r.z;
 #pragma unroll
             for (int j = 0; j < 2; j++)
                 if (b0 + sub + j * kGatherLanes < e0) gi0[j] = __ldcg(&s.ginc[b0 + sub + j * kGatherLanes]);
@@ -253,9 +263,10 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_gather(DevScene s, 
     ADMM_PDL_WAIT();
     for (int t = g0; t < ntv; t += gs) {  // uniform per group
         const bool first = t == g0;
-        const int i = first ? i0 : s.tv[t];
-        if (i >= s.nd) continue;
-        const int b = first ? b0 : s.vstart[i], e = first ? e0 : s.vstart[i + 1];
+        const int4 r = first ? make_int4(i0, b0, e0, 0) : s.tvr[t];
+        const int i = first ? i0 : r.x;
+        if (i < 0 || i >= s.nd) continue;
+        const int b = r.y, e = r.z;
         float4 p = p_src[i];
         float ax = 0.f, ay = 0.f, az = 0.f;
 #pragma unroll
@@ -305,17 +316,14 @@ struct PassRec {
 ADMM_DEV PassRec pass_rec(const DevScene& s, int c, int grp, int sub) {
     PassRec P;
     P.r = contact_rec(s, c);
-    P.v = grp == 0 ? P.r.q.x : grp == 1 ? P.r.q.y : grp == 2 ? P.r.q.z : P.r.q.w;
-    P.b = P.e = 0;
+    const int4 ci = __ldcg(&s.cinc[4 * c + grp]);  // beside the record, not after it
+    P.v = ci.x;
+    P.b = ci.y;
+    P.e = ci.z;
     P.gi = make_float2(0.f, 0.f);
     P.pst = f4(0.f, 0.f, 0.f);
-    if (P.v >= s.nd) {
-        P.pst = __ldcg(&s.p[P.v]);
-    } else {
-        P.b = __ldcg(&s.vstart[P.v]);
-        P.e = __ldcg(&s.vstart[P.v + 1]);
-        if (P.b + sub < P.e) P.gi = __ldcg(&s.ginc[P.b + sub]);
-    }
+    if (P.v >= s.nd) P.pst = __ldcg(&s.p[P.v]);
+    else if (P.b + sub < P.e) P.gi = __ldcg(&s.ginc[P.b + sub]);
     return P;
 }
 
@@ -391,7 +399,7 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_pass(DevScene s, co
     const int nc = __ldcg(s.nc);
     const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, ws = (gridDim.x * blockDim.x) >> 5;
     PassRec P0 = {};
-    if (w0 < nc) P0 = pass_rec(s, w0, grp, sub);
+    if (w0 < s.cap) P0 = pass_rec(s, w0, grp, sub);  // in bounds; beside nc, used below nc only
     ADMM_PDL_WAIT_THEN_TRIGGER();
     if (w0 < nc) pass_contact(s, w0, P0, lane, sub, gmask, p_old, p_new, du_old, du_new);
     for (int c = w0 + ws; c < nc; c += ws)  // uniform per warp

@@ -139,6 +139,8 @@ struct DevScene {
     int* tpos = nullptr;                  // [n] position of a vertex in the touched list
     int* tv = nullptr;                    // [n] vertices with contacts, ascending
     int* ntv = nullptr;                   // [1] their number
+    int4* cinc = nullptr;                 // [4*cap] per contact corner: (vertex, list begin, list end, 0)
+    int4* tvr = nullptr;                  // [n] per touched vertex, in tv order: (vertex, list begin, list end, 0)
     // collision geometry
     int nst = 0, nse = 0, nsv = 0;
     const int4* st = nullptr;             // surface triangles (w unused)
