@@ -255,9 +255,10 @@ __global__ void __launch_bounds__(kVertThreads) k_contact_p(DevScene s, int spli
     const int g0 = ((blockIdx.x - split) * blockDim.x + threadIdx.x) / kGatherLanes;
     const int gs = (gridDim.x - split) * blockDim.x / kGatherLanes;
     for (int t = g0; t < ntv; t += gs) {
-        const int i = s.tv[t];
+        const int4 r = s.tvr[t];  // the vertex and its list bounds in one load
+        const int i = r.x;
         if (i >= s.nd) continue;
-        const float4 warm = gather_group(s, s.rc, s.vstart[i], s.vstart[i + 1], sub, gmask);
+        const float4 warm = gather_group(s, s.rc, r.y, r.z, sub, gmask);
         if (sub == 0) {
             float4 p = contact_p_base<DUALC>(s, i);
             p.x += warm.x;
