@@ -46,9 +46,11 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_fill(DevScene s) {
 // sum in a fixed order (the reference's order depends on atomics, F13).  The
 // fill leaves the lists unsorted in vtmp; one warp per vertex writes each key
 // to vlist at its rank (the keys are distinct), counted against the list held
-// in two registers per lane up to 64 keys, else read back from vtmp.  Static
-// vertices are sorted too: their lists are read by no gather, but k_contact_p
-// and the incidence entries cover all positions.
+// in two registers per lane up to 64 keys, else read back from vtmp.  The lists
+// of static vertices are read by no gather: they are copied unsorted (a static
+// ground under an impact holds thousands of entries, and the quadratic sort of
+// those lists dominated the detection), so that vlist and the incidence entries
+// still cover every position.
 constexpr int kRankSortRegs = 64;
 
 // The vertices with contacts, ascending: tv[tpos[i]] = i for vcnt[i] > 0
@@ -73,7 +75,9 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_sort_lists(DevScene
     for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntv; t += (gridDim.x * blockDim.x) >> 5) {
         const int i = s.tv[t];
         const int b = s.vstart[i], e = s.vstart[i + 1], L = e - b;
-        if (L <= kRankSortRegs) {
+        if (i >= s.nd) {
+            for (int m = lane; m < L; m += 32) s.vlist[b + m] = s.vtmp[b + m];
+        } else if (L <= kRankSortRegs) {
             const int k0 = lane < L ? s.vtmp[b + lane] : 0x7fffffff;
             const int k1 = lane + 32 < L ? s.vtmp[b + 32 + lane] : 0x7fffffff;
             int r0 = 0, r1 = 0;

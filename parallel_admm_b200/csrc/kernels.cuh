@@ -331,7 +331,11 @@ ADMM_DEV void rhs_row(const DevScene& s, int i, float4 acc) {
 // after the row sum.  Same operations in the same order as ell_row_sum.
 constexpr int kPrefetch = 8;
 
-template <int T>
+// LONG: rows much longer than kPrefetch * 32 / (32 / T) entries (R, whose rows
+// hold every constraint row of a vertex): the rest of the row is unrolled so
+// that several of its loads are in flight; the sweep's short rows (A) keep the
+// plain loop, which measured faster there.
+template <int T, bool LONG = false>
 struct EllRowPf {
     static constexpr int S = 32 / T;
     int row, b, e;
@@ -361,13 +365,25 @@ struct EllRowPf {
                 az = fmaf(vv[j], q.z, az);
             }
         }
-        for (int k = b + lane + 32 * kPrefetch; k < e; k += 32) {
-            const int c = __ldg(&M.col[k]);
-            const float a = __ldg(&M.val[k]);
-            const float4 q = v[c];
-            ax = fmaf(a, q.x, ax);
-            ay = fmaf(a, q.y, ay);
-            az = fmaf(a, q.z, az);
+        if (LONG) {
+#pragma unroll 4
+            for (int k = b + lane + 32 * kPrefetch; k < e; k += 32) {
+                const int c = __ldg(&M.col[k]);
+                const float a = __ldg(&M.val[k]);
+                const float4 q = v[c];
+                ax = fmaf(a, q.x, ax);
+                ay = fmaf(a, q.y, ay);
+                az = fmaf(a, q.z, az);
+            }
+        } else {
+            for (int k = b + lane + 32 * kPrefetch; k < e; k += 32) {
+                const int c = __ldg(&M.col[k]);
+                const float a = __ldg(&M.val[k]);
+                const float4 q = v[c];
+                ax = fmaf(a, q.x, ax);
+                ay = fmaf(a, q.y, ay);
+                az = fmaf(a, q.z, az);
+            }
         }
 #pragma unroll
         for (int o = S; o < 32; o <<= 1) {
@@ -385,7 +401,7 @@ __global__ void __launch_bounds__(kVertThreads) k_rhs(DevScene s) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= s.R.nslices) return;
-    EllRowPf<T> r;
+    EllRowPf<T, true> r;
     r.load(s.R, w, lane);
     const int i = r.row;
     const bool own = i < s.nd, c = own && s.contact;
