@@ -411,7 +411,7 @@ def main():
     if world == 1 and not args.no_cpu_baseline:
         v, cores, secs, n, it_mean = cpu_baseline(sc, h, args.steps, args.cpu_stride)
         cpu = {"value": v, "unit": "steps/s", "cores": cores, "kind": "port",
-               "sample": f"{n} substeps, one at every {args.cpu_stride}th frame of frames 0..{args.steps - 1}, "
+               "sample": f"{n} substeps, one every {args.cpu_stride} frames of frames 0..{args.steps - 1}, "
                          f"each from the GPU run's state; {secs:.1f} s of CPU time (oracle FP32, OpenMP), "
                          f"mean {it_mean:.1f} ADMM iterations per step"}
     tn, gm = h.tuning(), h.global_mode()
