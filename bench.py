@@ -425,6 +425,8 @@ def main():
         "config": {"workload": CONFIGS[args.config]["workload"], "n_vert": sc.n_vert, "n_rows": sc.n_rows,
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) between timed steps",
                    "contacts_mean": float(np.mean(contacts)), "contacts_peak": int(peak),
+                   # contacts projected per second of substep device time (rank 0's count x ranks)
+                   "contacts_per_s": world * float(np.sum(contacts)) / (max_total_ms / 1e3),
                    "residual_tol": args.tol, "admm_iter_cap": sc.params.admm_max_iter,
                    "admm_iters_mean": float(np.mean(iters)),
                    "converged_fraction": float(np.mean(conv)) if args.tol > 0 else None,
