@@ -1,33 +1,34 @@
-"""Benchmark of the B200 ADMM substep: simulated steps/s to ADMM residual 1e-4, on one or more GPUs.
+"""Benchmark of the B200 ADMM substep: simulated steps/s to ADMM residual 1e-4, learned global
+step against plain Jacobi, on one or more GPUs.
 
 Metric: substeps per second, each substep iterating ADMM until both relative residuals
 (primal and dual, FP64 reductions) are <= 1e-4, tested after every chunk of 5 iterations,
-capped at the reference's own admm_max_iter (30).  With the reference algorithm (Jacobi
-global solve, Jacobi friction-cone contact, DCD every 5 iterations) contact-free frames
-converge within the first chunk and contact frames run to the cap, exactly like the
-reference's fixed-count step; the line reports the converged fraction and the mean
-iteration count.  `--tol 0` measures the fixed-count step.
+capped at the reference's admm_max_iter (30).  `value` is the learned global step
+(global_solver 3: the trained network's per-vertex scaling and warm start, the trained
+per-sweep schedule, judged per solve, plain Jacobi substep as the fallback); the plain
+Jacobi path (the reference's algorithm) runs the same frames in the same process and sits
+beside it in `config.plain_jacobi`, with iterations, converged fraction and fallback counts.
+On frames with contact neither reaches 1e-4 within 30 iterations (the reference's contact
+splitting plateaus near a 2e-2 primal residual), so both run to the cap there.
 
-Workload (default): the tetrahedralised cube, 20^3 cells (9261 vertices, 40000
-tets, 5 tets/cell, edge 0.5 m), dropped 1 m onto a ground quad, 30 ADMM
-iterations per substep, dt = 1/100 s, frames 0..K-1 of the drop (K = 200 by
-default: the whole 200-frame run, free fall, impact with thousands of contacts,
-rebound).  Synthetic, seeded scene (seed 0: E = 1.88e5, nu = 0.4).
+Workload (default, `--config batch`): 256 independent tet soft bodies (cubes and voxelised
+ellipsoids, 500-20000 vertices log-uniform, 1.45 M vertices and 6.07 M tets in all, E
+log-uniform in [1e4, 1e6], mu U(0.2, 0.6) per body), each released 6-20 mm above the
+ground (contact thickness 12 mm), so ground and self contacts start in the first frames;
+dt = 1/100, 30 ADMM iterations, DCD every 5.  The timed frames are start_frame ..
+start_frame + steps - 1 of the run.  Synthetic, seeded scene (seed = rank).
 
-One "step" is one full substep (IADMMBackend::step): pre-integration, 30 ADMM
-iterations with a DCD (LBVH build + traversal) every 5 iterations, contact
-projection (10 Jacobi passes), 20 Jacobi sweeps of the global solve, dual
-updates, post-process -- replayed as one CUDA graph.  The scene's working set
-(~30 MB) fits in L2, so L2 is flushed (a 256 MiB write) between timed steps.
+One "step" is one full substep (IADMMBackend::step), replayed as one CUDA graph.  L2 is
+flushed (a 256 MiB write) between timed steps.
 
-Multi-GPU: the substep of one coupled body does not shard (contacts and the
-global solve couple every vertex every iteration), so --gpus N runs N
-independent replicas, one per rank, with no collective in the data path
-("scaling": "weak"); value = total steps of all ranks / max over ranks of the
-device time.
+Multi-GPU: independent bodies shard by whole batches with no collective in the data path:
+--gpus N runs N batches, one per rank ("scaling": "weak"); value = total steps of all
+ranks / max over ranks of the device time.
 
-`--impl reference` times the CPU restatement of the reference's GPU-backend
-algorithm (the oracle, OpenMP on all host threads) on the same workload.
+`--impl reference` times the CPU restatement of the reference's GPU-backend algorithm
+(the oracle, OpenMP on all host threads, plain Jacobi) on a size-stratified sample of 16
+of the 256 bodies over the same frames, scaled to the whole batch by its share of the
+work (constraint rows + vertices).
 """
 from __future__ import annotations
 
@@ -55,8 +56,9 @@ CONFIGS = {
                    workload="4 x 512^2 cloth sheets on a sphere r=0.3, 40 ADMM iters/step, dt=1/300"),
     "batch": dict(fn="batch_bodies", kw=dict(n_bodies=256, seed=0), per_rank_seed=True,
                   workload="256 independent tet soft bodies (cubes and ellipsoids, 500-20000 verts log-uniform, "
-                           "E log-U[1e4,1e6], mu U(0.2,0.6) per body) dropped onto the ground, 30 ADMM iters/step, "
-                           "dt=1/100; each rank simulates its own batch (seed = rank)"),
+                           "1.45 M verts, 6.07 M tets, E log-U[1e4,1e6], mu U(0.2,0.6) per body) released 6-20 mm "
+                           "above the ground (contact from the first frames), self-contact, 30 ADMM iters/step, "
+                           "DCD every 5, dt=1/100; each rank simulates its own batch (seed = rank)"),
     "sheets_small": dict(fn="sheets_on_sphere", kw=dict(nx=256, layers=2, seed=0),
                          workload="2 x 256^2 cloth sheets on a sphere r=0.3, 40 ADMM iters/step, dt=1/300 "
                                   "(profiling stand-in for the sheets workload)"),
@@ -72,7 +74,10 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def make_scene(args, rank=0):
+WEIGHTS = os.path.join(ROOT, "parallel_admm_b200", "weights", "learned_step.npz")
+
+
+def make_scene(args, rank=0, only=None):
     """The configured scene with the solver options of the command line applied."""
     from parallel_admm_b200 import scene
     c = CONFIGS[args.config]
@@ -80,42 +85,48 @@ def make_scene(args, rank=0):
     if c.get("per_rank_seed"):
         from parallel_admm_b200 import replicas as R
         kw["seed"] = R.rank_seed(kw.get("seed", 0), rank)
+    if only is not None:
+        kw["only"] = only
     sc = getattr(scene, c["fn"])(**kw)
     sc.params.jacobi_mode = args.jacobi_mode
     sc.params.ell_lanes = args.ell_lanes
-    sc.params.global_solver = args.global_solver
     sc.params.pcg_iter = args.pcg_iter
     sc.params.query_lanes = args.query_lanes
     return sc
 
 
-def metric_name(tol, cap, solver=0, pcg_iter=0):
-    how = {0: "plain Jacobi", 1: f"PCG diag(A) x{pcg_iter}", 2: f"PCG learned blocks x{pcg_iter}"}[solver]
+def metric_name(tol, cap, arm):
+    how = {"learned": "learned global step (Jacobi fallback)", "jacobi": "plain Jacobi",
+           "pcg": "PCG diag(A)"}[arm]
     if tol > 0:
-        return f"sim steps/s to ADMM residual {tol:g} ({how}, cap {cap} ADMM iterations = reference count)"
-    return f"sim steps/s ({how}, fixed {cap} ADMM iterations = reference count)"
+        return f"sim steps/s to ADMM residual {tol:g}: {how}, cap {cap} ADMM iterations = reference count"
+    return f"sim steps/s: {how}, fixed {cap} ADMM iterations = reference count"
 
 
 def pair_nnz(sc):
-    """Off-diagonal non-zeros of A (vertex pairs coupled by a constraint)."""
-    pairs = set()
-
-    def add(ids):
-        ids = [int(i) for i in ids]
-        for a in ids:
-            for b in ids:
+    """Off-diagonal non-zeros of A (ordered vertex pairs coupled by a constraint)."""
+    keys = []
+    n = np.int64(sc.n_vert)
+    groups = [sc.tet_inds, sc.tri_inds]
+    for t in groups:
+        t = np.asarray(t, np.int64)
+        if len(t) == 0:
+            continue
+        for a in range(t.shape[1]):
+            for b in range(t.shape[1]):
                 if a != b:
-                    pairs.add((a, b))
-    for t in sc.tet_inds:
-        add(t)
-    for t in sc.tri_inds:
-        add(t)
+                    keys.append(t[:, a] * n + t[:, b])
     for c in range(len(sc.bend_w)):
-        add(sc.bend_inds[sc.bend_offsets[c]:sc.bend_offsets[c + 1]])
-    return len(pairs)
+        ids = np.asarray(sc.bend_inds[sc.bend_offsets[c]:sc.bend_offsets[c + 1]], np.int64)
+        ii, jj = np.meshgrid(ids, ids)
+        keep = ii != jj
+        keys.append(ii[keep] * n + jj[keep])
+    if not keys:
+        return 0
+    return int(len(np.unique(np.concatenate(keys))))
 
 
-def algorithmic_bytes(sc, kernel):
+def algorithmic_bytes(sc, kernel, nnz=None):
     """Bytes one launch must move at minimum (each array touched once, FP32, gathers once per element)."""
     n, nd, m = sc.n_vert, sc.n_dyn, sc.n_rows
     if kernel == "local":
@@ -124,10 +135,11 @@ def algorithmic_bytes(sc, kernel):
         ring = int(sc.bend_offsets[-1]) if len(sc.bend_w) else 0
         return (60 * m + 52 * len(sc.tet_inds) + 28 * len(sc.tri_inds) + 8 * ring +
                 16 * len(sc.pin_inds) + 12 * nd)
-    if kernel == "jacobi":
-        nnz = pair_nnz(sc)
-        # diag 4 + b 12 + x_out 12 per row, (4 val + 4 col) per off-diagonal, x_in gathered once
-        return 28 * nd + 8 * nnz + 12 * nd
+    if kernel in ("jacobi", "learned"):
+        nnz = pair_nnz(sc) if nnz is None else nnz
+        # Jacobi: diag 4 + b 12 + x_out 12 per row, (4 val + 4 col) per off-diagonal, x_in gathered once;
+        # learned sweep: + m 4 and the previous iterate 12 per row
+        return (28 + 12 + (16 if kernel == "learned" else 0)) * nd + 8 * nnz
     if kernel == "rhs":
         nnz_d = 4 * 3 * len(sc.tet_inds) + 3 * 2 * len(sc.tri_inds) + int(
             sc.bend_offsets[-1] if len(sc.bend_w) else 0) + len(sc.pin_inds)
@@ -185,98 +197,191 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(sc, h, frames, stride):
-    """The oracle (FP32 restatement of the reference GPU-backend algorithm) on the host cores.
+def stratified_bodies(sc_meta, k=16):
+    """k bodies of the batch spread evenly over its size distribution (by vertex count)."""
+    counts = np.array([c[0] for c in sc_meta["all_body_counts"]])
+    order = np.argsort(counts, kind="stable")
+    step = len(order) / k
+    return sorted(int(order[int(step * j + step / 2)]) for j in range(k))
 
-    Stratified sample of the workload: the GPU replays frames 0..frames-1; at every
-    `stride`-th frame its full state (x, v, both duals) is copied into the oracle, which
-    is timed for one substep.  Returns steps/s over the sampled substeps.
-    """
+
+def work_of(counts):
+    """Per-substep CPU work proxy of bodies: constraint rows (3 per tet) + vertices."""
+    return float(sum(3 * t + v for v, t in counts))
+
+
+def oracle_sample_rate(args, rank, frames, budget_s):
+    """The oracle (FP32 restatement of the reference GPU-backend algorithm, plain Jacobi, all
+    host threads) over frames 0.. of the workload, stopping once budget_s of CPU time is spent;
+    for the batch a size-stratified 16-body sample scaled to the whole batch by its work share.
+    Returns (steps/s, threads, description)."""
     from oracle import oracle as O
     from parallel_admm_b200 import backend as B
-    o = O.Oracle(h.holder, double=False)
-    h.reset()
-    secs = 0.0
-    n = 0
-    iters = 0
-    for f in range(frames):
-        if f % stride == 0:
-            x, v = h.get_state()
-            for buf, a in ((B.BUF_X0, x), (B.BUF_X, x), (B.BUF_V, v), (B.BUF_UE, h.read(B.BUF_UE)),
-                           (B.BUF_UC, h.read(B.BUF_UC))):
-                o.write(buf, a.astype(np.float64))
-            t = time.perf_counter()
-            iters += o.step(1)["iters"]
-            secs += time.perf_counter() - t
-            n += 1
-        h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
-    return n / secs, O.num_threads(), secs, n, iters / max(n, 1)
+    frac = 1.0
+    what = "the whole workload"
+    if args.config == "batch":
+        from parallel_admm_b200 import scene
+        c = CONFIGS["batch"]["kw"]
+        seed = c["seed"] + rank
+        meta = scene.batch_bodies(c["n_bodies"], seed, only=[]).meta
+        sel = stratified_bodies(meta)
+        sc = make_scene(args, rank, only=sel)
+        allc = meta["all_body_counts"]
+        frac = work_of([allc[b] for b in sel]) / work_of(allc)
+        what = (f"bodies {sel} (16 of {len(allc)}, size-stratified: {sc.n_dyn} verts, {len(sc.tet_inds)} tets), "
+                f"time scaled by their work share {frac:.4f} (constraint rows + vertices)")
+    else:
+        sc = make_scene(args, rank)
+    holder = B.DescHolder(sc, residual_tol=args.tol, global_solver=0)
+    o = O.Oracle(holder, double=False)
+    secs, k, iters = 0.0, 0, 0
+    for _ in range(frames):
+        t = time.perf_counter()
+        iters += o.step(1)["iters"]
+        secs += time.perf_counter() - t
+        k += 1
+        if secs >= budget_s:
+            break
+    rate = k / (secs / frac)
+    desc = (f"{what}; frames 0..{k - 1} ({secs:.1f} s of CPU time), mean {iters / max(k, 1):.1f} ADMM iterations "
+            f"per step, oracle FP32, OpenMP")
+    return rate, O.num_threads(), desc
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sc = make_scene(args)
-    from oracle import oracle as O
-    from parallel_admm_b200 import backend as B
-    holder = B.DescHolder(sc, residual_tol=args.tol)
-    o = O.Oracle(holder, double=False)
-    o.step(min(args.warmup, 3))
-    o.reset()
-    k = min(args.steps, args.ref_steps)
-    t = time.perf_counter()
-    iters = 0
-    for _ in range(k):
-        iters += o.step(1)["iters"]
-    dt = time.perf_counter() - t
-    value = k / dt
-    sample = (f"frames 0..{k - 1} of the workload ({k} of {args.steps} steps; CPU time bounded), "
-              f"mean {iters / k:.1f} ADMM iterations per step")
+    frames = args.start_frame + min(args.steps, args.ref_steps)
+    rate, cores, desc = oracle_sample_rate(args, 0, frames, budget_s=args.ref_budget)
     line = {
-        "impl": "reference", "metric": metric_name(args.tol, sc.params.admm_max_iter, args.global_solver,
-                              args.pcg_iter or max(1, sc.params.jacobi_iter // 2)),
-        "value": value, "unit": "steps/s", "n_gpus": args.gpus, "steps": k, "warmup": min(args.warmup, 3),
-        "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic", "config": {"workload": CONFIGS[args.config]["workload"]},
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": O.num_threads(), "kind": "port",
-                         "sample": sample},
-        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "impl": "reference", "metric": metric_name(args.tol, 30, "jacobi"),
+        "value": rate, "unit": "steps/s", "n_gpus": args.gpus, "steps": min(args.steps, args.ref_steps),
+        "warmup": 0, "ms_per_step": 1e3 / rate, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": CONFIGS[args.config]["workload"]},
+        "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port", "sample": desc},
+        "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def learned_model(args, h, sc):
+    """The trained learned global step applied to handle h (global_solver 3); without the
+    weights file, the untrained model (zero head = Jacobi scaling, Chebyshev schedule)."""
+    from parallel_admm_b200 import gnn
+    sysm = gnn.system(h)
+    x, ef = gnn.scene_features(sc, sysm)
+    if args.weights and os.path.exists(args.weights):
+        model = gnn.LearnedGlobalStep.load(args.weights)
+        source = os.path.relpath(args.weights, ROOT)
+    else:
+        model = gnn.LearnedGlobalStep(K=args.learned_sweeps)
+        model.init_chebyshev(gnn.jacobi_spectrum_top(sysm))
+        source = "untrained (Chebyshev schedule, Jacobi scaling)"
+    model.apply(h, sysm, x, ef)
+    info = {"weights": source, "sweeps": int(model.K)}
+    model.net.close()
+    return info
+
+
+def run_arm(args, B, R, sc, local, world, arm, flush, nnz):
+    """Warm-up, then the timed frames of one arm; returns its handle and numbers."""
+    import torch
+    import torch.distributed as dist
+    gs = {"learned": 3, "jacobi": 0, "pcg": 1}[arm]
+    h = B.Handle(sc, device=local, residual_tol=args.tol, global_solver=gs)
+    info = learned_model(args, h, sc) if arm == "learned" else {}
+    allow = (B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW)
+    for _ in range(args.warmup):
+        h.step(1, allow=allow)
+    h.reset()
+    for _ in range(args.start_frame):
+        h.step(1, allow=allow)
+    st0 = h.learned_stats() if arm == "learned" else None
+    dev_ms, contacts, iters, conv = [], [], [], []
+    launches, peak, status = 0, 0, 0
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with ClockSampler(local) as clk:
+        barrier()
+        for k in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            if args.profile_steps and k == 0:
+                torch.cuda.cudart().cudaProfilerStart()
+            st = h.step(1, allow=allow)
+            if args.profile_steps and k + 1 == args.profile_steps:
+                torch.cuda.cudart().cudaProfilerStop()
+            dev_ms.append(h.last_step_device_ms())
+            contacts.append(st["n_contacts"])
+            iters.append(st["iters"])
+            launches += h.kernels_per_step()
+            conv.append(st["primal"] <= args.tol and st["dual"] <= args.tol)
+            peak = max(peak, st["peak"])
+            status = status or st["status"]
+        barrier()
+    total_ms = float(np.sum(dev_ms))
+    max_total_ms = R.max_over_ranks(total_ms, f"cuda:{local}")
+    out = {"h": h, "value": R.job_throughput(args.steps, world, max_total_ms / 1e3),
+           "ms_per_step": max_total_ms / args.steps, "max_total_ms": max_total_ms, "clocks": clk.summary(),
+           "contacts": contacts, "iters": iters, "conv": conv, "peak": peak, "status": status,
+           "launches": launches, "info": info}
+    if arm == "learned":
+        st1 = h.learned_stats()
+        d = {k: st1[k] - st0[k] for k in st1}
+        out["learned"] = d
+        # a substep that fell back also ran the plain graph: count its launches
+        if d["fallbacks"]:
+            out["launches"] += d["fallbacks"] * launches // max(args.steps, 1)
+    return out
+
+
+def arm_summary(args, r, sc, world):
+    return {"steps_per_s": r["value"], "ms_per_step": r["ms_per_step"],
+            "admm_iters_mean": float(np.mean(r["iters"])),
+            "converged_fraction": float(np.mean(r["conv"])) if args.tol > 0 else None,
+            "contacts_mean": float(np.mean(r["contacts"])), "contacts_peak": int(r["peak"]),
+            "contacts_per_s": world * float(np.sum(r["contacts"])) / (r["max_total_ms"] / 1e3),
+            "kernels_launched": r["launches"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="cube", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="batch", choices=sorted(CONFIGS))
+    ap.add_argument("--solver", default="learned", choices=["learned", "jacobi", "pcg"],
+                    help="the arm reported as value; with learned, plain Jacobi runs beside it")
+    ap.add_argument("--weights", default=WEIGHTS, help="trained learned-step weights (npz)")
+    ap.add_argument("--learned-sweeps", type=int, default=10, help="sweeps of the untrained learned step")
     ap.add_argument("--probe", default="jacobi", choices=["local", "jacobi", "rhs"])
-    ap.add_argument("--cpu-stride", type=int, default=3,
-                    help="CPU-baseline sample: one substep every N frames (3: 67 of the cube's 200, ~13 s on 16 cores)")
     ap.add_argument("--tol", type=float, default=1e-4, help="ADMM residual tolerance (0 = fixed iteration count)")
     ap.add_argument("--ell-lanes", type=int, default=0, choices=[0, 1, 2, 4, 8],
                     help="pin the lanes per row of both sliced-ELL matrices (0 = autotuned; pin it under a profiler, "
                          "whose serialised launches mislead the autotuner)")
     ap.add_argument("--jacobi-mode", type=int, default=0, choices=[0, 1, 2, 3],
                     help="global step: 0 autotuned, 1 one kernel per sweep, 2 persistent kernel, 3 two sweeps per launch")
-    ap.add_argument("--global-solver", type=int, default=0, choices=[0, 1, 2],
-                    help="global step: 0 Jacobi sweeps (the reference's), 1 PCG with diag(A), 2 PCG with blocks")
     ap.add_argument("--pcg-iter", type=int, default=0, help="PCG iterations per global step (0 = jacobi_iter / 2)")
     ap.add_argument("--query-lanes", type=int, default=0, choices=[0, 8, 16, 32],
                     help="lanes per grid DCD query (0 = chosen from the number of queries)")
-    ap.add_argument("--ref-steps", type=int, default=200, help="cap on steps timed by --impl reference")
+    ap.add_argument("--ref-steps", type=int, default=20, help="cap on steps timed by --impl reference")
+    ap.add_argument("--ref-budget", type=float, default=60.0, help="CPU seconds the reference arm may spend")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="CPU seconds of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--start-frame", type=int, default=0,
-                    help="advance this many substeps (untimed) before the timed region, e.g. to time contact frames")
+                    help="advance this many substeps (untimed) before the timed region")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="open a CUDA profiler range (cudaProfilerStart/Stop) around the first N timed steps, "
                          "for ncu --profile-from-start off")
-    ap.add_argument("--profile", action="store_true", help="phase pass over all timed frames (default: the first 50)")
-    ap.add_argument("--phase-steps", type=int, default=50, help="substeps of the phase-probe pass (roofline)")
+    ap.add_argument("--phase-steps", type=int, default=10, help="substeps of the phase-probe pass (roofline)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -297,55 +402,27 @@ def main():
     from parallel_admm_b200 import replicas as R
 
     sc = make_scene(args, rank)
-    h = B.Handle(sc, device=local, residual_tol=args.tol)
-    for _ in range(args.warmup):
-        h.step(1, allow=(B.ERR_CONTACT_OVERFLOW,))
-    h.reset()
-
-    for _ in range(args.start_frame):
-        h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+    nnz = pair_nnz(sc)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-    dev_ms = []
-    contacts = []
-    iters = []
-    conv = []
-    launches = 0
-    peak = 0
-    status = 0
+    arms = [args.solver] + (["jacobi"] if args.solver == "learned" else [])
+    res = {}
+    for arm in arms:
+        res[arm] = run_arm(args, B, R, sc, local, world, arm, flush, nnz)
+        if arm != args.solver:
+            res[arm]["h"].close()
+            res[arm]["h"] = None
+    main_r = res[args.solver]
+    h = main_r["h"]
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    with ClockSampler(local) as clk:
-        barrier()
-        for k in range(args.steps):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            if args.profile_steps and k == 0:
-                torch.cuda.cudart().cudaProfilerStart()
-            st = h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
-            if args.profile_steps and k + 1 == args.profile_steps:
-                torch.cuda.cudart().cudaProfilerStop()
-            dev_ms.append(h.last_step_device_ms())
-            contacts.append(st["n_contacts"])
-            iters.append(st["iters"])
-            launches += h.kernels_per_step()
-            conv.append(st["primal"] <= args.tol and st["dual"] <= args.tol)
-            peak = max(peak, st["peak"])
-            status = status or st["status"]
-        barrier()
-    clocks = clk.summary()
-    total_ms = float(np.sum(dev_ms))
-    max_total_ms = R.max_over_ranks(total_ms, f"cuda:{local}")
-    ms_per_step = max_total_ms / args.steps
-    value = R.job_throughput(args.steps, world, max_total_ms / 1e3)
-
-    # end to end through the public C ABI: pinned host buffers in, one substep, host buffers out
+    # end to end through the public C ABI: pinned host buffers in, one substep, host buffers out,
+    # over the same frames as the timed region
+    allow = (B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW)
     h.reset()
-    x_in = torch.from_numpy(sc.verts.copy()).pin_memory().numpy()
-    v_in = torch.zeros((sc.n_vert, 3), dtype=torch.float32).pin_memory().numpy()
+    for _ in range(args.start_frame):
+        h.step(1, allow=allow)
+    x0, v0 = h.get_state()
+    x_in = torch.from_numpy(x0.copy()).pin_memory().numpy()
+    v_in = torch.from_numpy(v0.copy()).pin_memory().numpy()
     x_out = torch.zeros((sc.n_vert, 3), dtype=torch.float32).pin_memory().numpy()
     v_out = torch.zeros((sc.n_vert, 3), dtype=torch.float32).pin_memory().numpy()
     e2e_s = 0.0
@@ -360,35 +437,32 @@ def main():
     e2e_value = R.job_throughput(args.steps, world, R.max_over_ranks(e2e_s, f"cuda:{local}"))
     bytes_io = 2 * sc.n_vert * 3 * 4
 
-    # Device time per phase inside the step graph (events at phase changes, so the launch gaps
-    # inside a phase are included), over the same frames as the timed region (the first
-    # --phase-steps of them); with a residual tolerance only the first chunk of each step is
-    # covered.  The roofline below divides the probed kernel's bytes by its phase's time per launch.
+    # Device time per phase inside the step graph (events at phase changes), over the first
+    # --phase-steps timed frames (first chunk of each step); the roofline divides the probed
+    # kernel's bytes by its phase's time per launch.  Then an event pair around each of the
+    # first launches of the probed class (a pass of its own: the events break the overlap).
     phases = None
     probe_ms, probe_n = 0.0, 0
     if rank == 0:
-        nph = args.steps if args.profile else min(args.steps, args.phase_steps)
+        nph = min(args.steps, args.phase_steps)
         h.reset()
         for _ in range(args.start_frame):
-            h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+            h.step(1, allow=allow)
         h.set_probe("phases")
         h.phase_times()
         for _ in range(nph):
-            h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+            h.step(1, allow=allow)
         raw = h.phase_times()
         phases = {k: {"ms_per_step": v["ms"] / nph, "launches_per_step": v["launches"] / nph} for k, v in raw.items()}
         phases["scope"] = (f"frames {args.start_frame}..{args.start_frame + nph - 1}, "
                            + ("first chunk of each step" if args.tol > 0 else "whole step"))
-        # Isolated launches of the probed kernel class: an event pair around each of its first
-        # launches in the step graph (this breaks their programmatic overlap, so it runs in a
-        # pass of its own, never in the timed region).
         h.reset()
         for _ in range(args.start_frame):
-            h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+            h.step(1, allow=allow)
         h.set_probe(args.probe)
         h.probe_time()
         for _ in range(nph):
-            h.step(1, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+            h.step(1, allow=allow)
         probe_ms, probe_n = h.probe_time()
         h.set_probe("none")
 
@@ -398,42 +472,43 @@ def main():
         return 0
 
     peak_gbs, peak_kind = load_peaks()
-    alg = algorithmic_bytes(sc, args.probe)
+    pk = "learned" if (args.probe == "jacobi" and args.solver == "learned") else args.probe
+    alg = algorithmic_bytes(sc, pk, nnz)
     ph = phases.get(args.probe, {}) if phases else {}
+    if args.probe == "jacobi" and args.solver == "learned":
+        ph = phases.get("jacobi", {})
     phase_ms = ph["ms_per_step"] / ph["launches_per_step"] if ph.get("launches_per_step") else 0.0
     achieved = alg / (phase_ms * 1e-3) / 1e9 if phase_ms > 0 else None
     traffic = None
     tp = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get(args.config, {}).get(args.probe)
+            traffic = json.load(f).get(args.config, {}).get(pk)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        v, cores, secs, n, it_mean = cpu_baseline(sc, h, args.steps, args.cpu_stride)
-        cpu = {"value": v, "unit": "steps/s", "cores": cores, "kind": "port",
-               "sample": f"{n} substeps, one every {args.cpu_stride} frames of frames 0..{args.steps - 1}, "
-                         f"each from the GPU run's state; {secs:.1f} s of CPU time (oracle FP32, OpenMP), "
-                         f"mean {it_mean:.1f} ADMM iterations per step"}
+        rate, cores, desc = oracle_sample_rate(args, rank, args.start_frame + args.steps, args.cpu_budget)
+        cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port", "sample": desc}
     tn, gm = h.tuning(), h.global_mode()
     tuned = {"jacobi_lanes": tn["jacobi_lanes"], "rhs_lanes": tn["rhs_lanes"], "global_mode": gm["mode"]}
+    cfg = {"workload": CONFIGS[args.config]["workload"], "frames": f"{args.start_frame}..{args.start_frame + args.steps - 1}",
+           "n_vert": sc.n_vert, "n_rows": sc.n_rows, "parallelism": f"replicas x{world}",
+           "l2": "flushed (256 MiB write) between timed steps", "residual_tol": args.tol,
+           "admm_iter_cap": sc.params.admm_max_iter, "solver": args.solver, "tuned": tuned}
+    cfg.update(arm_summary(args, main_r, sc, world))
+    if args.solver == "learned":
+        cfg["learned"] = dict(main_r["info"], **main_r["learned"])
+        pj = arm_summary(args, res["jacobi"], sc, world)
+        cfg["plain_jacobi"] = pj
+        cfg["learned_over_plain"] = main_r["value"] / pj["steps_per_s"] if pj["steps_per_s"] else None
     line = {
-        "metric": metric_name(args.tol, sc.params.admm_max_iter, args.global_solver,
-                              args.pcg_iter or max(1, sc.params.jacobi_iter // 2)),
-        "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
-        "config": {"workload": CONFIGS[args.config]["workload"], "n_vert": sc.n_vert, "n_rows": sc.n_rows,
-                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) between timed steps",
-                   "contacts_mean": float(np.mean(contacts)), "contacts_peak": int(peak),
-                   # contacts projected per second of substep device time (rank 0's count x ranks)
-                   "contacts_per_s": world * float(np.sum(contacts)) / (max_total_ms / 1e3),
-                   "residual_tol": args.tol, "admm_iter_cap": sc.params.admm_max_iter,
-                   "admm_iters_mean": float(np.mean(iters)),
-                   "converged_fraction": float(np.mean(conv)) if args.tol > 0 else None,
-                   "tuned": tuned},
+        "metric": metric_name(args.tol, sc.params.admm_max_iter, args.solver),
+        "value": main_r["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": main_r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": cfg,
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
-        "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": args.probe, "achieved": achieved, "peak": peak_gbs,
+        "gpu_launches": main_r["launches"] + (res["jacobi"]["launches"] if args.solver == "learned" else 0),
+        "roofline": {"bound": "hbm", "kernel": {"learned": "k_lsweep (learned sweep)"}.get(pk, args.probe),
+                     "achieved": achieved, "peak": peak_gbs,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak_gbs) if achieved else None, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg, "mean_launch_ms": phase_ms,
@@ -442,8 +517,8 @@ def main():
                      "isolated_how": "event pair around each of the first launches of the class (adds the "
                                      "event overhead, breaks the programmatic overlap)"},
         "cpu_baseline": cpu,
-        "clocks": clocks,
-        "status": status,
+        "clocks": main_r["clocks"],
+        "status": main_r["status"],
     }
     if phases is not None:
         line["phases"] = phases

@@ -122,7 +122,10 @@ typedef struct AdmmB200Desc {
      * Jacobi sweeps (ADMMImplGPU); 1 = pcg_iter iterations of conjugate gradients
      * preconditioned by diag(A); 2 = the same with the per-vertex 3x3 blocks set
      * by admm_b200_set_preconditioner (diag(A) until then).  pcg_iter 0 =
-     * max(1, jacobi_iter / 2): the same kernel count as the Jacobi sweeps. */
+     * max(1, jacobi_iter / 2): the same kernel count as the Jacobi sweeps.
+     * 3 = the learned global step of admm_b200_set_learned (until that call: the
+     * Jacobi sweep written as x + (b - A x) / a_ii), judged per solve and with the
+     * plain Jacobi substep as its fallback. */
     int32_t global_solver;
     int32_t pcg_iter;
     /* Optional [n_vert] friction coefficient per vertex (NULL: mu for all).  A
@@ -323,6 +326,31 @@ int  admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, floa
  * vertex) for global_solver 2, e.g. the output of the learned preconditioner.
  * No reference counterpart. */
 int  admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd);
+/* --- learned global step (global_solver 3; north-star addition, no reference
+ * counterpart).  Replaces the jacobi_iter sweeps of cu_jacobi_global
+ * (jacobi_solver.cu:141-180, called from admm_impl_gpu.cu:364) by `sweeps`
+ * second-order sweeps
+ *     x_{k+1} = x_k + omega[k] m (b - A x_k) + beta[k] (x_k - x_{k-1})   (beta[0] ignored)
+ * from the warm start x_0 = x + theta (x - x_last) (x: the iterate the global step
+ * receives, x_last: the one the previous global step of the substep received; no
+ * warm start in a substep's first global step).  m [nd] scales the residual per
+ * dynamic vertex (NULL: 1 / a_ii), theta [nd] is the warm-start coefficient (NULL:
+ * 0); both come from the learned network (parallel_admm_b200/gnn.py).  Every solve is
+ * judged: a solve whose |b - A x_K| exceeds |b - A x_0| fails, and a substep with a
+ * failed solve is run again from its starting state with the plain Jacobi global
+ * step.  A learned substep therefore synchronises the stream once (to read the
+ * judge's count).  sweeps <= 32. */
+int  admm_b200_set_learned(AdmmB200* h, int sweeps, const float* omega, const float* beta, const float* m,
+                           const float* theta, int nd);
+/* out4: substeps run with the learned step, substeps run again with plain Jacobi,
+ * learned solves judged, learned solves that failed. */
+int  admm_b200_learned_stats(AdmmB200* h, int64_t* out4);
+/* Training data: runs one substep (eagerly, with the handle's global solver) and
+ * copies out, for its global step number `iteration` (1 .. admm_max_iter - 1,
+ * counted from 0 over the substep), the right-hand side b, the iterate x_cur the
+ * step receives and the iterate x_last the previous global step received (host,
+ * row-major nd x 3).  The substep counts as a step of the simulation. */
+int  admm_b200_record_global(AdmmB200* h, int iteration, float* b, float* x_cur, float* x_last, int nd);
 /* How the global step runs (jacobi_mode): persistent = 1 for the one-kernel
  * global step (blocks = its grid), 3 for two sweeps per launch over row tiles,
  * 0 for one kernel per sweep; the autotuner's ms per global step with one
@@ -351,6 +379,35 @@ int  admm_gnn_get_params(AdmmGnn* g, float* theta, int n_params);
 int  admm_gnn_forward(AdmmGnn* g, float* blocks9);
 int  admm_gnn_loss_grad(AdmmGnn* g, const float* residuals, int k, double* loss, float* grad);
 int  admm_gnn_adam(AdmmGnn* g, float lr);
+/* The network's outputs for the learned global step (global_solver 3): per vertex
+ * m_i = trace(B_i) / 3 (the isotropic part of the block; A is isotropic) and the
+ * warm-start coefficient theta_i = clamp(o_i6, -1, 1) (host, n each); an all-zero
+ * head gives m = 1 / a_ii and theta = 0, the plain Jacobi sweep. */
+int  admm_gnn_outputs(AdmmGnn* g, float* m, float* theta);
+/* Parameter gradient of a loss from its gradients gm, gtheta (host, n each) with
+ * respect to admm_gnn_outputs; grad (host, may be NULL) receives it and the next
+ * admm_gnn_adam applies it. */
+int  admm_gnn_backward(AdmmGnn* g, const float* gm, const float* gtheta, float* grad);
+
+/* --- training of the learned global step (north-star addition, no reference counterpart) ---
+ * A context over one system A (off-diagonal CSR with start[n] entries, and the
+ * diagonal).  admm_learn_loss_grad runs K sweeps of the learned global step from
+ * the warm start x_c + theta (x_c - x_l) on each of nsamp samples (b, x_c, x_l, x*:
+ * host, nsamp x n x 3, x* the converged solution of A x = b) and returns the mean
+ * of |x_K - x*|_A^2 / |x_c - x*|_A^2 and its gradients with respect to omega, beta
+ * (K each), m and theta (n each); any gradient pointer may be NULL.
+ * admm_learn_solve: conjugate gradients (diag(A) preconditioner) from x (host, in
+ * and out) until |r|_{D^-1} <= rel_tol |r_0|_{D^-1} or max_iter iterations. */
+typedef struct AdmmLearn AdmmLearn;
+int  admm_learn_create(int n, const int32_t* start, const int32_t* col, const float* val, const float* diag,
+                       AdmmLearn** out);
+void admm_learn_destroy(AdmmLearn* L);
+int  admm_learn_loss_grad(AdmmLearn* L, int K, const float* omega, const float* beta, const float* m,
+                          const float* theta, int nsamp, const float* b, const float* x_c, const float* x_l,
+                          const float* x_star, double* loss, float* g_omega, float* g_beta, float* g_m,
+                          float* g_theta);
+int  admm_learn_solve(AdmmLearn* L, const float* b, float* x, double rel_tol, int max_iter, int* iters);
+
 /* The global-step matrix A of a handle: nnz of the off-diagonal part when start
  * is NULL, else its CSR (start[n_dyn+1], col, val) and diagonal (host). */
 int  admm_b200_system(AdmmB200* h, int32_t* start, int32_t* col, float* val, float* diag);
@@ -365,8 +422,13 @@ int  admm_b200_system(AdmmB200* h, int32_t* start, int32_t* col, float* val, flo
  * `stream` (a cudaStream_t; NULL = the default stream).  Allocates nothing: the
  * ping-pong buffers are a static device array of 2 x 262144 x 3 floats, so
  * n <= 262144 (larger n returns ADMM_ERR_INVALID).  All calls in a process share
- * that array: calls that overlap on the GPU race.  The first call on a device
- * looks up the array's device address; make it before any stream capture. */
+ * that array: calls that overlap on the GPU race.  The array's device address is
+ * looked up in the calling thread's current context on every call made outside
+ * stream capture and remembered per context (so callers in their own driver-API
+ * contexts, and calls after a cudaDeviceReset, get the right address); a call made
+ * during capture uses the remembered address, so make one call in that context
+ * before any capture (else ADMM_ERR_STATE).  An error already pending on the
+ * calling thread is not cleared: the call returns ADMM_ERR_CUDA without launching. */
 int  admm_b200_jacobi_noalloc(int n, const int32_t* row_start, const int32_t* cols, const float* vals,
                               const float* diag, const float* b, const float* x_in, float* x_out, int sweeps,
                               void* stream);

@@ -245,6 +245,11 @@ struct Oracle {
     int chunk = 0;
     int global_solver = 0, pcg_iter = 0;
     std::vector<R> pblock;  // [9 nd] learned 3x3 preconditioner blocks (global_solver 2)
+    // learned global step (global_solver 3): sweeps, coefficients, per-vertex m and theta
+    int learn_K = 0;
+    std::vector<R> learn_omega, learn_beta, learn_m, learn_theta, xl;
+    int learn_fail = 0;
+    long long learn_substeps = 0, learn_fallbacks = 0, learn_solves = 0, learn_failed = 0;
     // matrices
     Csr D;        // m x nd
     Csr A;        // nd x nd off-diagonal part
@@ -690,6 +695,56 @@ struct Oracle {
         else jacobi(jacobi_iter);
     }
 
+    // Learned global step (the GPU's k_rhs_learn / k_lsweep / k_ljudge / k_ldecide):
+    // warm start x += theta (x - xl) unless first, xl <- x received; K sweeps
+    // x_{k+1} = x_k + omega_k m (b - A x_k) + beta_k (x_k - x_{k-1}); the solve fails
+    // when |b - A x_K|^2 > |b - A x_0|^2 (FP64 sums).
+    void learned_solve(bool first) {
+        const int N = 3 * nd;
+        if (learn_K == 0) {  // defaults: the Jacobi sweep
+            learn_K = std::max(1, jacobi_iter);
+            learn_omega.assign(learn_K, R(1));
+            learn_beta.assign(learn_K, R(0));
+            learn_m.resize(nd);
+            for (int i = 0; i < nd; i++) learn_m[i] = R(1) / Adiag[i];
+            learn_theta.assign(nd, R(0));
+        }
+        if ((int)xl.size() != N) xl.assign(N, R(0));
+        for (int i = 0; i < nd; i++)
+            for (int k = 0; k < 3; k++) {
+                const R xi = x[3 * i + k], xo = xl[3 * i + k];
+                xl[3 * i + k] = xi;
+                if (!first) x[3 * i + k] = learn_theta[i] * (xi - xo) + xi;
+            }
+        std::vector<R> xp(x.begin(), x.begin() + N), xn(N), ax(N);
+        double r0 = 0, rK = 0;
+        for (int s = 0; s < learn_K; s++) {
+            apply_A(x, ax);
+            for (int i = 0; i < nd; i++)
+                for (int k = 0; k < 3; k++) {
+                    const int q = 3 * i + k;
+                    const R r = b[q] - ax[q];
+                    if (s == 0) r0 += (double)r * (double)r;
+                    const R bt = s == 0 ? R(0) : learn_beta[s];
+                    xn[q] = (learn_omega[s] * learn_m[i]) * r + (bt * (x[q] - xp[q]) + x[q]);
+                }
+            for (int q = 0; q < N; q++) {
+                xp[q] = x[q];
+                x[q] = xn[q];
+            }
+        }
+        apply_A(x, ax);
+        for (int q = 0; q < N; q++) {
+            const R r = b[q] - ax[q];
+            rK += (double)r * (double)r;
+        }
+        learn_solves++;
+        if (!(rK <= r0)) {
+            learn_fail++;
+            learn_failed++;
+        }
+    }
+
     // Residuals after the global solve of an iteration, before its dual update:
     //   primal^2 = sum w^2 |D x - z|^2 + sum w_c |x - x0 - h p|^2
     //   dual^2   = sum w^2 |D (x - x_prev)|^2 + sum w_c |x - x_prev|^2
@@ -723,8 +778,25 @@ struct Oracle {
             }
     }
 
-    // ADMMImplGPU::step (admm_impl_gpu.cu:256-344)
+    // A substep; with the learned global step, judged: a substep with a failed
+    // learned solve is run again from its starting state with the Jacobi sweeps.
     int step() {
+        if (global_solver != 3) return step_once(false);
+        const std::vector<R> sx0 = x0, sv = v, sue = Ue, suc = Uc;
+        learn_fail = 0;
+        const int it = step_once(true);
+        learn_substeps++;
+        if (learn_fail == 0) return it;
+        x0 = sx0;
+        v = sv;
+        Ue = sue;
+        Uc = suc;
+        learn_fallbacks++;
+        return step_once(false);
+    }
+
+    // ADMMImplGPU::step (admm_impl_gpu.cu:256-344)
+    int step_once(bool learned) {
         const R eps = R(1) / (dt * dt * kappa + dt * beta);
         const R gam = dt * kappa / (dt * kappa + beta);
         pre_integration();
@@ -748,7 +820,8 @@ struct Oracle {
             xprev = x;
             std::vector<R> dxprev;
             Dx_rows(dxprev);
-            global_solve();
+            if (learned) learned_solve(it == 0);
+            else global_solve();
             std::vector<R> dx;
             Dx_rows(dx);
             double prim, dual, den;
@@ -802,6 +875,19 @@ template <class R> static std::vector<R>* buf_of(Oracle<R>* o, int which) {
 
 }  // namespace
 
+template <class R>
+static void set_learned_impl(Oracle<R>* o, int K, const float* om, const float* be, const float* m, const float* th) {
+    o->learn_K = K;
+    o->learn_omega.assign(om, om + K);
+    o->learn_beta.assign(be, be + K);
+    o->learn_beta[0] = R(0);
+    o->learn_m.resize(o->nd);
+    o->learn_theta.assign(o->nd, R(0));
+    for (int i = 0; i < o->nd; i++) {
+        o->learn_m[i] = m ? (R)m[i] : R(1) / o->Adiag[i];
+        if (th) o->learn_theta[i] = (R)th[i];
+    }
+}
 extern "C" {
 
 void* orc_create(const AdmmB200Desc* d, int use_double) {
@@ -899,6 +985,24 @@ int orc_system(void* hp, int32_t* start, int32_t* col, double* val, double* diag
 void orc_pcg(void* hp, int iters) {
     Handle* h = (Handle*)hp;
     if (h->d) h->d->pcg(iters); else h->f->pcg(iters);
+}
+
+// Learned global step (global_solver 3): K coefficient pairs, per-vertex m and theta
+// (null: 1 / a_ii and 0).
+void orc_set_learned(void* hp, int K, const float* om, const float* be, const float* m, const float* th) {
+    auto* h = static_cast<Handle*>(hp);
+    if (h->d) set_learned_impl(h->d, K, om, be, m, th);
+    else set_learned_impl(h->f, K, om, be, m, th);
+}
+void orc_learned_stats(void* hp, long long* out4) {
+    auto* h = static_cast<Handle*>(hp);
+    if (h->d) {
+        out4[0] = h->d->learn_substeps; out4[1] = h->d->learn_fallbacks;
+        out4[2] = h->d->learn_solves; out4[3] = h->d->learn_failed;
+    } else {
+        out4[0] = h->f->learn_substeps; out4[1] = h->f->learn_fallbacks;
+        out4[2] = h->f->learn_solves; out4[3] = h->f->learn_failed;
+    }
 }
 
 // Learned preconditioner blocks (9 per dynamic vertex, row-major) for global_solver 2.

@@ -54,6 +54,8 @@ def lib():
         L.orc_system.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_system.restype = ctypes.c_int
         L.orc_set_preconditioner.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_learned.argtypes = [ctypes.c_void_p, ctypes.c_int, _f, _f, _f, _f]
+        L.orc_learned_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
         L.orc_detect.restype = ctypes.c_int
         L.orc_detect.argtypes = [ctypes.c_void_p]
         L.orc_contacts.restype = ctypes.c_int
@@ -146,6 +148,21 @@ class Oracle:
         a = np.ascontiguousarray(a, np.float64).reshape(n, 3)
         if lib().orc_write(self.h, which, _p(a, _d), n) != 0:
             raise ValueError("bad buffer")
+
+    def set_learned(self, omega, beta, m=None, theta=None):
+        """Learned global step (global_solver 3), the same arguments as the CUDA library's."""
+        om = np.ascontiguousarray(omega, np.float32).ravel()
+        be = np.ascontiguousarray(beta, np.float32).ravel()
+        mm = None if m is None else np.ascontiguousarray(m, np.float32).ravel()
+        th = None if theta is None else np.ascontiguousarray(theta, np.float32).ravel()
+        lib().orc_set_learned(self.h, len(om), _p(om, _f), _p(be, _f), None if mm is None else _p(mm, _f),
+                              None if th is None else _p(th, _f))
+        self._learned_keep = (om, be, mm, th)
+
+    def learned_stats(self):
+        out = (ctypes.c_longlong * 4)()
+        lib().orc_learned_stats(self.h, out)
+        return {"substeps": out[0], "fallbacks": out[1], "solves": out[2], "failed_solves": out[3]}
 
     def local_step(self):
         lib().orc_local_step(self.h)

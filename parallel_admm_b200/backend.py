@@ -205,6 +205,9 @@ def lib():
             "admm_b200_clear_tracks": (ctypes.c_int, [vp]),
             "admm_b200_jacobi_noalloc": (ctypes.c_int, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int,
                                                         vp]),
+            "admm_b200_set_learned": (ctypes.c_int, [vp, ctypes.c_int, _f, _f, _f, _f, ctypes.c_int]),
+            "admm_b200_learned_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64)]),
+            "admm_b200_record_global": (ctypes.c_int, [vp, ctypes.c_int, _f, _f, _f, ctypes.c_int]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -230,6 +233,8 @@ def exported_symbols():
         "admm_b200_set_rigid_track", "admm_b200_set_point_track", "admm_b200_clear_tracks",
         "admm_b200_system", "admm_gnn_create", "admm_gnn_set_graph", "admm_gnn_destroy", "admm_gnn_num_params",
         "admm_gnn_set_params", "admm_gnn_get_params", "admm_gnn_forward", "admm_gnn_loss_grad", "admm_gnn_adam",
+        "admm_b200_set_learned", "admm_b200_learned_stats", "admm_b200_record_global", "admm_gnn_outputs",
+        "admm_gnn_backward", "admm_learn_create", "admm_learn_destroy", "admm_learn_loss_grad", "admm_learn_solve",
     ]
 
 
@@ -403,6 +408,33 @@ class Handle:
         """Per-vertex 3x3 blocks (n_dyn x 9 or n_dyn x 3 x 3) for global_solver 2."""
         blk = np.ascontiguousarray(blocks, np.float32).reshape(self.n_dyn, 9)
         self.check(lib().admm_b200_set_preconditioner(self.h, _p(blk), self.n_dyn), "set_preconditioner")
+
+    def set_learned(self, omega: np.ndarray, beta: np.ndarray, m: Optional[np.ndarray] = None,
+                    theta: Optional[np.ndarray] = None):
+        """Learned global step (global_solver 3): per-sweep (omega, beta), per-vertex m and theta."""
+        om = np.ascontiguousarray(omega, np.float32).ravel()
+        be = np.ascontiguousarray(beta, np.float32).ravel()
+        if len(om) != len(be):
+            raise ValueError("omega and beta need one entry per sweep")
+        mm = None if m is None else np.ascontiguousarray(m, np.float32).reshape(self.n_dyn)
+        th = None if theta is None else np.ascontiguousarray(theta, np.float32).reshape(self.n_dyn)
+        self.check(lib().admm_b200_set_learned(self.h, len(om), _p(om), _p(be), None if mm is None else _p(mm),
+                                               None if th is None else _p(th), self.n_dyn), "set_learned")
+
+    def learned_stats(self) -> Dict[str, int]:
+        out = (ctypes.c_int64 * 4)()
+        self.check(lib().admm_b200_learned_stats(self.h, out), "learned_stats")
+        return {"substeps": out[0], "fallbacks": out[1], "solves": out[2], "failed_solves": out[3]}
+
+    def record_global(self, iteration: int, allow=()):
+        """One substep; (b, x_cur, x_last) of its global step number `iteration` (n_dyn x 3 each)."""
+        nd = self.n_dyn
+        b = np.zeros((nd, 3), np.float32)
+        xc = np.zeros((nd, 3), np.float32)
+        xl = np.zeros((nd, 3), np.float32)
+        self.check(lib().admm_b200_record_global(self.h, iteration, _p(b), _p(xc), _p(xl), nd), "record_global",
+                   allow)
+        return b, xc, xl
 
     def set_rigid_track(self, v_begin: int, v_end: int, pos: np.ndarray, quat_xyzw: np.ndarray):
         """Static vertices [v_begin, v_end) follow pos[f] + quat[f] * rest (one row per frame)."""

@@ -24,6 +24,7 @@
 #include "grid.cuh"
 #include "kernels.cuh"
 #include "lbvh.cuh"
+#include "learn.cuh"
 #include "scan_sort.cuh"
 #include "setup.hpp"
 
@@ -66,6 +67,19 @@ struct AdmmB200 {
     int pcg_iter = 0;
     PcgDev pcg;
     float* pcg_blocks = nullptr;    // [9 nd] learned blocks (global_solver 2)
+    // learned global step (global_solver 3)
+    LearnDev learn;
+    int learn_sweeps = 0;
+    std::vector<float> learn_omega, learn_beta;
+    cudaGraphExec_t plain_exec = nullptr;   // the same substep with the Jacobi global step (fallback)
+    float4 *sv_x0 = nullptr, *sv_v = nullptr, *sv_ue = nullptr, *sv_uc = nullptr;  // substep start state
+    int* sv_anim = nullptr;
+    int* fail_host = nullptr;       // pinned copy of learn.fail
+    int64_t learn_substeps = 0, learn_fallbacks = 0;
+    bool force_plain = false;       // enqueue the Jacobi global step whatever global_solver says
+    // recording of one global step's inputs (admm_b200_record_global, eager substeps)
+    int rec_target = -1, rec_count = 0;
+    float4 *rec_b = nullptr, *rec_cur = nullptr, *rec_last = nullptr;
     int enqueue_rc = ADMM_OK;       // first error while enqueueing or capturing a substep
     float grid_cell_size = 0.f;
     int grid_buckets = 0;
@@ -545,20 +559,97 @@ void enqueue_pcg(AdmmB200* h, int iters) {
 #undef PCG_T
 }
 
-void enqueue_global(AdmmB200* h, bool save_prev) {
-    if (h->global_solver > 0) {
+// The learned global step: right-hand side with the warm start, learn_sweeps
+// second-order sweeps (x_k in {x, jac0, jac1}[k % 3]), the judge's pass that
+// leaves x_K in x, and the decision.
+void enqueue_learned(AdmmB200* h, bool save_prev, bool first) {
+    DevScene& s = h->s;
+    LearnDev& L = h->learn;
+    set_phase(h, ADMM_PHASE_RHS);
+    const int gr = blocks(s.R.nslices * 32, kVertThreads);
+    const int ex = first ? 0 : 1;
+#define RHSL_CASE(T)                                                                                \
+    if (save_prev) LAUNCH_P(ADMM_KERNEL_RHS, (k_rhs_learn<T, true>), gr, kVertThreads, s, L, ex);   \
+    else LAUNCH_P(ADMM_KERNEL_RHS, (k_rhs_learn<T, false>), gr, kVertThreads, s, L, ex);
+    switch (s.R.lanes) {
+        case 1: RHSL_CASE(1) break;
+        case 2: RHSL_CASE(2) break;
+        case 4: RHSL_CASE(4) break;
+        default: RHSL_CASE(8) break;
+    }
+#undef RHSL_CASE
+    set_phase(h, ADMM_PHASE_JACOBI);
+    const int K = h->learn_sweeps;
+    float4* buf[3] = {s.x, s.jac[0], s.jac[1]};
+#define LS_CASE(T)                                                                                         \
+    for (int k = 0; k < K; k++) {                                                                          \
+        const float4* src = buf[k % 3];                                                                    \
+        const float4* prv = buf[(k + 2) % 3];                                                              \
+        float4* dst = buf[(k + 1) % 3];                                                                    \
+        if (k == 0)                                                                                        \
+            LAUNCH_P(ADMM_KERNEL_JACOBI, (k_lsweep<T, true>), L.blocks, kVertThreads, s, L, src, prv, dst, \
+                     h->learn_omega[k], h->learn_beta[k]);                                                 \
+        else                                                                                               \
+            LAUNCH_P(ADMM_KERNEL_JACOBI, (k_lsweep<T, false>), L.blocks, kVertThreads, s, L, src, prv, dst, \
+                     h->learn_omega[k], h->learn_beta[k]);                                                 \
+    }                                                                                                      \
+    LAUNCH(k_ljudge<T>, L.blocks, kVertThreads, s, L, (const float4*)buf[K % 3]);
+    switch (s.A.lanes) {
+        case 1: LS_CASE(1) break;
+        case 2: LS_CASE(2) break;
+        case 4: LS_CASE(4) break;
+        default: LS_CASE(8) break;
+    }
+#undef LS_CASE
+    LAUNCH(k_ldecide, 1, 256, L);
+}
+
+// Copies of one global step's inputs for admm_b200_record_global (eager only):
+// x as received by global step rec_target - 1 and rec_target, b of rec_target.
+void record_before_rhs(AdmmB200* h) {
+    if (h->rec_target < 0) return;
+    const size_t bytes = sizeof(float4) * (size_t)h->s.nd;
+    if (h->rec_count == h->rec_target - 1) cudaMemcpyAsync(h->rec_last, h->s.x, bytes, cudaMemcpyDeviceToDevice, h->cstream);
+    if (h->rec_count == h->rec_target) cudaMemcpyAsync(h->rec_cur, h->s.x, bytes, cudaMemcpyDeviceToDevice, h->cstream);
+}
+
+void record_after_rhs(AdmmB200* h) {
+    if (h->rec_target < 0) return;
+    if (h->rec_count == h->rec_target)
+        cudaMemcpyAsync(h->rec_b, h->s.b, sizeof(float4) * (size_t)h->s.nd, cudaMemcpyDeviceToDevice, h->cstream);
+    h->rec_count++;
+}
+
+void enqueue_global(AdmmB200* h, bool save_prev, bool first) {
+    record_before_rhs(h);
+    if (h->global_solver == 3 && !h->force_plain && h->rec_target < 0) {
+        enqueue_learned(h, save_prev, first);
+        record_after_rhs(h);
+        return;
+    }
+    if (h->global_solver == 3 && !h->force_plain) {
+        // recording: the right-hand side alone first, so that b can be copied
+        // before the sweeps (the learned step then runs its own right-hand side)
+        launch_rhs(h, false);
+        record_after_rhs(h);
+        enqueue_learned(h, save_prev, first);
+        return;
+    }
+    if (h->global_solver > 0 && h->global_solver < 3) {
         set_phase(h, ADMM_PHASE_RHS);
         launch_rhs(h, save_prev);
+        record_after_rhs(h);
         enqueue_pcg(h, h->pcg_iter);
         return;
     }
-    if (h->persist && h->jac_iter >= 2) {
+    if (h->persist && h->jac_iter >= 2 && h->rec_target < 0) {
         set_phase(h, ADMM_PHASE_JACOBI);
         launch_persist(h, true, save_prev, h->jac_iter);
         return;
     }
     set_phase(h, ADMM_PHASE_RHS);
     launch_rhs(h, save_prev);
+    record_after_rhs(h);
     enqueue_jacobi(h, h->jac_iter);
 }
 
@@ -671,19 +762,21 @@ int time_global(AdmmB200* h, int mode, float* ms) {
     const bool keep = h->persist, keep_t = h->tiled;
     h->persist = mode == 2;
     h->tiled = mode == 3;
+    h->force_plain = true;
     h->cstream = h->stream;
     constexpr int kReps = 8;
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
     bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (ok) {
-        for (int r = 0; r < kReps; r++) enqueue_global(h, false);
+        for (int r = 0; r < kReps; r++) enqueue_global(h, false, false);
         ok = cudaStreamEndCapture(h->stream, &g) == cudaSuccess && g;
     }
     ok = ok && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess;
     if (g) cudaGraphDestroy(g);
     h->persist = keep;
     h->tiled = keep_t;
+    h->force_plain = false;
     if (!ok) {
         cudaGetLastError();
         if (ge) cudaGraphExecDestroy(ge);
@@ -871,7 +964,7 @@ void enqueue_iteration(AdmmB200* h, int it, bool first, bool residual) {
         if (rc != ADMM_OK && h->enqueue_rc == ADMM_OK) h->enqueue_rc = rc;
     }
     if (branches) cudaStreamWaitEvent(main, h->ev_join, 0);
-    enqueue_global(h, residual);
+    enqueue_global(h, residual, first);
     if (residual) enqueue_residual(h);
 }
 
@@ -1030,6 +1123,111 @@ int build_step_graph(AdmmB200* h) {
             h->last_error.c_str());
     h->persist = false;
     return build_step_graph_once(h);
+}
+
+// The substep graph with the plain Jacobi global step, the fallback of a
+// learned substep whose judge failed (built once, beside the learned graph).
+int build_plain_graph(AdmmB200* h) {
+    if (h->plain_exec) return ADMM_OK;
+    cudaGraphExec_t keep = h->step_exec;
+    const int kps = h->kernels_per_step, kb = h->kernels_body, probe = h->probe_kernel;
+    h->step_exec = nullptr;
+    h->force_plain = true;
+    h->probe_kernel = 0;
+    const int rc = build_step_graph(h);
+    h->plain_exec = h->step_exec;
+    h->step_exec = keep;
+    h->force_plain = false;
+    h->probe_kernel = probe;
+    h->kernels_per_step = kps;
+    h->kernels_body = kb;
+    return rc;
+}
+
+bool learned_active(const AdmmB200* h) { return h->global_solver == 3; }
+
+// Substep starting state of a learned substep (what a re-run needs).
+int save_substep_state(AdmmB200* h) {
+    DevScene& s = h->s;
+    if (!h->sv_x0) {
+        TRY(dalloc(h, &h->sv_x0, s.n));
+        TRY(dalloc(h, &h->sv_v, s.n));
+        TRY(dalloc(h, &h->sv_ue, s.m));
+        TRY(dalloc(h, &h->sv_uc, s.nd));
+        TRY(dalloc(h, &h->sv_anim, 1));
+        CK(cudaHostAlloc((void**)&h->fail_host, sizeof(int), cudaHostAllocDefault));
+    }
+    CK(cudaMemcpyAsync(h->sv_x0, s.x0, sizeof(float4) * s.n, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->sv_v, s.v, sizeof(float4) * s.n, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->sv_ue, s.ue, sizeof(float4) * s.m, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->sv_uc, s.uc, sizeof(float4) * s.nd, cudaMemcpyDeviceToDevice, h->stream));
+    if (h->anim.counter) CK(cudaMemcpyAsync(h->sv_anim, h->anim.counter, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemsetAsync(h->learn.fail, 0, sizeof(int), h->stream));
+    return ADMM_OK;
+}
+
+int restore_substep_state(AdmmB200* h) {
+    DevScene& s = h->s;
+    CK(cudaMemcpyAsync(s.x0, h->sv_x0, sizeof(float4) * s.n, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(s.v, h->sv_v, sizeof(float4) * s.n, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(s.ue, h->sv_ue, sizeof(float4) * s.m, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(s.uc, h->sv_uc, sizeof(float4) * s.nd, cudaMemcpyDeviceToDevice, h->stream));
+    if (h->anim.counter) CK(cudaMemcpyAsync(h->anim.counter, h->sv_anim, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+    return ADMM_OK;
+}
+
+// Failed learned solves of the substep just enqueued (synchronises the stream).
+int read_learn_fail(AdmmB200* h, int* failed) {
+    CK(cudaMemcpyAsync(h->fail_host, h->learn.fail, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *failed = *h->fail_host;
+    return ADMM_OK;
+}
+
+// One substep from the graphs: a learned substep is judged and, when one of its
+// global solves failed to reduce the residual, run again from its starting state
+// with the plain Jacobi global step.
+int launch_substep(AdmmB200* h) {
+    if (!learned_active(h)) {
+        CK(cudaGraphLaunch(h->step_exec, h->stream));
+        return ADMM_OK;
+    }
+    TRY(build_plain_graph(h));
+    TRY(save_substep_state(h));
+    CK(cudaGraphLaunch(h->step_exec, h->stream));
+    int failed = 0;
+    TRY(read_learn_fail(h, &failed));
+    h->learn_substeps++;
+    if (failed) {
+        TRY(restore_substep_state(h));
+        CK(cudaGraphLaunch(h->plain_exec, h->stream));
+        h->learn_fallbacks++;
+    }
+    return ADMM_OK;
+}
+
+// The eager (profiling / recording) substep, judged the same way.
+int run_substep_eager(AdmmB200* h) {
+    h->cstream = h->stream;
+    const bool learned = learned_active(h) && h->rec_target < 0;
+    if (learned) TRY(save_substep_state(h));
+    if (h->residual_tol > 0.f) TRY(run_step_tol_eager(h, h->residual_tol));
+    else enqueue_step(h);
+    CK(cudaGetLastError());
+    if (learned) {
+        int failed = 0;
+        TRY(read_learn_fail(h, &failed));
+        h->learn_substeps++;
+        if (failed) {
+            TRY(restore_substep_state(h));
+            h->force_plain = true;
+            int rc = h->residual_tol > 0.f ? run_step_tol_eager(h, h->residual_tol) : (enqueue_step(h), ADMM_OK);
+            h->force_plain = false;
+            TRY(rc);
+            h->learn_fallbacks++;
+        }
+    }
+    return ADMM_OK;
 }
 
 float4 pack(const float* p) { return make_float4(p[0], p[1], p[2], 0.f); }
@@ -1397,7 +1595,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         return fail(h, ADMM_ERR_INVALID, "ell_lanes must be 0, 1, 2, 4 or 8");
     TRY(autotune_ell(h, as, d->ell_lanes, &h->tune_lanes_a, &h->tune_lanes_r, &h->tune_ms_a, &h->tune_ms_r));
     if (d->jacobi_mode < 0 || d->jacobi_mode > 3) return fail(h, ADMM_ERR_INVALID, "jacobi_mode must be 0, 1, 2 or 3");
-    if (d->global_solver < 0 || d->global_solver > 2) return fail(h, ADMM_ERR_INVALID, "global_solver must be 0, 1 or 2");
+    if (d->global_solver < 0 || d->global_solver > 3) return fail(h, ADMM_ERR_INVALID, "global_solver must be 0, 1, 2 or 3");
     if (d->pcg_iter < 0) return fail(h, ADMM_ERR_INVALID, "pcg_iter");
     h->global_solver = d->global_solver;
     h->pcg_iter = d->pcg_iter > 0 ? d->pcg_iter : std::max(1, d->jacobi_iter / 2);
@@ -1412,12 +1610,33 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         TRY(dalloc(h, &g.part, 2 * (size_t)g.blocks));
         TRY(dalloc(h, &g.scal, 8));
     }
+    {
+        // learned global step: the Jacobi sweep until admm_b200_set_learned (m = 1 / a_ii)
+        LearnDev& L = h->learn;
+        L.blocks = blocks(s.A.nslices * 32, kVertThreads);
+        float* minv = nullptr;
+        float* theta = nullptr;
+        TRY(dalloc(h, &minv, nd));
+        TRY(dalloc(h, &theta, nd));
+        std::vector<float> mv(nd);
+        for (int i = 0; i < nd; i++) mv[i] = 1.f / as.a_diag[i];
+        CK(cudaMemcpy(minv, mv.data(), sizeof(float) * nd, cudaMemcpyHostToDevice));
+        L.minv = minv;
+        L.theta = theta;
+        TRY(dalloc(h, &L.xl, nd));
+        TRY(dalloc(h, &L.part, 2 * (size_t)L.blocks));
+        TRY(dalloc(h, &L.stats, 4));
+        TRY(dalloc(h, &L.fail, 1));
+        h->learn_sweeps = std::max(1, h->jac_iter);
+        h->learn_omega.assign(h->learn_sweeps, 1.f);
+        h->learn_beta.assign(h->learn_sweeps, 0.f);
+    }
     h->hostA = as.A;
     h->hostAdiag = as.a_diag;
     TRY(build_persist_plan(h, as.A));
     TRY(build_tiles_dev(h, as.A));
     h->persist = h->tiled = false;
-    if (h->jac_iter >= 2 && d->global_solver == 0) {
+    if (h->jac_iter >= 2 && (d->global_solver == 0 || d->global_solver == 3)) {
         if (d->jacobi_mode == 2 && h->persist_ok) {
             h->persist = true;
         } else if (d->jacobi_mode == 3) {
@@ -1587,6 +1806,8 @@ void admm_b200_destroy(AdmmB200* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+    if (h->plain_exec) cudaGraphExecDestroy(h->plain_exec);
+    if (h->fail_host) cudaFreeHost(h->fail_host);
     for (void* p : h->allocs)
         if (p) cudaFree(p);
     for (auto e : h->prof_ev) cudaEventDestroy(e);
@@ -1612,10 +1833,7 @@ int admm_b200_step_async(AdmmB200* h, int n_steps) {
         CK(cudaEventRecord(h->ev0, h->stream));
         for (int k = 0; k < n_steps; k++) {
             h->prof_used = 0;
-            h->cstream = h->stream;
-            if (h->residual_tol > 0.f) TRY(run_step_tol_eager(h, h->residual_tol));
-            else enqueue_step(h);
-            CK(cudaGetLastError());
+            TRY(run_substep_eager(h));
             CK(cudaStreamSynchronize(h->stream));
             TRY(accumulate_timers(h));
         }
@@ -1625,7 +1843,7 @@ int admm_b200_step_async(AdmmB200* h, int n_steps) {
     }
     TRY(build_step_graph(h));
     CK(cudaEventRecord(h->ev0, h->stream));
-    for (int k = 0; k < n_steps; k++) CK(cudaGraphLaunch(h->step_exec, h->stream));
+    for (int k = 0; k < n_steps; k++) TRY(launch_substep(h));
     CK(cudaEventRecord(h->ev1, h->stream));
     h->frame += n_steps;
     return ADMM_OK;
@@ -1836,7 +2054,7 @@ int admm_b200_local_step(AdmmB200* h) {
 int admm_b200_global_step(AdmmB200* h) {
     if (!h) return ADMM_ERR_INVALID;
     CK(cudaSetDevice(h->device));
-    enqueue_global(h, false);
+    enqueue_global(h, false, true);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->stream));
     return ADMM_OK;
@@ -1995,7 +2213,7 @@ int admm_b200_step_host(AdmmB200* h, const float* x_in, const float* v_in, float
     CK(cudaMemcpyAsync(h->stage, x_in, bytes, cudaMemcpyHostToDevice, h->stream));
     if (v_in) CK(cudaMemcpyAsync(h->stage + 3 * (size_t)n, v_in, bytes, cudaMemcpyHostToDevice, h->stream));
     k_unpack_state<<<blocks(n, 256), 256, 0, h->stream>>>(h->s, h->stage, v_in ? 1 : 0);
-    CK(cudaGraphLaunch(h->step_exec, h->stream));
+    TRY(launch_substep(h));
     k_pack_state<<<blocks(n, 256), 256, 0, h->stream>>>(h->s, h->stage);
     if (x_out) CK(cudaMemcpyAsync(x_out, h->stage, bytes, cudaMemcpyDeviceToHost, h->stream));
     if (v_out) CK(cudaMemcpyAsync(v_out, h->stage + 3 * (size_t)n, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -2076,6 +2294,84 @@ int admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd) {
     if (h->step_exec) {
         cudaGraphExecDestroy(h->step_exec);
         h->step_exec = nullptr;
+    }
+    return ADMM_OK;
+}
+
+int admm_b200_set_learned(AdmmB200* h, int sweeps, const float* omega, const float* beta, const float* m,
+                          const float* theta, int nd) {
+    if (!h || !omega || !beta) return ADMM_ERR_INVALID;
+    if (sweeps < 1 || sweeps > kLearnMaxSweeps) return fail(h, ADMM_ERR_INVALID, "sweeps must be 1..32");
+    if (nd != h->s.nd) return fail(h, ADMM_ERR_INVALID, "nd must equal n_dyn");
+    for (int k = 0; k < sweeps; k++)
+        if (!std::isfinite(omega[k]) || !std::isfinite(beta[k])) return fail(h, ADMM_ERR_INVALID, "omega/beta");
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<float> mv(nd), th(nd, 0.f);
+    for (int i = 0; i < nd; i++) {
+        mv[i] = m ? m[i] : 1.f / h->hostAdiag[i];
+        if (theta) th[i] = theta[i];
+        if (!std::isfinite(mv[i]) || !std::isfinite(th[i])) return fail(h, ADMM_ERR_INVALID, "m/theta");
+    }
+    CK(cudaMemcpy(const_cast<float*>(h->learn.minv), mv.data(), sizeof(float) * nd, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(const_cast<float*>(h->learn.theta), th.data(), sizeof(float) * nd, cudaMemcpyHostToDevice));
+    h->learn_sweeps = sweeps;
+    h->learn_omega.assign(omega, omega + sweeps);
+    h->learn_beta.assign(beta, beta + sweeps);
+    h->learn_beta[0] = 0.f;  // the first sweep has no previous iterate
+    // the coefficients are kernel arguments of the step graph: capture it again
+    if (h->step_exec) {
+        cudaGraphExecDestroy(h->step_exec);
+        h->step_exec = nullptr;
+    }
+    return ADMM_OK;
+}
+
+int admm_b200_learned_stats(AdmmB200* h, int64_t* out4) {
+    if (!h || !out4) return ADMM_ERR_INVALID;
+    CK(cudaSetDevice(h->device));
+    CK(cudaStreamSynchronize(h->stream));
+    unsigned long long d[2] = {0, 0};
+    CK(cudaMemcpy(d, h->learn.stats, sizeof(d), cudaMemcpyDeviceToHost));
+    out4[0] = h->learn_substeps;
+    out4[1] = h->learn_fallbacks;
+    out4[2] = (int64_t)d[0];
+    out4[3] = (int64_t)d[1];
+    return ADMM_OK;
+}
+
+int admm_b200_record_global(AdmmB200* h, int iteration, float* b, float* x_cur, float* x_last, int nd) {
+    if (!h || !b || !x_cur || !x_last) return ADMM_ERR_INVALID;
+    if (nd != h->s.nd) return fail(h, ADMM_ERR_INVALID, "nd must equal n_dyn");
+    if (iteration < 1 || iteration >= h->admm_max_iter) return fail(h, ADMM_ERR_INVALID, "iteration must be 1..admm_max_iter-1");
+    CK(cudaSetDevice(h->device));
+    if (!h->rec_b) {
+        TRY(dalloc(h, &h->rec_b, nd));
+        TRY(dalloc(h, &h->rec_cur, nd));
+        TRY(dalloc(h, &h->rec_last, nd));
+    }
+    h->rec_target = iteration;
+    h->rec_count = 0;
+    const bool prof = h->profiling;
+    h->profiling = false;
+    const int rc = run_substep_eager(h);
+    h->profiling = prof;
+    const int recorded = h->rec_count;
+    h->rec_target = -1;
+    TRY(rc);
+    CK(cudaStreamSynchronize(h->stream));
+    h->frame += 1;
+    if (recorded <= iteration) return fail(h, ADMM_ERR_STATE, "the substep ended before the recorded iteration");
+    std::vector<float4> t(nd);
+    float* outs[3] = {b, x_cur, x_last};
+    float4* srcs[3] = {h->rec_b, h->rec_cur, h->rec_last};
+    for (int k = 0; k < 3; k++) {
+        CK(cudaMemcpy(t.data(), srcs[k], sizeof(float4) * nd, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < nd; i++) {
+            outs[k][3 * i] = t[i].x;
+            outs[k][3 * i + 1] = t[i].y;
+            outs[k][3 * i + 2] = t[i].z;
+        }
     }
     return ADMM_OK;
 }

@@ -33,7 +33,7 @@ constexpr int kFin = 6;       // node features
 constexpr int kFe = 2;        // edge features
 constexpr int kEdgeIn = 2 * kH + kFe;
 constexpr int kNodeIn = 2 * kH;
-constexpr int kOut = 6;       // head: lower-triangular factor of the block
+constexpr int kOut = 7;       // head: lower-triangular factor of the block (6), warm-start coefficient (1)
 constexpr int kRowsPerBlockW = 2048;  // rows per partial of a weight gradient
 
 __device__ __forceinline__ float wval(const float* W, int i, int bf16) {
@@ -330,7 +330,7 @@ __global__ void k_accum_gB(const float* __restrict__ gz, const float* __restrict
 
 // Head backward: go from gB (dL/dB) -- G = gB / a, gL = (G + G^T) L, go as in the header.
 __global__ void k_head_grad(const float* __restrict__ gB, const float* __restrict__ o, const float* __restrict__ adiag,
-                            int n, float* __restrict__ go) {
+                            int n, float* __restrict__ go, const float* __restrict__ gth) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float L[9], G[9], gL[9];
@@ -351,6 +351,25 @@ __global__ void k_head_grad(const float* __restrict__ gB, const float* __restric
     g[3] = gL[3];
     g[4] = gL[6];
     g[5] = gL[7];
+    g[6] = (gth && fabsf(oi[6]) < 1.f) ? gth[i] : 0.f;
+}
+
+// m_i = trace(B_i) / 3 (the isotropic part of the block: the system is A (x) I3),
+// theta_i = clamp(o_i6, -1, 1).
+__global__ void k_outputs(const float* __restrict__ B, const float* __restrict__ o, int n, float* __restrict__ m,
+                          float* __restrict__ th) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    m[i] = (B[(size_t)i * 9] + B[(size_t)i * 9 + 4] + B[(size_t)i * 9 + 8]) * (1.f / 3.f);
+    th[i] = fminf(fmaxf(o[(size_t)i * kOut + 6], -1.f), 1.f);
+}
+
+// gB_i = (gm_i / 3) I
+__global__ void k_gm_to_gB(const float* __restrict__ gm, int n, float* __restrict__ gB) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = gm[i] * (1.f / 3.f);
+    for (int k = 0; k < 9; k++) gB[(size_t)i * 9 + k] = (k % 4 == 0) ? v : 0.f;
 }
 
 // d = g * (z > 0)
@@ -503,6 +522,8 @@ int tc_status(AdmmGnn* g) {
     return ADMM_ERR_TIMEOUT;
 }
 
+void backward_from_head(AdmmGnn* g);
+
 }  // namespace
 
 extern "C" {
@@ -630,8 +651,7 @@ int admm_gnn_forward(AdmmGnn* g, float* blocks9) {
 // null) receives it.
 int admm_gnn_loss_grad(AdmmGnn* g, const float* R, int K, double* loss, float* grad) {
     if (!g || g->n <= 0 || !R || K <= 0) return ADMM_ERR_INVALID;
-    const Off f = offsets();
-    const int n = g->n, E = g->E;
+    const int n = g->n;
     forward(g);
     cudaMemsetAsync(g->grad, 0, sizeof(float) * g->P, g->st);
     cudaMemsetAsync(g->gB, 0, sizeof(float) * 9 * (size_t)n, g->st);
@@ -656,7 +676,52 @@ int admm_gnn_loss_grad(AdmmGnn* g, const float* R, int K, double* loss, float* g
         k_accum_gB<<<nblk(n, 256), 256, 0, g->st>>>(g->gzv, g->r, n, g->scal, g->gB);
         if (cudaStreamSynchronize(g->st) != cudaSuccess) return ADMM_ERR_CUDA;
     }
-    k_head_grad<<<nblk(n, 256), 256, 0, g->st>>>(g->gB, g->o, g->adiag, n, g->go);
+    k_head_grad<<<nblk(n, 256), 256, 0, g->st>>>(g->gB, g->o, g->adiag, n, g->go, nullptr);
+    backward_from_head(g);
+    if (grad) cudaMemcpyAsync(grad, g->grad, sizeof(float) * g->P, cudaMemcpyDeviceToHost, g->st);
+    if (cudaStreamSynchronize(g->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ADMM_ERR_CUDA;
+    if (loss) *loss = total;
+    return tc_status(g);
+}
+
+// Per-vertex outputs of the learned global step: m (n) and theta (n), host.
+int admm_gnn_outputs(AdmmGnn* g, float* m, float* theta) {
+    if (!g || g->n <= 0 || !m || !theta) return ADMM_ERR_INVALID;
+    forward(g);
+    k_outputs<<<nblk(g->n, 256), 256, 0, g->st>>>(g->B, g->o, g->n, g->r, g->zv);
+    cudaMemcpyAsync(m, g->r, sizeof(float) * g->n, cudaMemcpyDeviceToHost, g->st);
+    cudaMemcpyAsync(theta, g->zv, sizeof(float) * g->n, cudaMemcpyDeviceToHost, g->st);
+    if (cudaStreamSynchronize(g->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ADMM_ERR_CUDA;
+    return tc_status(g);
+}
+
+// Gradient of a loss with respect to the parameters, given its gradients gm and
+// gtheta (host, n each) with respect to the outputs of admm_gnn_outputs (at the
+// current parameters and graph); grad (host, may be null) receives it, and the
+// next admm_gnn_adam applies it.
+int admm_gnn_backward(AdmmGnn* g, const float* gm, const float* gtheta, float* grad) {
+    if (!g || g->n <= 0 || !gm || !gtheta) return ADMM_ERR_INVALID;
+    const int n = g->n;
+    forward(g);
+    cudaMemsetAsync(g->grad, 0, sizeof(float) * g->P, g->st);
+    cudaMemcpyAsync(g->r, gm, sizeof(float) * n, cudaMemcpyHostToDevice, g->st);
+    cudaMemcpyAsync(g->zv, gtheta, sizeof(float) * n, cudaMemcpyHostToDevice, g->st);
+    k_gm_to_gB<<<nblk(n, 256), 256, 0, g->st>>>(g->r, n, g->gB);
+    k_head_grad<<<nblk(n, 256), 256, 0, g->st>>>(g->gB, g->o, g->adiag, n, g->go, g->zv);
+    backward_from_head(g);
+    if (grad) cudaMemcpyAsync(grad, g->grad, sizeof(float) * g->P, cudaMemcpyDeviceToHost, g->st);
+    if (cudaStreamSynchronize(g->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ADMM_ERR_CUDA;
+    return tc_status(g);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The backward pass from the head gradient go (dL/do) into g->grad.
+void backward_from_head(AdmmGnn* g) {
+    const Off f = offsets();
+    const int n = g->n, E = g->E;
     dense_bwd(g, g->go, g->h[3], n, kH, f.Wo, kOut, g->gh);          // gh = dL/dh3
     for (int l = 2; l >= 0; l--) {
         const size_t nh = (size_t)n * kH;
@@ -669,11 +734,11 @@ int admm_gnn_loss_grad(AdmmGnn* g, const float* R, int K, double* loss, float* g
     }
     k_relu_mask<<<nblk((size_t)n * kH, 256), 256, 0, g->st>>>(g->gh, g->z0, (size_t)n * kH, g->gz);
     dense_bwd(g, g->gz, g->x, n, kFin, f.W0, kH, nullptr);
-    if (grad) cudaMemcpyAsync(grad, g->grad, sizeof(float) * g->P, cudaMemcpyDeviceToHost, g->st);
-    if (cudaStreamSynchronize(g->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return ADMM_ERR_CUDA;
-    if (loss) *loss = total;
-    return tc_status(g);
 }
+
+}  // namespace
+
+extern "C" {
 
 // One Adam step on the gradient of the last admm_gnn_loss_grad.
 int admm_gnn_adam(AdmmGnn* g, float lr) {

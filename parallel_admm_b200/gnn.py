@@ -45,6 +45,13 @@ def _lib():
             "admm_gnn_loss_grad": (ctypes.c_int, [vp, _f, ctypes.c_int, _d, _f]),
             "admm_gnn_adam": (ctypes.c_int, [vp, ctypes.c_float]),
             "admm_b200_system": (ctypes.c_int, [vp, _i, _i, _f, _f]),
+            "admm_gnn_outputs": (ctypes.c_int, [vp, _f, _f]),
+            "admm_gnn_backward": (ctypes.c_int, [vp, _f, _f, _f]),
+            "admm_learn_create": (ctypes.c_int, [ctypes.c_int, _i, _i, _f, _f, ctypes.POINTER(vp)]),
+            "admm_learn_destroy": (None, [vp]),
+            "admm_learn_loss_grad": (ctypes.c_int, [vp, ctypes.c_int, _f, _f, _f, _f, ctypes.c_int, _f, _f, _f, _f,
+                                                    _d, _f, _f, _f, _f]),
+            "admm_learn_solve": (ctypes.c_int, [vp, _f, _f, ctypes.c_double, ctypes.c_int, _i]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -243,6 +250,27 @@ class LearnedPreconditioner:
             raise B.AdmmError(rc, "admm_gnn_loss_grad")
         return loss.value, grad
 
+    def outputs(self, sysm: System, x: np.ndarray, ef: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        """(m, theta) per vertex for the learned global step (global_solver 3)."""
+        self.bind(sysm, x, ef)
+        m = np.zeros(sysm.n, np.float32)
+        th = np.zeros(sysm.n, np.float32)
+        rc = _lib().admm_gnn_outputs(self.g, _p(m, _f), _p(th, _f))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_gnn_outputs")
+        return m, th
+
+    def backward(self, sysm: System, x: np.ndarray, ef: np.ndarray, gm: np.ndarray, gth: np.ndarray) -> np.ndarray:
+        """Parameter gradient from the gradients with respect to (m, theta); Adam applies it."""
+        self.bind(sysm, x, ef)
+        gm = np.ascontiguousarray(gm, np.float32)
+        gth = np.ascontiguousarray(gth, np.float32)
+        grad = np.zeros(self.P, np.float32)
+        rc = _lib().admm_gnn_backward(self.g, _p(gm, _f), _p(gth, _f), _p(grad, _f))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_gnn_backward")
+        return grad
+
     def step(self, lr: float):
         rc = _lib().admm_gnn_adam(self.g, ctypes.c_float(lr))
         if rc != B.OK:
@@ -266,6 +294,185 @@ class LearnedPreconditioner:
         return hist
 
 
+class SweepTrainer:
+    """GPU context of the learned global step's training on one system (learn.cu)."""
+
+    def __init__(self, sysm: System):
+        self.sysm = sysm
+        self.L = vp()
+        rc = _lib().admm_learn_create(sysm.n, _p(sysm.start, _i), _p(sysm.col, _i), _p(sysm.val, _f),
+                                      _p(sysm.diag, _f), ctypes.byref(self.L))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_learn_create")
+
+    def close(self):
+        if self.L:
+            _lib().admm_learn_destroy(self.L)
+            self.L = vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, b: np.ndarray, x0: np.ndarray, tol: float = 1e-6, maxit: int = 20000) -> Tuple[np.ndarray, int]:
+        """The converged solution of A x = b (conjugate gradients from x0)."""
+        bb = np.ascontiguousarray(b, np.float32)
+        x = np.array(x0, np.float32, copy=True, order="C")
+        it = ctypes.c_int32()
+        rc = _lib().admm_learn_solve(self.L, _p(bb, _f), _p(x, _f), tol, maxit, ctypes.byref(it))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_learn_solve")
+        return x, it.value
+
+    def loss_grad(self, omega, beta, m, theta, b, xc, xl, xs):
+        """Mean |x_K - x*|_A^2 / |x_c - x*|_A^2 over the samples and its gradients
+        (omega, beta, m, theta)."""
+        K = len(omega)
+        om = np.ascontiguousarray(omega, np.float32)
+        be = np.ascontiguousarray(beta, np.float32)
+        mm = np.ascontiguousarray(m, np.float32)
+        th = np.ascontiguousarray(theta, np.float32)
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (b, xc, xl, xs)]
+        S = arrs[0].shape[0]
+        loss = ctypes.c_double()
+        go, gb = np.zeros(K, np.float32), np.zeros(K, np.float32)
+        gm, gt = np.zeros(self.sysm.n, np.float32), np.zeros(self.sysm.n, np.float32)
+        rc = _lib().admm_learn_loss_grad(self.L, K, _p(om, _f), _p(be, _f), _p(mm, _f), _p(th, _f), S,
+                                         *[_p(a, _f) for a in arrs], ctypes.byref(loss), _p(go, _f), _p(gb, _f),
+                                         _p(gm, _f), _p(gt, _f))
+        if rc != B.OK:
+            raise B.AdmmError(rc, "admm_learn_loss_grad")
+        return loss.value, go, gb, gm, gt
+
+
+def global_samples(h: "B.Handle", trainer: SweepTrainer, frames: int, iterations: Sequence[int],
+                   tol: float = 1e-6) -> Tuple[np.ndarray, ...]:
+    """(b, x_c, x_l, x*) samples of the global step from plain substeps: frame f records
+    global step iterations[f % len(iterations)] (every recording is one substep of the
+    simulation); x* by conjugate gradients on the GPU."""
+    bs, xcs, xls, xss = [], [], [], []
+    for f in range(frames):
+        it = int(iterations[f % len(iterations)])
+        b, xc, xl = h.record_global(it, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
+        xs, _ = trainer.solve(b, xc, tol)
+        bs.append(b)
+        xcs.append(xc)
+        xls.append(xl)
+        xss.append(xs)
+    return tuple(np.array(a, np.float32) for a in (bs, xcs, xls, xss))
+
+
+def chebyshev_coefficients(K: int, lo: float, hi: float) -> Tuple[np.ndarray, np.ndarray]:
+    """(omega, beta) of K steps of the three-term Chebyshev iteration for the spectrum
+    [lo, hi] of the preconditioned matrix (Saad, Iterative Methods, Alg. 12.1)."""
+    theta = (hi + lo) / 2.0
+    delta = (hi - lo) / 2.0
+    sigma = theta / delta
+    rho = 1.0 / sigma
+    om, be = [1.0 / theta], [0.0]
+    for _ in range(1, K):
+        rn = 1.0 / (2.0 * sigma - rho)
+        om.append(2.0 * rn / delta)
+        be.append(rn * rho)
+        rho = rn
+    return np.array(om, np.float32), np.array(be, np.float32)
+
+
+def jacobi_spectrum_top(sysm: System, iters: int = 60, seed: int = 0) -> float:
+    """Largest eigenvalue of D^-1 A by the power method (host, FP64)."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(sysm.n, 1))
+    d = sysm.diag.astype(np.float64)
+    lam = 1.0
+    for _ in range(iters):
+        w = sysm.matvec(np.repeat(v, 3, 1))[:, :1] / d[:, None]
+        lam = float(np.linalg.norm(w) / max(np.linalg.norm(v), 1e-300))
+        v = w / max(np.linalg.norm(w), 1e-300)
+    return lam
+
+
+class LearnedGlobalStep:
+    """The learned global step: the network (per-vertex m and warm-start theta) and the
+    per-sweep coefficients (omega, beta), trained together on the error after K sweeps.
+
+    Starts as plain Jacobi at the network's side (zero head: m = 1 / a_ii, theta = 0);
+    the coefficients start as K steps of Chebyshev on [lo_frac * lam_max, lam_max] of
+    D^-1 A (omega = 1, beta = 0 with chebyshev=False)."""
+
+    def __init__(self, K: int = 10, bf16: bool = True, seed: int = 0):
+        self.K = K
+        self.net = LearnedPreconditioner(bf16=bf16, seed=seed)
+        self.omega = np.ones(K, np.float32)
+        self.beta = np.zeros(K, np.float32)
+        self._m = np.zeros(2 * K)
+        self._v = np.zeros(2 * K)
+        self._t = 0
+
+    def init_chebyshev(self, lam_max: float, lo_frac: float = 0.1):
+        self.omega, self.beta = chebyshev_coefficients(self.K, lo_frac * lam_max, 1.02 * lam_max)
+
+    def outputs(self, sysm: System, x: np.ndarray, ef: np.ndarray):
+        return self.net.outputs(sysm, x, ef)
+
+    def fit(self, data, epochs: int = 5, batch: int = 8, lr: float = 1e-3, lr_coef: float = 2e-3,
+            seed: int = 0) -> List[float]:
+        """data: list of (sysm, node feats, edge feats, SweepTrainer, (b, xc, xl, xs) arrays).
+        Adam on the network (GPU) and on the coefficients (host) with the GPU gradients;
+        returns the mean loss per epoch."""
+        rng = np.random.default_rng(seed)
+        hist = []
+        for _ in range(epochs):
+            tot, cnt = 0.0, 0
+            for k in rng.permutation(len(data)):
+                sysm, x, ef, tr, S = data[k]
+                order = rng.permutation(S[0].shape[0])
+                for j in range(0, len(order), batch):
+                    sel = order[j:j + batch]
+                    m, th = self.net.outputs(sysm, x, ef)
+                    loss, go, gb, gm, gt = tr.loss_grad(self.omega, self.beta, m, th, *(a[sel] for a in S))
+                    self.net.backward(sysm, x, ef, gm, gt)
+                    self.net.step(lr)
+                    self._adam_coef(go, gb, lr_coef)
+                    tot += loss
+                    cnt += 1
+            hist.append(tot / max(cnt, 1))
+        return hist
+
+    def _adam_coef(self, go, gb, lr, b1=0.9, b2=0.999, eps=1e-8):
+        g = np.concatenate([go, gb]).astype(np.float64)
+        g[self.K] = 0.0  # beta_0 is not used
+        self._t += 1
+        self._m = b1 * self._m + (1 - b1) * g
+        self._v = b2 * self._v + (1 - b2) * g * g
+        step = lr * (self._m / (1 - b1 ** self._t)) / (np.sqrt(self._v / (1 - b2 ** self._t)) + eps)
+        self.omega = (self.omega - step[:self.K]).astype(np.float32)
+        self.beta = (self.beta - step[self.K:]).astype(np.float32)
+        self.beta[0] = 0.0
+
+    def evaluate(self, tr: SweepTrainer, m, th, S) -> float:
+        return tr.loss_grad(self.omega, self.beta, m, th, *S)[0]
+
+    def apply(self, h: "B.Handle", sysm: System, x: np.ndarray, ef: np.ndarray):
+        """Hand the learned step to a handle created with global_solver 3."""
+        m, th = self.net.outputs(sysm, x, ef)
+        h.set_learned(self.omega, self.beta, m, th)
+        return m, th
+
+    def save(self, path: str):
+        np.savez(path, params=self.net.params(), omega=self.omega, beta=self.beta, K=self.K)
+
+    @classmethod
+    def load(cls, path: str, bf16: bool = True) -> "LearnedGlobalStep":
+        d = np.load(path)
+        obj = cls(K=int(d["K"]), bf16=bf16)
+        obj.net.set_params(d["params"])
+        obj.omega = d["omega"].astype(np.float32)
+        obj.beta = d["beta"].astype(np.float32)
+        return obj
+
+
 def init_params(seed: int = 0) -> np.ndarray:
     """Scaled normal weights, zero biases, zero head (the network starts as diag(A)^-1)."""
     rng = np.random.default_rng(seed)
@@ -273,7 +480,7 @@ def init_params(seed: int = 0) -> np.ndarray:
     shapes = [(H, F_IN), (H,)]
     for _ in range(3):
         shapes += [(H, 2 * H + F_E), (H,), (H, 2 * H), (H,)]
-    shapes += [(6, H), (6,)]
+    shapes += [(7, H), (7,)]
     parts = []
     for s in shapes:
         parts.append(rng.normal(scale=1.0 / np.sqrt(s[1]), size=s) if len(s) == 2 else np.zeros(s))

@@ -271,13 +271,13 @@ def lumped_mass(n: int, verts: np.ndarray, faces: np.ndarray, face_density: np.n
         area = 0.5 * np.linalg.norm(np.cross(v[faces[:, 1]] - v[faces[:, 0]],
                                              v[faces[:, 2]] - v[faces[:, 0]]), axis=1)
         for j in range(3):
-            np.add.at(mass, faces[:, j], area / 3.0 * face_density)
+            mass += np.bincount(faces[:, j], weights=area / 3.0 * face_density, minlength=n)
     if len(tets):
         d = np.stack([v[tets[:, 1]] - v[tets[:, 0]], v[tets[:, 2]] - v[tets[:, 0]],
                       v[tets[:, 3]] - v[tets[:, 0]]], axis=2)
         vol = np.abs(np.linalg.det(d)) / 6.0
         for j in range(4):
-            np.add.at(mass, tets[:, j], vol / 4.0 * tet_density)
+            mass += np.bincount(tets[:, j], weights=vol / 4.0 * tet_density, minlength=n)
     return mass
 
 
@@ -294,8 +294,11 @@ def boundary_facets(tets: np.ndarray) -> np.ndarray:
     """Faces that belong to exactly one tet, oriented outward (igl::boundary_facets)."""
     faces = np.concatenate([tets[:, [1, 2, 3]], tets[:, [0, 3, 2]],
                             tets[:, [0, 1, 3]], tets[:, [0, 2, 1]]])
-    key = np.sort(faces, axis=1)
-    _, inv, cnt = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+    key = np.sort(faces, axis=1).astype(np.int64)
+    nv = int(key.max()) + 1 if len(key) else 1
+    # one int64 per sorted face (nv^3 < 2^63 for nv < 2 M), so the duplicate count is a 1-D unique
+    k1 = (key[:, 0] * nv + key[:, 1]) * nv + key[:, 2]
+    _, inv, cnt = np.unique(k1, return_inverse=True, return_counts=True)
     return faces[cnt[inv.ravel()] == 1].astype(np.int32)
 
 
@@ -612,13 +615,17 @@ def sheets_on_sphere(nx: int = 512, layers: int = 4, seed: int = 0, side: float 
                     meta={"config": "sheets on sphere", "seed": seed, "nx": nx, "layers": layers})
 
 
-def batch_bodies(n_bodies: int = 256, seed: int = 0, vmin: int = 500, vmax: int = 20000) -> Scene:
+def batch_bodies(n_bodies: int = 256, seed: int = 0, vmin: int = 500, vmax: int = 20000,
+                 only: Optional[List[int]] = None) -> Scene:
     """`n_bodies` independent tet soft bodies of uneven size: cubes and voxelised ellipsoids with
     log-uniform vertex counts in [vmin, vmax], E log-uniform in [1e4, 1e6], friction U(0.2, 0.6)
-    per body, each dropped 0.1-0.5 m onto the ground.  The bodies sit on a square layout with
-    gaps wider than any body, over one ground quad (for bodies that never meet, the same as a
-    ground each); h = 1/100, 30 ADMM iterations.  The engine treats the batch as one scene:
-    one block-diagonal segmented matrix, one collision grid.
+    per body, each released at rest with its lowest point 6-20 mm above the ground (contact
+    thickness 12 mm), so the ground contacts start in the first frames and last through the
+    run.  The bodies sit on a square layout with gaps wider than any body, over one ground quad
+    (for bodies that never meet, the same as a ground each); h = 1/100, 30 ADMM iterations.
+    The engine treats the batch as one scene: one block-diagonal segmented matrix, one
+    collision grid.  `only` keeps the listed bodies (same sizes, materials and placements as
+    in the full batch), e.g. a size-stratified sample for a CPU baseline.
     """
     rng = np.random.default_rng(seed)
     cell = 0.02
@@ -641,6 +648,9 @@ def batch_bodies(n_bodies: int = 256, seed: int = 0, vmin: int = 500, vmax: int 
         specs.append((ellipsoid, dims))
         pitch = max(pitch, max(dims) * cell)
     pitch = pitch * 1.5 + 0.1
+    keep_set = None if only is None else set(int(k) for k in only)
+    body_ids = []
+    all_counts = []
     for b, (ellipsoid, dims) in enumerate(specs):
         if ellipsoid:
             half = np.array(dims) * cell / 2
@@ -654,16 +664,23 @@ def batch_bodies(n_bodies: int = 256, seed: int = 0, vmin: int = 500, vmax: int 
         v = v - v.mean(0)
         v = v @ _rand_rot(rng).T
         gx, gz = (b % nside - (nside - 1) / 2) * pitch, (b // nside - (nside - 1) / 2) * pitch
-        v = v + np.array([gx, -v[:, 1].min() + rng.uniform(0.1, 0.5), gz])
+        v = v + np.array([gx, -v[:, 1].min() + rng.uniform(0.006, 0.02), gz])
         E = float(10 ** rng.uniform(4, 6))
-        bodies.append(_Body(v, np.zeros((0, 3), np.int32), t, 1000.0, E / (1 + 0.4),
-                            mu=float(rng.uniform(0.2, 0.6))))
+        mu = float(rng.uniform(0.2, 0.6))
+        all_counts.append((len(v), len(t)))
+        if keep_set is not None and b not in keep_set:
+            continue
+        bodies.append(_Body(v, np.zeros((0, 3), np.int32), t, 1000.0, E / (1 + 0.4), mu=mu))
+        body_ids.append(b)
     gv, gf = ground_quad(nside * pitch / 2 + 1.0, 0.0)
     bodies.append(_Body(gv, gf, np.zeros((0, 4), np.int32), 1e12, 0.0, static=True))
     params = SolverParams(dt=1.0 / 100, g=9.8, mu=0.4, thickness=0.6 * cell, admm_max_iter=30,
                           dcd_interval=5, gs_max_iter=10, jacobi_iter=20, max_contacts=2_000_000)
     return assemble(f"batch{n_bodies}", bodies, [], params,
-                    meta={"config": "batched soft bodies", "seed": seed, "bodies": n_bodies})
+                    meta={"config": "batched soft bodies", "seed": seed, "bodies": n_bodies,
+                          "only": None if only is None else sorted(keep_set), "body_ids": body_ids,
+                          "body_verts": [len(b.verts) for b in bodies if not b.static],
+                          "all_body_counts": all_counts})
 
 
 CONFIGS = {

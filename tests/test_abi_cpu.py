@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _header_symbols():
     txt = open(os.path.join(ROOT, "include", "admm_b200.h")).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(admm_(?:b200|gnn)_\w+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(admm_(?:b200|gnn|learn)_\w+)\s*\(", txt)))
 
 
 def test_library_exports_every_declared_symbol():

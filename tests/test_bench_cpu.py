@@ -24,9 +24,11 @@ def test_reference_arm_prints_one_contract_line():
     assert d["unit"] == "steps/s" and d["higher_is_better"] is True
     assert d["value"] > 0 and d["steps"] == 2 and d["n_gpus"] == 1
     assert d["metric"].startswith("sim steps/s")
-    assert d["config"]["workload"].startswith("tet cube 20^3")
+    assert d["config"]["workload"].startswith("256 independent tet soft bodies")
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
+    # a size-stratified sample of 16 bodies, scaled to the batch by its work share
+    assert "16 of 256" in cb["sample"] and "work share" in cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
 

@@ -111,6 +111,29 @@ def test_noalloc_jacobi_matches_handle_path_twice():
         got = t_out.cpu().numpy()
         err = np.abs(got - ref).max() / max(1.0, np.abs(ref).max())
         assert err <= TOL, (call, sweeps, err)
+    # in place (x_out == x_in): no sweep (nothing to do), one sweep (through the scratch, then a
+    # copy back) and two sweeps, each against the handle path
+    for sweeps in (0, 1, 2):
+        b = rng.normal(size=(nd, 3)).astype(np.float32) * np.float32(0.1)
+        x = sc.verts[:nd] + rng.normal(scale=1e-3, size=(nd, 3)).astype(np.float32)
+        xh = np.zeros((sc.n_vert, 3), np.float32)
+        xh[:nd] = x
+        xh[nd:] = sc.verts[nd:]
+        h.write(B.BUF_X, xh)
+        h.write(B.BUF_B, b)
+        if sweeps:
+            h.jacobi(sweeps)
+        ref = h.read(B.BUF_X)[:nd]
+        t_b = torch.from_numpy(b).to(dev)
+        t_x = torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+        stream = torch.cuda.current_stream().cuda_stream
+        rc = B.lib().admm_b200_jacobi_noalloc(nd, _ptr(t_start), _ptr(t_cols), _ptr(t_vals), _ptr(t_diag),
+                                             _ptr(t_b), _ptr(t_x), _ptr(t_x), sweeps, ctypes.c_void_p(stream))
+        assert rc == B.OK, ("in place", sweeps, rc)
+        torch.cuda.synchronize()
+        got = t_x.cpu().numpy()
+        err = np.abs(got - ref).max() / max(1.0, np.abs(ref).max())
+        assert err <= TOL, ("in place", sweeps, err)
     # sizes beyond the static scratch are rejected, nothing is launched
     rc = B.lib().admm_b200_jacobi_noalloc(262145, _ptr(t_start), _ptr(t_cols), _ptr(t_vals), _ptr(t_diag),
                                          _ptr(t_b), _ptr(t_x), _ptr(t_out), 1, None)
