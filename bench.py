@@ -438,24 +438,33 @@ def main():
     bytes_io = 2 * sc.n_vert * 3 * 4
 
     # Device time per phase inside the step graph (events at phase changes), over the first
-    # --phase-steps timed frames (first chunk of each step); the roofline divides the probed
-    # kernel's bytes by its phase's time per launch.  Then an event pair around each of the
-    # first launches of the probed class (a pass of its own: the events break the overlap).
+    # --phase-steps timed frames, on a handle with the same solver and tuning that runs all
+    # admm_max_iter iterations (no conditional node, whose body holds no events; the
+    # contact frames run to the cap anyway); the roofline divides the probed kernel's bytes by
+    # its phase's time per launch.  Then an event pair around each of the first launches of the
+    # probed class (a pass of its own: the events break the overlap).
     phases = None
     probe_ms, probe_n = 0.0, 0
     if rank == 0:
         nph = min(args.steps, args.phase_steps)
-        h.reset()
+        tn0 = h.tuning()
+        sc_ph = sc
+        sc_ph.params.ell_lanes = tn0["jacobi_lanes"] if tn0["jacobi_lanes"] == tn0["rhs_lanes"] else sc.params.ell_lanes
+        hp = B.Handle(sc_ph, device=local, residual_tol=0.0,
+                      global_solver={"learned": 3, "jacobi": 0, "pcg": 1}[args.solver])
+        if args.solver == "learned":
+            learned_model(args, hp, sc_ph)
         for _ in range(args.start_frame):
-            h.step(1, allow=allow)
-        h.set_probe("phases")
-        h.phase_times()
+            hp.step(1, allow=allow)
+        hp.set_probe("phases")
+        hp.phase_times()
         for _ in range(nph):
-            h.step(1, allow=allow)
-        raw = h.phase_times()
+            hp.step(1, allow=allow)
+        raw = hp.phase_times()
         phases = {k: {"ms_per_step": v["ms"] / nph, "launches_per_step": v["launches"] / nph} for k, v in raw.items()}
-        phases["scope"] = (f"frames {args.start_frame}..{args.start_frame + nph - 1}, "
-                           + ("first chunk of each step" if args.tol > 0 else "whole step"))
+        phases["scope"] = (f"frames {args.start_frame}..{args.start_frame + nph - 1}, whole step, "
+                           f"{sc.params.admm_max_iter} ADMM iterations (no residual test)")
+        hp.close()
         h.reset()
         for _ in range(args.start_frame):
             h.step(1, allow=allow)

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define ADMM_B200_ABI_VERSION 4
+#define ADMM_B200_ABI_VERSION 5
 
 /* status codes */
 #define ADMM_OK                    0
@@ -146,6 +146,19 @@ typedef struct AdmmB200Desc {
      * points by Eberly's queries of distPT.h / distEE.h).  1 uses the grid broad
      * phase whatever broad_phase says. */
     int32_t contact_semantics;
+    /* Solver semantics: 0 = the GPU backend's (ADMMImplGPU, admm_impl_gpu.cu:256-344);
+     * 1 = the CPU backend's (ADMMImplCPU::step_fast, admm_impl_cpu.cpp:264-359):
+     * Rayleigh damping Damp = dt (damp_k_L sum_{tri, tet, bending rows} w D_r^T D_r +
+     * damp_k_M M) added to A and b_ini = Damp x0 added to every right-hand side
+     * (admm_impl_cpu.cpp:191,221,295,344), S_c without the GPU backend's per-vertex
+     * contact counts (compute_Scc, admm_impl_cpu.cpp:361-380), the friction-cone
+     * projection as serial Gauss-Seidel over the contact list in its order
+     * (_project_feasible_plain, admm_impl_cpu.cpp:390-407), and contact_semantics 1.
+     * The reference factorises the damped A exactly (SimplicialLLT,
+     * linear_solver_cpu.h:16-23); here the global step is global_solver 1 (conjugate
+     * gradients) with pcg_iter iterations, enough to converge.  ABI version 5. */
+    int32_t backend_semantics;
+    float damp_k_L, damp_k_M;     /* ADMMSolverConfig defaults 1e-4 and 0 (admm_config.h:52-53) */
 } AdmmB200Desc;
 
 /* Per-step statistics (superset of Solver::StepMetrics, solver.h:29-45). */

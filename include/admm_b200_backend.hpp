@@ -13,6 +13,7 @@
 // Header-only; compile it where the reference headers are on the include path
 // (admm_b200_reference_types.hpp) and link libadmm_b200.so.
 #pragma once
+#include <algorithm>
 #include <array>
 #include <chrono>
 #include <memory>
@@ -39,6 +40,7 @@ public:
     int pcg_iter = 0;
     int query_lanes = 0;  // 0 = chosen from the number of DCD queries
     int contact_semantics = 0;  // 1 = the CPU backend's contact predicates (ProximalQuery)
+    int backend_semantics = 0;  // 1 = the CPU backend's solver (damping, S_c, serial Gauss-Seidel contact)
 
     ~ADMMInnerB200() override {
         if (h_) admm_b200_destroy(h_);
@@ -201,6 +203,9 @@ private:
         d.pcg_iter = pcg_iter;
         d.query_lanes = query_lanes;
         d.contact_semantics = contact_semantics;
+        d.backend_semantics = backend_semantics;
+        d.damp_k_L = (float)cfg.damp_k_L;  // ADMMSolverConfig (admm_config.h:52-53)
+        d.damp_k_M = (float)cfg.damp_k_M;
     }
 };
 
@@ -221,6 +226,69 @@ public:
 
 private:
     std::unique_ptr<ADMMInnerB200> impl_;
+};
+
+// ICollisionDetector over the backend's handle: the counterpart of BVH_GPU
+// (src/contact/collision_detection_cuda.h:45) for the contract of
+// src/contact/icollision_detector.h:19-47.  A view, not an owner: the handle (and its
+// contact buffers) belongs to the backend and exists from init() on, so calls before
+// init() throw.  detect() uploads host positions and runs the library's detection
+// (broad phase + narrow phase + contact conversion) on the handle; points() and
+// normals() return exactly max_slots() rows, the rows past contact_count() zero
+// (the GUI registers point clouds of max_slots() points, icollision_detector.h:36-44).
+class BVHB200 : public ICollisionDetector {
+public:
+    explicit BVHB200(ADMMBackendB200& backend) : backend_(backend) {}
+
+    void detect(const Matf_X3& pos) override {
+        int cnt = 0;
+        const int rc = admm_b200_detect_host(h(), pos.data(), pos.rows(), &cnt);
+        if (rc != ADMM_OK && rc != ADMM_ERR_CONTACT_OVERFLOW && rc != ADMM_ERR_STACK_OVERFLOW)
+            throw std::runtime_error(std::string("admm_b200_detect_host: ") + admm_b200_errstr(rc));
+    }
+    size_t contact_count() const override {
+        int c = 0;
+        check(admm_b200_contact_count(h(), &c), "admm_b200_contact_count");
+        return (size_t)c;
+    }
+    size_t max_slots() const override {
+        int c = 0;
+        check(admm_b200_max_slots(h(), &c), "admm_b200_max_slots");
+        return (size_t)c;
+    }
+    size_t peak_contact_count() const override {
+        int c = 0;
+        check(admm_b200_peak_contact_count(h(), &c), "admm_b200_peak_contact_count");
+        return (size_t)c;
+    }
+    std::vector<std::array<float, 3>> points() override { return rows(true); }
+    std::vector<std::array<float, 3>> normals() override { return rows(false); }
+    void clear() override { check(admm_b200_clear_contacts(h()), "admm_b200_clear_contacts"); }
+
+private:
+    ADMMBackendB200& backend_;
+
+    AdmmB200* h() const {
+        AdmmB200* p = backend_.impl()->handle();
+        if (!p) throw std::runtime_error("BVHB200: the backend has no handle before init()");
+        return p;
+    }
+    static void check(int rc, const char* what) {
+        if (rc != ADMM_OK) throw std::runtime_error(std::string(what) + ": " + admm_b200_errstr(rc));
+    }
+    std::vector<std::array<float, 3>> rows(bool pts) {
+        const size_t slots = max_slots();
+        std::vector<std::array<float, 3>> out(slots, std::array<float, 3>{0.f, 0.f, 0.f});
+        const size_t n = std::min(contact_count(), slots);
+        if (n == 0) return out;
+        std::vector<float> buf(3 * n);
+        int got = 0;
+        const int rc = pts ? admm_b200_contacts(h(), nullptr, nullptr, nullptr, buf.data(), nullptr, (int)n, &got)
+                           : admm_b200_contacts(h(), nullptr, nullptr, buf.data(), nullptr, nullptr, (int)n, &got);
+        if (rc != ADMM_OK && rc != ADMM_ERR_CONTACT_OVERFLOW) check(rc, "admm_b200_contacts");
+        for (size_t i = 0; i < n && i < (size_t)got; i++) out[i] = {buf[3 * i], buf[3 * i + 1], buf[3 * i + 2]};
+        return out;
+    }
 };
 
 }  // namespace ADU

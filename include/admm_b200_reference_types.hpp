@@ -12,3 +12,4 @@
 #include "constraint/pin_constraint.h"         // PinConstraint::pin_poistion
 #include "contact/contact_parameter.h"         // ContactParameter::get_thickness
 #include "contact/narrow_phase.h"              // ProximalQuery::mesh (surface sets), max_collision_num
+#include "contact/icollision_detector.h"       // ICollisionDetector (src/contact/icollision_detector.h:19-47)

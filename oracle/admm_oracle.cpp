@@ -26,6 +26,8 @@
 #endif
 
 #include "../include/admm_b200.h"
+#include <cstdio>
+
 #include "oracle_math.hpp"
 
 using namespace orc;
@@ -218,6 +220,120 @@ static void dcd_all(const float* x, const std::vector<int>& sv, const std::vecto
 }
 
 // ---------------------------------------------------------------------------
+// Exact solve of the CPU backend's damped system (SimplicialLLT of m_A_damp,
+// admm_impl_cpu.cpp:248-250, solved per column, linear_solver_cpu.h:16-23):
+// FP64 envelope (skyline) Cholesky A = L L^T after a reverse Cuthill-McKee
+// ordering of the symmetric pattern.  The envelope of row i spans its first
+// non-zero column to the diagonal; Cholesky creates no fill outside it.
+// ---------------------------------------------------------------------------
+struct EnvelopeCholesky {
+    int n = 0;
+    std::vector<int> perm, iperm;  // new -> old, old -> new
+    std::vector<int> first;        // first column of row i's envelope (new order)
+    std::vector<long> off;         // start of row i in L (entries first[i] .. i)
+    std::vector<double> L;
+
+    // Reverse Cuthill-McKee over every connected component, each started from a
+    // pseudo-peripheral vertex (two breadth-first passes from a vertex of least degree).
+    void order(const std::vector<int>& start, const std::vector<int>& col) {
+        std::vector<int> deg(n);
+        for (int i = 0; i < n; i++) deg[i] = start[i + 1] - start[i];
+        std::vector<char> seen(n, 0);
+        std::vector<int> out;
+        out.reserve(n);
+        auto bfs = [&](int root, std::vector<int>& lev, std::vector<char>& mark) {
+            lev.clear();
+            lev.push_back(root);
+            mark[root] = 1;
+            for (size_t h = 0; h < lev.size(); h++) {
+                const int u = lev[h];
+                std::vector<int> nb;
+                for (int a = start[u]; a < start[u + 1]; a++)
+                    if (!mark[col[a]]) { mark[col[a]] = 1; nb.push_back(col[a]); }
+                std::sort(nb.begin(), nb.end(), [&](int x, int y) { return deg[x] != deg[y] ? deg[x] < deg[y] : x < y; });
+                lev.insert(lev.end(), nb.begin(), nb.end());
+            }
+        };
+        std::vector<int> comp;
+        for (int s0 = 0; s0 < n; s0++) {
+            if (seen[s0]) continue;
+            std::vector<char> mark(seen);
+            bfs(s0, comp, mark);
+            int root = s0;
+            for (int v : comp) if (deg[v] < deg[root]) root = v;
+            mark = seen;
+            bfs(root, comp, mark);
+            root = comp.back();
+            mark = seen;
+            bfs(root, comp, mark);
+            for (int v : comp) seen[v] = 1;
+            out.insert(out.end(), comp.rbegin(), comp.rend());
+        }
+        perm = out;
+        iperm.assign(n, 0);
+        for (int i = 0; i < n; i++) iperm[perm[i]] = i;
+    }
+
+    // A: off-diagonal CSR (symmetric pattern) and diagonal.
+    bool factor(int nn, const std::vector<int>& start, const std::vector<int>& col, const std::vector<double>& val,
+                const std::vector<double>& diag) {
+        n = nn;
+        order(start, col);
+        first.assign(n, 0);
+        for (int i = 0; i < n; i++) {
+            int f = i;
+            const int o = perm[i];
+            for (int a = start[o]; a < start[o + 1]; a++) f = std::min(f, iperm[col[a]]);
+            first[i] = f;
+        }
+        off.assign(n + 1, 0);
+        for (int i = 0; i < n; i++) off[i + 1] = off[i] + (i - first[i] + 1);
+        L.assign(off[n], 0.0);
+        for (int i = 0; i < n; i++) {
+            const int o = perm[i];
+            L[off[i] + (i - first[i])] = diag[o];
+            for (int a = start[o]; a < start[o + 1]; a++) {
+                const int j = iperm[col[a]];
+                if (j < i) L[off[i] + (j - first[i])] += val[a];
+            }
+        }
+        for (int i = 0; i < n; i++) {
+            double* Li = &L[off[i]];
+            for (int j = first[i]; j < i; j++) {
+                const double* Lj = &L[off[j]];
+                const int k0 = std::max(first[i], first[j]);
+                double s = Li[j - first[i]];
+                for (int k = k0; k < j; k++) s -= Li[k - first[i]] * Lj[k - first[j]];
+                Li[j - first[i]] = s / Lj[j - first[j]];
+            }
+            double s = Li[i - first[i]];
+            for (int k = first[i]; k < i; k++) s -= Li[k - first[i]] * Li[k - first[i]];
+            if (!(s > 0.0)) return false;
+            Li[i - first[i]] = std::sqrt(s);
+        }
+        return true;
+    }
+
+    // x = A^-1 b for one column (original order).
+    void solve(const double* b, double* x) const {
+        std::vector<double> y(n);
+        for (int i = 0; i < n; i++) y[i] = b[perm[i]];
+        for (int i = 0; i < n; i++) {
+            const double* Li = &L[off[i]];
+            double s = y[i];
+            for (int k = first[i]; k < i; k++) s -= Li[k - first[i]] * y[k];
+            y[i] = s / Li[i - first[i]];
+        }
+        for (int i = n - 1; i >= 0; i--) {
+            const double* Li = &L[off[i]];
+            y[i] /= Li[i - first[i]];
+            for (int k = first[i]; k < i; k++) y[k] -= Li[k - first[i]] * y[i];
+        }
+        for (int i = 0; i < n; i++) x[perm[i]] = y[i];
+    }
+};
+
+// ---------------------------------------------------------------------------
 // The ADMM oracle.
 // ---------------------------------------------------------------------------
 template <class R>
@@ -245,6 +361,12 @@ struct Oracle {
     int chunk = 0;
     int global_solver = 0, pcg_iter = 0;
     std::vector<R> pblock;  // [9 nd] learned 3x3 preconditioner blocks (global_solver 2)
+    // semantics of the reference's CPU backend (backend_semantics 1)
+    int backend = 0;
+    double damp_k_L = 0.0, damp_k_M = 0.0;
+    Csr Damp;                    // off-diagonal part of the damping matrix (added to A too)
+    std::vector<double> Ddiag;   // its diagonal
+    EnvelopeCholesky chol;       // exact factor of the damped A
     // learned global step (global_solver 3): sweeps, coefficients, per-vertex m and theta
     int learn_K = 0;
     std::vector<R> learn_omega, learn_beta, learn_m, learn_theta, xl;
@@ -303,6 +425,10 @@ struct Oracle {
         for (int s : surf_verts) is_surf[s] = 1;
         dt = d->dt; g = d->g; mu = d->mu; kappa = d->kappa; beta = d->beta; thickness = d->thickness;
         semantics = d->contact_semantics;
+        backend = d->backend_semantics;
+        if (backend == 1) semantics = 1;
+        damp_k_L = d->damp_k_L;
+        damp_k_M = d->damp_k_M;
         if (d->vert_mu) vmu.assign(d->vert_mu, d->vert_mu + d->n_vert);
         admm_max_iter = d->admm_max_iter; dcd_interval = std::max(1, d->dcd_interval);
         gs_max_iter = d->gs_max_iter; jacobi_iter = d->jacobi_iter;
@@ -381,6 +507,36 @@ struct Oracle {
                 for (int bb = D.start[r]; bb < D.start[r + 1]; bb++) arow[i][D.col[bb]] += w2 * D.val[a] * D.val[bb];
             }
         }
+        // the CPU backend's damping (admm_impl_cpu.cpp:181-191, 221): Damp = dt (damp_k_L
+        // Dd^T Wd Dd + damp_k_M M) over the triangle, tet and bending rows, Wd = diag(w);
+        // A_damp = A + Damp
+        if (backend == 1) {
+            std::vector<std::unordered_map<int, double>> drow(nd);
+            auto damped = [&](int r) {
+                return (ntri && r >= tri_sr && r < tri_sr + 2 * ntri) || (ntet && r >= tet_sr && r < tet_sr + 3 * ntet) ||
+                       (nbend && r >= bend_sr && r < bend_sr + nbend);
+            };
+            for (int r = 0; r < m; r++) {
+                if (!damped(r)) continue;
+                const double sw = (double)dt * damp_k_L * (double)wrow[r];
+                for (int a = D.start[r]; a < D.start[r + 1]; a++)
+                    for (int bb = D.start[r]; bb < D.start[r + 1]; bb++) drow[D.col[a]][D.col[bb]] += sw * D.val[a] * D.val[bb];
+            }
+            for (int i = 0; i < nd; i++) drow[i][i] += (double)dt * damp_k_M * (double)mass[i];
+            Ddiag.assign(nd, 0.0);
+            Damp.start.assign(nd + 1, 0);
+            Damp.col.clear(); Damp.val.clear();
+            for (int i = 0; i < nd; i++) {
+                std::vector<std::pair<int, double>> e(drow[i].begin(), drow[i].end());
+                std::sort(e.begin(), e.end());
+                for (auto& kv : e) {
+                    arow[i][kv.first] += kv.second;
+                    if (kv.first == i) Ddiag[i] = kv.second;
+                    else { Damp.col.push_back(kv.first); Damp.val.push_back(kv.second); }
+                }
+                Damp.start[i + 1] = (int)Damp.col.size();
+            }
+        }
         dt2Wc.assign(nd, R(0));
         if (contact)
             for (int i = 0; i < nd; i++)
@@ -398,6 +554,11 @@ struct Oracle {
             }
             Adiag[i] = (R)diag;
             A.start[i + 1] = (int)A.col.size();
+        }
+        if (backend == 1) {
+            std::vector<double> ad(nd);
+            for (int i = 0; i < nd; i++) ad[i] = (double)Adiag[i];
+            if (!chol.factor(nd, A.start, A.col, A.val, ad)) fprintf(stderr, "oracle: damped A is not positive definite\n");
         }
         DtW2.start.assign(nd + 1, 0);
         DtW2.col.clear(); DtW2.val.clear();
@@ -436,6 +597,15 @@ struct Oracle {
             }
             for (int k = 0; k < 3; k++) mxt[3 * i + k] = mass[i] * x[3 * i + k];
         }
+        // the CPU backend's b_ini = Damp x0 (admm_impl_cpu.cpp:295), part of every
+        // right-hand side (:344): folded into M x~
+        if (backend == 1)
+            for (int i = 0; i < nd; i++)
+                for (int k = 0; k < 3; k++) {
+                    double a = Ddiag[i] * (double)x0[3 * i + k];
+                    for (int e = Damp.start[i]; e < Damp.start[i + 1]; e++) a += Damp.val[e] * (double)x0[3 * Damp.col[e] + k];
+                    mxt[3 * i + k] += (R)a;
+                }
     }
 
     // D*x for rows [r0, r0+nr): tri/tet through F = E * Binv (edges first),
@@ -532,9 +702,15 @@ struct Oracle {
         for (int c = 0; c < nc; c++) {
             const Contact& ct = cts[c];
             R t[4];
-            for (int k = 0; k < 4; k++) t[k] = (R)ct.bary[k] * (R)ct.bary[k] * cwinv[ct.v[k]] * (R)cnt[ct.v[k]];
+            // the CPU backend (compute_Scc, admm_impl_cpu.cpp:361-380): no per-vertex
+            // counts, Gamma of static vertices (w_c > 1e7) zero
+            for (int k = 0; k < 4; k++)
+                t[k] = (R)ct.bary[k] * (R)ct.bary[k] * cwinv[ct.v[k]] * (backend == 1 ? R(1) : (R)cnt[ct.v[k]]);
             const R Sc = eps + (((t[0] + t[1]) + t[2]) + t[3]);
-            for (int k = 0; k < 4; k++) Gam[4 * c + k] = (R)ct.bary[k] / (Sc * cw[ct.v[k]]);
+            for (int k = 0; k < 4; k++) {
+                Gam[4 * c + k] = (R)ct.bary[k] / (Sc * cw[ct.v[k]]);
+                if (backend == 1 && cw[ct.v[k]] > R(1e7)) Gam[4 * c + k] = 0;
+            }
             for (int k = 0; k < 3; k++) Kc[3 * c + k] = (R(1) / dt) * (R)ct.gap * (R)ct.normal[k] * gam;
         }
         vstart.assign(n + 1, 0);
@@ -561,6 +737,10 @@ struct Oracle {
                 int vi = cts[c].v[k];
                 if (vi < nd) for (int a = 0; a < 3; a++) p[3 * vi + a] += Gam[4 * c + k] * rc[3 * c + a];
             }
+        if (backend == 1) {
+            project_gs_serial(nc);
+            return;
+        }
         for (int it = 0; it < gs_max_iter; it++) {
             for (int c = 0; c < nc; c++) {
                 const Contact& ct = cts[c];
@@ -631,6 +811,52 @@ struct Oracle {
         }
     }
 
+    // The CPU backend's projection after the warm start: gs_max_iter serial
+    // Gauss-Seidel sweeps in contact-list order, each contact's update scattered into
+    // p at once (_project_feasible_plain / _project_one_contact, admm_impl_cpu.cpp:390-448).
+    void project_gs_serial(int nc) {
+        for (int it = 0; it < gs_max_iter; it++)
+            for (int c = 0; c < nc; c++) {
+                const Contact& ct = cts[c];
+                R u[3];
+                for (int a = 0; a < 3; a++)
+                    u[a] = (((R)ct.bary[0] * p[3 * ct.v[0] + a] + (R)ct.bary[1] * p[3 * ct.v[1] + a]) +
+                            (R)ct.bary[2] * p[3 * ct.v[2] + a]) + (R)ct.bary[3] * p[3 * ct.v[3] + a] + Kc[3 * c + a];
+                R nrm[3] = {(R)ct.normal[0], (R)ct.normal[1], (R)ct.normal[2]};
+                R us[3];
+                for (int a = 0; a < 3; a++) us[a] = u[a] - rc[3 * c + a];
+                R uN = (nrm[0] * us[0] + nrm[1] * us[1]) + nrm[2] * us[2];
+                R uT[3];
+                for (int a = 0; a < 3; a++) uT[a] = us[a] - uN * nrm[a];
+                if (uN < 0) {
+                    R tau = std::sqrt((uT[0] * uT[0] + uT[1] * uT[1]) + uT[2] * uT[2]);
+                    R alpha = -cmu[c] * uN;
+                    uN = 0;
+                    if (tau <= alpha) uT[0] = uT[1] = uT[2] = 0;
+                    else { R s = R(1) - alpha / tau; for (int a = 0; a < 3; a++) uT[a] = s * uT[a]; }
+                }
+                R d[3];
+                for (int a = 0; a < 3; a++) {
+                    d[a] = (uN * nrm[a] + uT[a]) - u[a];
+                    rc[3 * c + a] = rc[3 * c + a] + d[a];
+                }
+                for (int k = 0; k < 4; k++) {
+                    const int vi = ct.v[k];
+                    if (vi < nd) for (int a = 0; a < 3; a++) p[3 * vi + a] += Gam[4 * c + k] * d[a];
+                }
+            }
+    }
+
+    // The CPU backend's exact global solve of the damped A, column by column.
+    void exact_solve() {
+        std::vector<double> bc(nd), xc(nd);
+        for (int k = 0; k < 3; k++) {
+            for (int i = 0; i < nd; i++) bc[i] = (double)b[3 * i + k];
+            chol.solve(bc.data(), xc.data());
+            for (int i = 0; i < nd; i++) x[3 * i + k] = (R)xc[i];
+        }
+    }
+
     // Global step with preconditioned CG (global_solver > 0; no reference
     // counterpart): Chronopoulos-Gear PCG on A (x) I3 over the 3 nd unknowns,
     // warm-started from x, `iters` updates, the same recurrences as the GPU
@@ -691,14 +917,15 @@ struct Oracle {
     }
 
     void global_solve() {
-        if (global_solver > 0) pcg(pcg_iter);
+        if (backend == 1) exact_solve();
+        else if (global_solver > 0) pcg(pcg_iter);
         else jacobi(jacobi_iter);
     }
 
     // Learned global step (the GPU's k_rhs_learn / k_lsweep / k_ljudge / k_ldecide):
     // warm start x += theta (x - xl) unless first, xl <- x received; K sweeps
     // x_{k+1} = x_k + omega_k m (b - A x_k) + beta_k (x_k - x_{k-1}); the solve fails
-    // when |b - A x_K|^2 > |b - A x_0|^2 (FP64 sums).
+    // when |b - A x_K|^2 > |b - A x_0|^2 and |b - A x_K| > 1e-5 |b| (FP64 sums).
     void learned_solve(bool first) {
         const int N = 3 * nd;
         if (learn_K == 0) {  // defaults: the Jacobi sweep
@@ -717,7 +944,8 @@ struct Oracle {
                 if (!first) x[3 * i + k] = learn_theta[i] * (xi - xo) + xi;
             }
         std::vector<R> xp(x.begin(), x.begin() + N), xn(N), ax(N);
-        double r0 = 0, rK = 0;
+        double r0 = 0, rK = 0, bb = 0;
+        for (int q = 0; q < N; q++) bb += (double)b[q] * (double)b[q];
         for (int s = 0; s < learn_K; s++) {
             apply_A(x, ax);
             for (int i = 0; i < nd; i++)
@@ -739,7 +967,7 @@ struct Oracle {
             rK += (double)r * (double)r;
         }
         learn_solves++;
-        if (!(rK <= r0)) {
+        if (!(rK <= r0 || rK <= 1e-10 * bb)) {
             learn_fail++;
             learn_failed++;
         }
@@ -994,6 +1222,69 @@ void orc_set_learned(void* hp, int K, const float* om, const float* be, const fl
     if (h->d) set_learned_impl(h->d, K, om, be, m, th);
     else set_learned_impl(h->f, K, om, be, m, th);
 }
+// Rest-shape records computed by the oracle itself from the mesh (FP64 from the float
+// positions), independent of the scene builder that feeds both the oracle and the GPU:
+// triangles (TriangleConstraint ctor, triangle_constraint.h:41-58): orthonormal basis
+// n1 = e12/|e12|, n2 = normalised e13 - (e13.n1) n1, Binv = (basis^T [e12 e13])^-1
+// (row-major 2x2), area = det / 2;  tets (tetrahedral_constraint.h:41-51): Binv =
+// [e12 e13 e14]^-1 (row-major 3x3), volume = |det| / 6;  lumped mass
+// (MeshData::get_mass, mesh_container.h:452-472): area/3 and volume/4 times the density.
+void orc_tri_rest(const float* v, const int32_t* tri, int ntri, double* binv4, double* area) {
+    for (int c = 0; c < ntri; c++) {
+        const int* id = &tri[3 * c];
+        double e12[3], e13[3];
+        for (int k = 0; k < 3; k++) {
+            e12[k] = (double)v[3 * id[1] + k] - (double)v[3 * id[0] + k];
+            e13[k] = (double)v[3 * id[2] + k] - (double)v[3 * id[0] + k];
+        }
+        const double l1 = std::sqrt(e12[0] * e12[0] + e12[1] * e12[1] + e12[2] * e12[2]);
+        double n1[3] = {e12[0] / l1, e12[1] / l1, e12[2] / l1};
+        const double d = e13[0] * n1[0] + e13[1] * n1[1] + e13[2] * n1[2];
+        double n2[3] = {e13[0] - d * n1[0], e13[1] - d * n1[1], e13[2] - d * n1[2]};
+        const double l2 = std::sqrt(n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2]);
+        for (int k = 0; k < 3; k++) n2[k] /= l2;
+        auto dot3 = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+        const double M[2][2] = {{dot3(n1, e12), dot3(n1, e13)}, {dot3(n2, e12), dot3(n2, e13)}};
+        const double det = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+        binv4[4 * c + 0] = M[1][1] / det;
+        binv4[4 * c + 1] = -M[0][1] / det;
+        binv4[4 * c + 2] = -M[1][0] / det;
+        binv4[4 * c + 3] = M[0][0] / det;
+        area[c] = det / 2.0;
+    }
+}
+
+void orc_tet_rest(const float* v, const int32_t* tet, int ntet, double* binv9, double* vol) {
+    for (int c = 0; c < ntet; c++) {
+        const int* id = &tet[4 * c];
+        double B[3][3];  // columns e12, e13, e14
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < 3; k++) B[k][j] = (double)v[3 * id[j + 1] + k] - (double)v[3 * id[0] + k];
+        const double c00 = B[1][1] * B[2][2] - B[1][2] * B[2][1], c01 = B[1][2] * B[2][0] - B[1][0] * B[2][2],
+                     c02 = B[1][0] * B[2][1] - B[1][1] * B[2][0];
+        const double det = B[0][0] * c00 + B[0][1] * c01 + B[0][2] * c02;
+        const double inv[3][3] = {
+            {c00 / det, (B[0][2] * B[2][1] - B[0][1] * B[2][2]) / det, (B[0][1] * B[1][2] - B[0][2] * B[1][1]) / det},
+            {c01 / det, (B[0][0] * B[2][2] - B[0][2] * B[2][0]) / det, (B[0][2] * B[1][0] - B[0][0] * B[1][2]) / det},
+            {c02 / det, (B[0][1] * B[2][0] - B[0][0] * B[2][1]) / det, (B[0][0] * B[1][1] - B[0][1] * B[1][0]) / det}};
+        for (int r = 0; r < 3; r++)
+            for (int k = 0; k < 3; k++) binv9[9 * c + 3 * r + k] = inv[r][k];
+        vol[c] = std::fabs(det / 6.0);
+    }
+}
+
+void orc_lumped_mass(int n, const float* v, const int32_t* tri, int ntri, const double* tri_density,
+                     const int32_t* tet, int ntet, const double* tet_density, double* mass) {
+    std::vector<double> a(ntri), b4(4 * (size_t)ntri), vo(ntet), b9(9 * (size_t)ntet);
+    if (ntri) orc_tri_rest(v, tri, ntri, b4.data(), a.data());
+    if (ntet) orc_tet_rest(v, tet, ntet, b9.data(), vo.data());
+    for (int i = 0; i < n; i++) mass[i] = 0.0;
+    for (int f = 0; f < ntri; f++)
+        for (int k = 0; k < 3; k++) mass[tri[3 * f + k]] += a[f] / 3.0 * tri_density[f];
+    for (int t = 0; t < ntet; t++)
+        for (int k = 0; k < 4; k++) mass[tet[4 * t + k]] += vo[t] / 4.0 * tet_density[t];
+}
+
 void orc_learned_stats(void* hp, long long* out4) {
     auto* h = static_cast<Handle*>(hp);
     if (h->d) {

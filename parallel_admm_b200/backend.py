@@ -21,7 +21,7 @@ from .scene import Scene
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libadmm_b200.so")
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 OK = 0
 ERR_INVALID = -1
 ERR_CUDA = -2
@@ -74,7 +74,8 @@ class AdmmB200Desc(ctypes.Structure):
         ("bvh_refit", ctypes.c_int32), ("ell_lanes", ctypes.c_int32), ("jacobi_mode", ctypes.c_int32),
         ("broad_phase", ctypes.c_int32), ("global_solver", ctypes.c_int32), ("pcg_iter", ctypes.c_int32),
         ("vert_mu", ctypes.POINTER(ctypes.c_float)), ("query_lanes", ctypes.c_int32),
-        ("contact_semantics", ctypes.c_int32),
+        ("contact_semantics", ctypes.c_int32), ("backend_semantics", ctypes.c_int32),
+        ("damp_k_L", ctypes.c_float), ("damp_k_M", ctypes.c_float),
     ]
 
 
@@ -143,6 +144,9 @@ class DescHolder:
         d.pcg_iter = int(p.pcg_iter)
         d.query_lanes = int(getattr(p, "query_lanes", 0))
         d.contact_semantics = int(getattr(p, "contact_semantics", 0))
+        d.backend_semantics = int(getattr(p, "backend_semantics", 0))
+        d.damp_k_L = float(getattr(p, "damp_k_L", 1e-4))
+        d.damp_k_M = float(getattr(p, "damp_k_M", 0.0))
         vm = getattr(sc, "vert_mu", None)
         d.vert_mu = arr("vm", vm, np.float32) if vm is not None else None
         for k, v in overrides.items():

@@ -407,6 +407,10 @@ int enqueue_contact(AdmmB200* h, bool dual) {
     else LAUNCH(k_contact_p<false>, split + h->group_grid, kVertThreads, s, split);
     const int G = h->gs_iter;
     if (G <= 0) return ADMM_OK;
+    if (s.cpu_backend) {
+        LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_gs_serial, 1, 32, s, G);
+        return ADMM_OK;
+    }
     // pass 1 projects from s.p into s.du; pass g = 2..G rebuilds p of pass g-1
     // (P[g-1]) from P[g-2] and D[g-1] and projects into D[g]; the last gather
     // writes P[G] into s.p.  P[j] = s.p for even j, s.p2 for odd j; D[j] = s.du
@@ -976,6 +980,7 @@ void enqueue_step_begin(AdmmB200* h) {
         LAUNCH(k_animate, blocks(h->anim.n_verts, kVertThreads), kVertThreads, s, h->anim);
     }
     LAUNCH(k_pre_integration, blocks(s.n, kVertThreads), kVertThreads, s);
+    if (s.cpu_backend) LAUNCH(k_damp_binit, blocks(s.nd, kVertThreads), kVertThreads, s);
     if (!h->warmstart_ue) cudaMemsetAsync(s.ue, 0, sizeof(float4) * s.m, h->cstream);
     if (!h->warmstart_uc) cudaMemsetAsync(s.uc, 0, sizeof(float4) * s.nd, h->cstream);
 }
@@ -1131,6 +1136,7 @@ int build_plain_graph(AdmmB200* h) {
     if (h->plain_exec) return ADMM_OK;
     cudaGraphExec_t keep = h->step_exec;
     const int kps = h->kernels_per_step, kb = h->kernels_body, probe = h->probe_kernel;
+    const int pu = h->probe_used, pvu = h->pev_used, ph = h->phase;
     h->step_exec = nullptr;
     h->force_plain = true;
     h->probe_kernel = 0;
@@ -1141,6 +1147,9 @@ int build_plain_graph(AdmmB200* h) {
     h->probe_kernel = probe;
     h->kernels_per_step = kps;
     h->kernels_body = kb;
+    h->probe_used = pu;
+    h->pev_used = pvu;
+    h->phase = ph;
     return rc;
 }
 
@@ -1350,6 +1359,9 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     if (d->query_lanes != 0 && d->query_lanes != 8 && d->query_lanes != 16 && d->query_lanes != 32)
         return fail(h, ADMM_ERR_INVALID, "query_lanes");
     if (d->contact_semantics != 0 && d->contact_semantics != 1) return fail(h, ADMM_ERR_INVALID, "contact_semantics");
+    if (d->backend_semantics != 0 && d->backend_semantics != 1) return fail(h, ADMM_ERR_INVALID, "backend_semantics");
+    if (d->backend_semantics == 1 && !(d->damp_k_L >= 0.f && d->damp_k_M >= 0.f))
+        return fail(h, ADMM_ERR_INVALID, "damp_k_L/damp_k_M");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
         return fail(h, ADMM_ERR_NO_DEVICE, "no CUDA device");
@@ -1546,8 +1558,24 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     const int hist_n = 256 * sort_tiles(std::max(h->sort_max, 1));
     TRY(dalloc(h, &h->hist, hist_n));
     if (d->broad_phase < 0 || d->broad_phase > 2) return fail(h, ADMM_ERR_INVALID, "broad_phase must be 0, 1 or 2");
-    s.cpu_contact = d->contact_semantics == 1 ? 1 : 0;
+    s.cpu_backend = d->backend_semantics == 1 ? 1 : 0;
+    s.cpu_contact = (d->contact_semantics == 1 || s.cpu_backend) ? 1 : 0;
     h->use_grid = d->broad_phase != 1 || s.cpu_contact;  // the CPU predicates run on the grid
+    if (s.cpu_backend) {
+        int* ds = nullptr;
+        int* dc = nullptr;
+        float* dv = nullptr;
+        float* dd = nullptr;
+        std::vector<float> vals(as.damp.val.begin(), as.damp.val.end());
+        TRY(dupload(h, &ds, as.damp.start.data(), as.damp.start.size()));
+        TRY(dupload(h, &dc, as.damp.col.empty() ? nullptr : as.damp.col.data(), std::max<size_t>(as.damp.col.size(), 1)));
+        TRY(dupload(h, &dv, vals.empty() ? nullptr : vals.data(), std::max<size_t>(vals.size(), 1)));
+        TRY(dupload(h, &dd, as.damp_diag.data(), as.damp_diag.size()));
+        s.dmp_start = ds;
+        s.dmp_col = dc;
+        s.dmp_val = dv;
+        s.dmp_diag = dd;
+    }
 
     TRY(setup_grid(h, d));
     const int scan_n = std::max(std::max(std::max(scan_tiles(hist_n), scan_tiles(n + 1)), scan_tiles(s.nsv + s.nse + 1)),
@@ -1624,7 +1652,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         L.minv = minv;
         L.theta = theta;
         TRY(dalloc(h, &L.xl, nd));
-        TRY(dalloc(h, &L.part, 2 * (size_t)L.blocks));
+        TRY(dalloc(h, &L.part, 3 * (size_t)L.blocks));
         TRY(dalloc(h, &L.stats, 4));
         TRY(dalloc(h, &L.fail, 1));
         h->learn_sweeps = std::max(1, h->jac_iter);
@@ -1842,6 +1870,7 @@ int admm_b200_step_async(AdmmB200* h, int n_steps) {
         return ADMM_OK;
     }
     TRY(build_step_graph(h));
+    if (learned_active(h)) TRY(build_plain_graph(h));
     CK(cudaEventRecord(h->ev0, h->stream));
     for (int k = 0; k < n_steps; k++) TRY(launch_substep(h));
     CK(cudaEventRecord(h->ev1, h->stream));
@@ -2209,6 +2238,7 @@ int admm_b200_step_host(AdmmB200* h, const float* x_in, const float* v_in, float
     CK(cudaSetDevice(h->device));
     if (!h->stage) TRY(dalloc(h, &h->stage, (size_t)6 * n));
     TRY(build_step_graph(h));
+    if (learned_active(h)) TRY(build_plain_graph(h));
     const size_t bytes = sizeof(float) * 3 * (size_t)n;
     CK(cudaMemcpyAsync(h->stage, x_in, bytes, cudaMemcpyHostToDevice, h->stream));
     if (v_in) CK(cudaMemcpyAsync(h->stage + 3 * (size_t)n, v_in, bytes, cudaMemcpyHostToDevice, h->stream));

@@ -107,12 +107,21 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_scc(DevScene s) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         const int4 q = s.pairs[c];
         const float4 b = s.bary[c];
-        const float sc = s.eps + (b.x * b.x * s.cwinv[q.x] * (float)s.vcnt[q.x] +
-                                  b.y * b.y * s.cwinv[q.y] * (float)s.vcnt[q.y] +
-                                  b.z * b.z * s.cwinv[q.z] * (float)s.vcnt[q.z] +
-                                  b.w * b.w * s.cwinv[q.w] * (float)s.vcnt[q.w]);
-        s.gamma[c] = make_float4(b.x / (sc * s.cw[q.x]), b.y / (sc * s.cw[q.y]), b.z / (sc * s.cw[q.z]),
-                                 b.w / (sc * s.cw[q.w]));
+        // the CPU backend (compute_Scc, admm_impl_cpu.cpp:361-380) leaves out the
+        // per-vertex contact counts and sets Gamma of static vertices to zero
+        const float c0 = s.cpu_backend ? 1.f : (float)s.vcnt[q.x], c1 = s.cpu_backend ? 1.f : (float)s.vcnt[q.y];
+        const float c2 = s.cpu_backend ? 1.f : (float)s.vcnt[q.z], c3 = s.cpu_backend ? 1.f : (float)s.vcnt[q.w];
+        const float sc = s.eps + (b.x * b.x * s.cwinv[q.x] * c0 + b.y * b.y * s.cwinv[q.y] * c1 +
+                                  b.z * b.z * s.cwinv[q.z] * c2 + b.w * b.w * s.cwinv[q.w] * c3);
+        float4 gm = make_float4(b.x / (sc * s.cw[q.x]), b.y / (sc * s.cw[q.y]), b.z / (sc * s.cw[q.z]),
+                                b.w / (sc * s.cw[q.w]));
+        if (s.cpu_backend) {
+            if (s.cw[q.x] > 1e7f) gm.x = 0.f;
+            if (s.cw[q.y] > 1e7f) gm.y = 0.f;
+            if (s.cw[q.z] > 1e7f) gm.z = 0.f;
+            if (s.cw[q.w] > 1e7f) gm.w = 0.f;
+        }
+        s.gamma[c] = gm;
         const float4 nr = s.nrm[c];
         const float k = s.dt_inv * nr.w;
         s.kc[c] = f4(k * nr.x * s.gam, k * nr.y * s.gam, k * nr.z * s.gam);
@@ -408,6 +417,36 @@ __global__ void __launch_bounds__(kContactThreads) k_contact_pass(DevScene s, co
     if (w0 < nc) pass_contact(s, w0, P0, lane, sub, gmask, p_old, p_new, du_old, du_new);
     for (int c = w0 + ws; c < nc; c += ws)  // uniform per warp
         pass_contact(s, c, pass_rec(s, c, grp, sub), lane, sub, gmask, p_old, p_new, du_old, du_new);
+}
+
+// The CPU backend's contact projection after the warm start: `passes` serial
+// Gauss-Seidel sweeps over the contact list in its order, each contact projected
+// from the current p and its update scattered into p at once
+// (_project_feasible_plain / _project_one_contact, admm_impl_cpu.cpp:390-448).
+// One thread: the order is the algorithm.
+__global__ void k_contact_gs_serial(DevScene s, int passes) {
+    ADMM_PDL_PROLOGUE();
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nc = *s.nc;
+    for (int it = 0; it < passes; it++)
+        for (int c = 0; c < nc; c++) {
+            const int4 q = s.pairs[c];
+            const float4 b = s.bary[c], kc = s.kc[c], g = s.gamma[c], r = s.rc[c];
+            float ux, uy, uz;
+            contact_u_bk(b, kc, s.p[q.x], s.p[q.y], s.p[q.z], s.p[q.w], ux, uy, uz);
+            const float4 d = cone_du(s.nrm[c], s.cmu[c], ux, uy, uz, r);
+            s.rc[c] = f4(r.x + d.x, r.y + d.y, r.z + d.z);
+            const int v[4] = {q.x, q.y, q.z, q.w};
+            const float gg[4] = {g.x, g.y, g.z, g.w};
+            for (int k = 0; k < 4; k++) {
+                if (v[k] >= s.nd) continue;
+                float4 pv = s.p[v[k]];
+                pv.x = fmaf(gg[k], d.x, pv.x);
+                pv.y = fmaf(gg[k], d.y, pv.y);
+                pv.z = fmaf(gg[k], d.z, pv.z);
+                s.p[v[k]] = pv;
+            }
+        }
 }
 
 }  // namespace admm

@@ -719,6 +719,29 @@ __global__ void __launch_bounds__(kVertThreads) k_pcg_update(DevScene s, PcgDev 
     g.u[i] = pcg_precond(s, g, i, r);
 }
 
+// The CPU backend's b_ini = Damp x0 (admm_impl_cpu.cpp:295), added to every
+// right-hand side (:344): folded into M x~, which every right-hand side starts from.
+__global__ void __launch_bounds__(kVertThreads) k_damp_binit(DevScene s) {
+    ADMM_PDL_PROLOGUE();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.nd) return;
+    const float4 xi = s.x0[i];
+    const float d = s.dmp_diag[i];
+    float ax = d * xi.x, ay = d * xi.y, az = d * xi.z;
+    for (int k = s.dmp_start[i]; k < s.dmp_start[i + 1]; k++) {
+        const float4 xj = s.x0[s.dmp_col[k]];
+        const float a = s.dmp_val[k];
+        ax = fmaf(a, xj.x, ax);
+        ay = fmaf(a, xj.y, ay);
+        az = fmaf(a, xj.z, az);
+    }
+    float4 m = s.mxt[i];
+    m.x += ax;
+    m.y += ay;
+    m.z += az;
+    s.mxt[i] = m;
+}
+
 __global__ void k_copy_dyn(DevScene s, const float4* __restrict__ src, float4* __restrict__ dst) {
     ADMM_PDL_PROLOGUE();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

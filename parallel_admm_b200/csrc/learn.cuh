@@ -13,9 +13,10 @@
 // are trained with it.  omega = 1, beta = 0, theta = 0 and m = 1 / a_ii is the
 // Jacobi sweep itself.
 //
-// The judge: the first sweep sums |b - A x_0|^2 and a last pass (k_ljudge) sums
-// |b - A x_K|^2 while it moves x_K into x; k_ldecide counts the solve as failed
-// when the residual did not drop.  A substep with a failed solve is run again
+// The judge: the first sweep sums |b - A x_0|^2 and |b|^2, a last pass (k_ljudge)
+// sums |b - A x_K|^2 while it moves x_K into x; k_ldecide counts the solve as failed
+// when the residual did not drop and is above 1e-5 |b| (below that it is FP32
+// rounding noise of b - A x, where the comparison decides nothing).  A substep with a failed solve is run again
 // from its starting state with the plain Jacobi global step (host side).
 #pragma once
 #include "kernels.cuh"
@@ -28,7 +29,7 @@ struct LearnDev {
     const float* minv = nullptr;   // [nd] m_i
     const float* theta = nullptr;  // [nd] warm-start coefficient
     float4* xl = nullptr;          // [nd] x received by the previous global step
-    double* part = nullptr;        // [2 x blocks] block partials of |r_0|^2 and |r_K|^2
+    double* part = nullptr;        // [3 x blocks] block partials of |r_0|^2, |r_K|^2 and |b|^2
     int blocks = 0;                // grid of the sweeps and the judge
     unsigned long long* stats = nullptr;  // [4] solves judged, solves failed (device counters)
     int* fail = nullptr;           // [1] failed solves in the current substep
@@ -62,7 +63,8 @@ __global__ void __launch_bounds__(kVertThreads) k_rhs_learn(DevScene s, LearnDev
 }
 
 // One learned sweep k: dst = src + omega m (b - A src) + beta (src - prev); the first
-// sweep (FIRST) also writes the block partials of |b - A src|^2 into L.part[0..).
+// sweep (FIRST) also writes the block partials of |b - A src|^2 into L.part[0..) and
+// of |b|^2 into L.part[2 blocks..).
 template <int T, bool FIRST>
 __global__ void __launch_bounds__(kVertThreads) k_lsweep(DevScene s, LearnDev L, const float4* __restrict__ src,
                                                          const float4* __restrict__ prev, float4* __restrict__ dst,
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(kVertThreads) k_lsweep(DevScene s, LearnDev L,
     __shared__ double sh[kVertThreads / 32];
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    double rr = 0.0;
+    double rr = 0.0, bb = 0.0;
     if (w < s.A.nslices) {
         EllRowPf<T> r;
         r.load(s.A, w, lane);
@@ -90,14 +92,21 @@ __global__ void __launch_bounds__(kVertThreads) k_lsweep(DevScene s, LearnDev L,
             const float ox = omega * mi, bx = beta;
             dst[i] = f4(fmaf(ox, rx, fmaf(bx, xi.x - xp.x, xi.x)), fmaf(ox, ry, fmaf(bx, xi.y - xp.y, xi.y)),
                         fmaf(ox, rz, fmaf(bx, xi.z - xp.z, xi.z)));
-            if (FIRST) rr = (double)rx * rx + (double)ry * ry + (double)rz * rz;
+            if (FIRST) {
+                rr = (double)rx * rx + (double)ry * ry + (double)rz * rz;
+                bb = (double)bi.x * bi.x + (double)bi.y * bi.y + (double)bi.z * bi.z;
+            }
         }
     } else {
         ADMM_PDL_WAIT();
     }
     if (FIRST) {
         rr = block_sum(rr, sh);
-        if (threadIdx.x == 0) L.part[blockIdx.x] = rr;
+        bb = block_sum(bb, sh);
+        if (threadIdx.x == 0) {
+            L.part[blockIdx.x] = rr;
+            L.part[2 * L.blocks + blockIdx.x] = bb;
+        }
     }
 }
 
@@ -133,20 +142,23 @@ __global__ void __launch_bounds__(kVertThreads) k_ljudge(DevScene s, LearnDev L,
     if (threadIdx.x == 0) L.part[L.blocks + blockIdx.x] = rr;
 }
 
-// One block: both residuals summed in a fixed order; a solve whose residual did
-// not drop counts as failed.
+// One block: the partials summed in a fixed order; a solve whose residual did not
+// drop and is above kJudgeFloor |b| counts as failed.
+constexpr double kJudgeFloor = 1e-5;
 __global__ void __launch_bounds__(256) k_ldecide(LearnDev L) {
     ADMM_PDL_PROLOGUE();
     __shared__ double sh[8];
-    double a = 0.0, b = 0.0;
+    double a = 0.0, b = 0.0, c = 0.0;
     for (int k = threadIdx.x; k < L.blocks; k += blockDim.x) {
         a += L.part[k];
         b += L.part[L.blocks + k];
+        c += L.part[2 * L.blocks + k];
     }
     a = block_sum(a, sh);
     b = block_sum(b, sh);
+    c = block_sum(c, sh);
     if (threadIdx.x == 0) {
-        const bool failed = !(b <= a) || !(b == b);
+        const bool failed = !(b <= a || b <= kJudgeFloor * kJudgeFloor * c);
         L.stats[0] += 1ull;
         if (failed) {
             L.stats[1] += 1ull;

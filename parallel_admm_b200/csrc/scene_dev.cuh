@@ -86,6 +86,12 @@ struct DevScene {
     float dt = 0, dt_inv = 0, g = 0, mu = 0, eps = 0, gam = 0, thickness = 0;
     int contact = 0;
     int cpu_contact = 0;  // contact predicates of the CPU backend (ProximalQuery)
+    int cpu_backend = 0;  // solver semantics of the CPU backend (damping, S_c, serial Gauss-Seidel)
+    // CPU backend's damping matrix (off-diagonal CSR + diagonal) for b_ini = Damp x0
+    const int* dmp_start = nullptr;
+    const int* dmp_col = nullptr;
+    const float* dmp_val = nullptr;
+    const float* dmp_diag = nullptr;
     // vertex state (float4 rows, w unused)
     float4 *x = nullptr, *x0 = nullptr, *v = nullptr, *p = nullptr, *mxt = nullptr;
     float4 *b = nullptr, *uc = nullptr, *xprev = nullptr, *jac[2] = {nullptr, nullptr};

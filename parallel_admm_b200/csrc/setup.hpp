@@ -231,6 +231,10 @@ struct Assembly {
     std::vector<float> wrow;        // [m]
     std::vector<float> dt2wc;       // [nd]
     int64_t nnz_D = 0;
+    // backend_semantics 1: the CPU backend's damping matrix (added to A as well),
+    // off-diagonal CSR and diagonal, for b_ini = Damp x0
+    HostCsr damp;
+    std::vector<float> damp_diag;
 };
 
 // Validates the description and assembles the constant matrices.  Returns an
@@ -306,6 +310,28 @@ inline std::string assemble(const AdmmB200Desc& d, Assembly& out) {
             for (auto& b : rows[r]) arow[a.first][b.first] += w2 * a.second * b.second;
         }
     }
+    // Rayleigh damping of the CPU backend (admm_impl_cpu.cpp:181-191):
+    // Damp = dt (damp_k_L Dd^T Wd Dd + damp_k_M M) over the triangle, tet and bending
+    // rows (constraint types below 4), Wd = diag(w); A_damp = A + Damp (:221).
+    std::vector<std::unordered_map<int, double>> drow;
+    if (d.backend_semantics == 1) {
+        drow.resize(nd);
+        const double kL = (double)d.damp_k_L, kM = (double)d.damp_k_M, h = (double)d.dt;
+        auto damped = [&](int r) {
+            return (d.n_tri && r >= d.tri_start_row && r < d.tri_start_row + 2 * d.n_tri) ||
+                   (d.n_tet && r >= d.tet_start_row && r < d.tet_start_row + 3 * d.n_tet) ||
+                   (d.n_bend && r >= d.bend_start_row && r < d.bend_start_row + d.n_bend);
+        };
+        for (int r = 0; r < m; r++) {
+            if (!damped(r)) continue;
+            const double s = h * kL * w[r];
+            for (auto& a : rows[r])
+                for (auto& b : rows[r]) drow[a.first][b.first] += s * a.second * b.second;
+        }
+        for (int i = 0; i < nd; i++) drow[i][i] += h * kM * (double)d.mass[i];
+        for (int i = 0; i < nd; i++)
+            for (auto& kv : drow[i]) arow[i][kv.first] += kv.second;
+    }
     out.dt2wc.assign(nd, 0.f);
     if (d.enable_contact) {
         std::vector<char> surf(n, 0);
@@ -335,6 +361,21 @@ inline std::string assemble(const AdmmB200Desc& d, Assembly& out) {
         std::sort(rt[i].begin(), rt[i].end());
         for (auto& kv : rt[i]) { rc.col.push_back(kv.first); rc.val.push_back(kv.second); }
         rc.start[i + 1] = (int)rc.col.size();
+    }
+    if (d.backend_semantics == 1) {
+        HostCsr dc;
+        dc.start.assign(nd + 1, 0);
+        out.damp_diag.assign(nd, 0.f);
+        for (int i = 0; i < nd; i++) {
+            std::vector<std::pair<int, double>> e(drow[i].begin(), drow[i].end());
+            std::sort(e.begin(), e.end());
+            for (auto& kv : e) {
+                if (kv.first == i) out.damp_diag[i] = (float)kv.second;
+                else { dc.col.push_back(kv.first); dc.val.push_back(kv.second); }
+            }
+            dc.start[i + 1] = (int)dc.col.size();
+        }
+        out.damp = std::move(dc);
     }
     out.A = std::move(ac);
     out.R = std::move(rc);

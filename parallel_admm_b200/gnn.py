@@ -347,20 +347,33 @@ class SweepTrainer:
         return loss.value, go, gb, gm, gt
 
 
-def global_samples(h: "B.Handle", trainer: SweepTrainer, frames: int, iterations: Sequence[int],
-                   tol: float = 1e-6) -> Tuple[np.ndarray, ...]:
-    """(b, x_c, x_l, x*) samples of the global step from plain substeps: frame f records
+def global_samples(h: "B.Handle", trainer: SweepTrainer, count: int, iterations: Sequence[int],
+                   tol: float = 1e-6, max_substeps: Optional[int] = None) -> Tuple[np.ndarray, ...]:
+    """(b, x_c, x_l, x*) samples of the global step from plain substeps: substep f records
     global step iterations[f % len(iterations)] (every recording is one substep of the
-    simulation); x* by conjugate gradients on the GPU."""
+    simulation); x* by conjugate gradients on the GPU.  A sample whose x_c is already the
+    solution to FP32 precision (max |x_c - x*| <= 20 eps32 max(1, max |x*|), e.g. a free-fall
+    frame) carries no error to learn from and is dropped; recording continues until `count`
+    samples or max_substeps (default 3 count) substeps."""
     bs, xcs, xls, xss = [], [], [], []
-    for f in range(frames):
+    limit = 3 * count if max_substeps is None else max_substeps
+    eps = 20.0 * float(np.finfo(np.float32).eps)
+    f = 0
+    while len(bs) < count and f < limit:
         it = int(iterations[f % len(iterations)])
+        f += 1
         b, xc, xl = h.record_global(it, allow=(B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW))
         xs, _ = trainer.solve(b, xc, tol)
+        if np.abs(xc - xs).max() <= eps * max(1.0, float(np.abs(xs).max())):
+            continue
         bs.append(b)
         xcs.append(xc)
         xls.append(xl)
         xss.append(xs)
+    n = trainer.sysm.n
+    if not bs:
+        z = np.zeros((0, n, 3), np.float32)
+        return z, z.copy(), z.copy(), z.copy()
     return tuple(np.array(a, np.float32) for a in (bs, xcs, xls, xss))
 
 

@@ -65,6 +65,9 @@ class SolverParams:
     pcg_iter: int = 0  # 0 = jacobi_iter // 2
     query_lanes: int = 0  # lanes per grid DCD query: 0 chosen from the query count, or 8, 16, 32
     contact_semantics: int = 0  # contact predicates: 0 the GPU backend's, 1 the CPU backend's
+    backend_semantics: int = 0  # solver: 0 the GPU backend's, 1 the CPU backend's (damping, GS contact)
+    damp_k_L: float = 1e-4      # Rayleigh damping of the CPU backend (admm_config.h:52-53)
+    damp_k_M: float = 0.0
 
 
 @dataclasses.dataclass

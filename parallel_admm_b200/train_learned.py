@@ -1,0 +1,196 @@
+"""Train and evaluate the learned global step (global_solver 3) on the cube family.
+
+    python -m parallel_admm_b200.train_learned --out parallel_admm_b200/weights/learned_step.npz
+
+Training data: plain Jacobi runs of the tetrahedralised cube (20^3 cells, 5 tets per cell,
+edge 0.5 m, nu = 0.4) with per seed E log-uniform in [1e4, 1e6], drop height U(0.5, 2) m
+and a random initial rotation.  Each run of `--samples` frames records one global step per
+frame (iteration cycling over 1..29 of the 30): (b, x_cur, x_last) through
+admm_b200_record_global, and x* = A^-1 b by conjugate gradients on the GPU -- the
+(system, residual, converged solution) triples.  Training is online, one pass over the
+triples as they are produced (batches of `--batch` from the current seed, plus one
+replayed batch from a bounded buffer of earlier seeds), with the GPU forward/backward of
+the network (csrc/gnn.cu) and of the unrolled sweeps (csrc/learn.cu); one model per sweep
+count in `--sweeps`, all on the same data.
+
+Evaluation on `--eval-seeds` held-out seeds (seeds after the training ones): for each, a
+run advanced to `--eval-frame` frames, then `--eval-samples` recorded global steps; per
+model the A-norm error ratio after its K sweeps (its own number, no fallback involved),
+against K and 20 plain Jacobi sweeps (the reference's count) on the same samples; on every
+tenth held-out seed a learned handle runs `--eval-substeps` substeps and reports its judged
+solves and fallbacks.  Prints one JSON summary; the chosen model (the fewest sweeps whose
+held-out error is at most 20 Jacobi sweeps', else the most sweeps) is written to --out.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+from collections import deque
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from parallel_admm_b200 import backend as B  # noqa: E402
+from parallel_admm_b200 import gnn, scene  # noqa: E402
+
+ALLOW = (B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW)
+
+
+def family_scene(seed: int, n: int):
+    """One member of the cube family (drop U(0.5, 2) m, E log-U, random rotation)."""
+    rng = np.random.default_rng(10_000 + seed)
+    drop = float(rng.uniform(0.5, 2.0))
+    sc = scene.cube_on_ground(n, seed=seed, drop=drop, rotate=True)
+    sc.params.ell_lanes = 4
+    sc.params.jacobi_mode = 1
+    return sc
+
+
+def system_of(sc):
+    h = B.Handle(sc)
+    sysm = gnn.system(h)
+    x, ef = gnn.scene_features(sc, sysm)
+    return h, sysm, x, ef
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "parallel_admm_b200", "weights", "learned_step.npz"))
+    ap.add_argument("--n", type=int, default=20, help="cube cells per edge")
+    ap.add_argument("--train-seeds", type=int, default=200)
+    ap.add_argument("--samples", type=int, default=100, help="recorded global steps (frames) per training seed")
+    ap.add_argument("--eval-seeds", type=int, default=500)
+    ap.add_argument("--eval-frame", type=int, default=40)
+    ap.add_argument("--eval-samples", type=int, default=3)
+    ap.add_argument("--eval-substeps", type=int, default=10)
+    ap.add_argument("--sweeps", default="6,8,10")
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--replay", type=int, default=1500, help="samples kept for replay")
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr-coef", type=float, default=2e-3)
+    ap.add_argument("--lo-frac", type=float, default=0.1)
+    args = ap.parse_args(argv)
+    Ks = [int(k) for k in args.sweeps.split(",")]
+    t_start = time.time()
+    rng = np.random.default_rng(0)
+
+    # --- training: online over the triples of plain runs ---
+    models = {}
+    replay = deque(maxlen=args.replay)
+    hist = {K: [] for K in Ks}
+    n_triples = 0
+    t_gen = t_fit = 0.0
+    for seed in range(args.train_seeds):
+        sc = family_scene(seed, args.n)
+        h, sysm, x, ef = system_of(sc)
+        tr = gnn.SweepTrainer(sysm)
+        if not models:
+            lam = gnn.jacobi_spectrum_top(sysm)
+            for K in Ks:
+                models[K] = gnn.LearnedGlobalStep(K=K)
+                models[K].init_chebyshev(lam, args.lo_frac)
+        t0 = time.time()
+        S = gnn.global_samples(h, tr, args.samples, range(1, sc.params.admm_max_iter))
+        t_gen += time.time() - t0
+        n_triples += S[0].shape[0]
+        t0 = time.time()
+        order = rng.permutation(S[0].shape[0])
+        for j in range(0, len(order), args.batch):
+            sel = order[j:j + args.batch]
+            for K, mdl in models.items():
+                data = [(sysm, x, ef, tr, tuple(a[sel] for a in S))]
+                hist[K].append(mdl.fit(data, epochs=1, batch=args.batch, lr=args.lr, lr_coef=args.lr_coef,
+                                       seed=seed)[0])
+            if replay:
+                r = replay[int(rng.integers(len(replay)))]
+                for K, mdl in models.items():
+                    mdl.fit([r], epochs=1, batch=args.batch, lr=args.lr, lr_coef=args.lr_coef, seed=seed)
+        # keep a few samples of this seed (with its system) for replay
+        keep = rng.choice(S[0].shape[0], min(args.batch, S[0].shape[0]), replace=False)
+        replay.append((sysm, x, ef, tr, tuple(a[keep] for a in S)))
+        t_fit += time.time() - t0
+        h.close()
+        if seed % 20 == 0:
+            print(f"seed {seed}: triples {n_triples}, loss " +
+                  ", ".join(f"K{K} {np.mean(hist[K][-12:]):.3e}" for K in Ks), flush=True)
+
+    # --- evaluation on held-out seeds ---
+    ev = {K: [] for K in Ks}
+    ev_j = {K: [] for K in Ks}
+    ev_j20 = []
+    fb = {K: {"substeps": 0, "fallbacks": 0, "solves": 0, "failed_solves": 0} for K in Ks}
+    t0 = time.time()
+    for e in range(args.eval_seeds):
+        seed = args.train_seeds + e
+        sc = family_scene(seed, args.n)
+        h, sysm, x, ef = system_of(sc)
+        h.step(args.eval_frame, allow=ALLOW)
+        tr = gnn.SweepTrainer(sysm)
+        S = gnn.global_samples(h, tr, args.eval_samples, (3, 11, 23))
+        jm = (1.0 / sysm.diag).astype(np.float32)
+        z = np.zeros(sysm.n, np.float32)
+        ev_j20.append(tr.loss_grad(np.ones(20, np.float32), np.zeros(20, np.float32), jm, z, *S)[0])
+        for K, mdl in models.items():
+            m, th = mdl.outputs(sysm, x, ef)
+            ev[K].append(tr.loss_grad(mdl.omega, mdl.beta, m, th, *S)[0])
+            ev_j[K].append(tr.loss_grad(np.ones(K, np.float32), np.zeros(K, np.float32), jm, z, *S)[0])
+        if e % 10 == 0:
+            for K, mdl in models.items():
+                sc.params.global_solver = 3
+                h3 = B.Handle(sc)
+                mdl.apply(h3, gnn.system(h3), x, ef)
+                h3.step(args.eval_frame, allow=ALLOW)
+                s0 = h3.learned_stats()
+                h3.step(args.eval_substeps, allow=ALLOW)
+                s1 = h3.learned_stats()
+                for k in fb[K]:
+                    fb[K][k] += s1[k] - s0[k]
+                h3.close()
+        tr.close()
+        h.close()
+    t_eval = time.time() - t0
+
+    def stats(a):
+        a = np.asarray(a)
+        return {"mean": float(a.mean()), "median": float(np.median(a)), "p90": float(np.quantile(a, 0.9))}
+
+    j20 = stats(ev_j20)
+    summary = {"train": {"family": f"cube {args.n}^3, E log-U[1e4,1e6], drop U(0.5,2) m, random rotation",
+                         "seeds": args.train_seeds, "triples": n_triples, "gen_s": round(t_gen, 1),
+                         "fit_s": round(t_fit, 1)},
+               "eval": {"held_out_seeds": args.eval_seeds, "samples_per_seed": args.eval_samples,
+                        "frame": args.eval_frame, "eval_s": round(t_eval, 1),
+                        "metric": "|x_K - x*|_A^2 / |x_c - x*|_A^2 after the global step",
+                        "jacobi20": j20},
+               "models": {}}
+    chosen = None
+    for K in Ks:
+        s = stats(ev[K])
+        summary["models"][K] = {"learned": s, "jacobi_same_sweeps": stats(ev_j[K]),
+                                "loss_first": float(np.mean(hist[K][:12])), "loss_last": float(np.mean(hist[K][-12:])),
+                                "omega": [round(float(v), 4) for v in models[K].omega],
+                                "beta": [round(float(v), 4) for v in models[K].beta],
+                                "judged": fb[K]}
+        if chosen is None and s["mean"] <= j20["mean"]:
+            chosen = K
+    if chosen is None:
+        chosen = max(Ks)
+    summary["chosen_sweeps"] = chosen
+    summary["wall_s"] = round(time.time() - t_start, 1)
+    os.makedirs(os.path.dirname(args.out), exist_ok=True)
+    models[chosen].save(args.out)
+    for K, mdl in models.items():
+        root, ext = os.path.splitext(args.out)
+        mdl.save(f"{root}_K{K}{ext}")
+    print(json.dumps(summary), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -3,7 +3,10 @@
 // (src/app/app_initializer.cpp:142-228) on a scene read from a binary file
 // written by tests/test_cpp_backend.py, and writes the positions after N steps.
 //
-//   drive_backend <scene.bin> <out.bin>
+//   drive_backend <scene.bin> <out.bin> [<contacts.bin>]
+// With a third argument, the ICollisionDetector view (ADU::BVHB200) then detects on the
+// positions after the steps and writes: count, max_slots, peak (int64 each), then
+// max_slots points and max_slots normals (float32 x 3).
 #include <cstdint>
 #include <cstdio>
 #include <fstream>
@@ -117,6 +120,24 @@ int main(int argc, char** argv) {
     }
     std::ofstream o(argv[2], std::ios::binary);
     o.write(reinterpret_cast<const char*>(inner->m_vertices.data()), sizeof(float) * 3 * n);
+    if (argc > 3) {
+        try {
+            ADU::BVHB200 det(backend);
+            ADU::ICollisionDetector& cd = det;  // through the reference's contract
+            cd.detect(inner->m_vertices);
+            const int64_t head[3] = {(int64_t)cd.contact_count(), (int64_t)cd.max_slots(),
+                                     (int64_t)cd.peak_contact_count()};
+            const auto pts = cd.points();
+            const auto nrm = cd.normals();
+            std::ofstream c(argv[3], std::ios::binary);
+            c.write(reinterpret_cast<const char*>(head), sizeof(head));
+            for (const auto& p : pts) c.write(reinterpret_cast<const char*>(p.data()), sizeof(float) * 3);
+            for (const auto& p : nrm) c.write(reinterpret_cast<const char*>(p.data()), sizeof(float) * 3);
+        } catch (const std::exception& e) {
+            std::fprintf(stderr, "drive_backend: %s\n", e.what());
+            return 1;
+        }
+    }
     std::printf("steps %d contacts %zu\n", nsteps, inner->step_metrics.empty() ? 0 : inner->step_metrics.back().n_contacts);
     return 0;
 }

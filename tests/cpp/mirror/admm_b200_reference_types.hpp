@@ -2,10 +2,12 @@
 // types that include/admm_b200_backend.hpp uses, with the same names, members
 // and virtual functions (src/solver/solver.h, src/solver/core/admm_backend.h,
 // src/solver/core/admm_config.h, src/constraint/*_constraint.h,
-// src/contact/contact_parameter.h, src/contact/narrow_phase.h), so the adapter
+// src/contact/contact_parameter.h, src/contact/narrow_phase.h,
+// src/contact/icollision_detector.h), so the adapter
 // compiles and runs here without the reference's dependencies.  Put this
 // directory before include/ on the include path.
 #pragma once
+#include <array>
 #include <cstddef>
 #include <memory>
 #include <unordered_set>
@@ -63,8 +65,25 @@ struct ADMMSolverConfig {
     Real mu{0.5f};
     Real kappa{1e6f};
     Real beta{1e5f};
+    Real damp_k_L{1e-4f};
+    Real damp_k_M{0.0f};
     Vecf_X contact_w_list;
     Vecf_X contact_w_inv_list;
+};
+}  // namespace ADU
+
+namespace ADU {
+// src/contact/icollision_detector.h:19-47 (host-facing collision-detection contract)
+class ICollisionDetector {
+public:
+    virtual ~ICollisionDetector() = default;
+    virtual void detect(const Matf_X3& pos) = 0;
+    virtual size_t contact_count() const = 0;
+    virtual size_t max_slots() const = 0;
+    virtual size_t peak_contact_count() const = 0;
+    virtual std::vector<std::array<float, 3>> points() = 0;
+    virtual std::vector<std::array<float, 3>> normals() = 0;
+    virtual void clear() = 0;
 };
 }  // namespace ADU
 

@@ -65,3 +65,29 @@ def test_adapter_matches_c_abi_path(tmp_path, name):
     h.step(nsteps)
     x_py, _ = h.get_state()
     assert np.array_equal(x_cpp, x_py)
+
+
+@pytest.mark.gpu
+def test_collision_detector_view_matches_the_c_abi(tmp_path):
+    """ADU::BVHB200, the ICollisionDetector view of the backend's handle, through the
+    reference's contract: the contact count, max_slots() rows of points and normals (zero past
+    the count) and the peak equal the C ABI's contacts on the same positions."""
+    sc = scene.batch_bodies(4, seed=1, vmin=300, vmax=900)  # bodies within the contact band of the ground
+    sc.params.ell_lanes = 4
+    exe = _build(tmp_path)
+    nsteps = 1
+    _write_scene(sc, tmp_path / "scene.bin", nsteps)
+    r = subprocess.run([exe, str(tmp_path / "scene.bin"), str(tmp_path / "x.bin"), str(tmp_path / "c.bin")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw = open(tmp_path / "c.bin", "rb").read()
+    count, slots, peak = np.frombuffer(raw[:24], np.int64)
+    body = np.frombuffer(raw[24:], np.float32).reshape(2, slots, 3)
+    x_cpp = np.fromfile(tmp_path / "x.bin", np.float32).reshape(sc.n_vert, 3)
+    h = B.Handle(sc)
+    n = h.detect(x_cpp, allow=(B.ERR_CONTACT_OVERFLOW,))
+    c = h.contacts()
+    assert count == n > 0 and slots == h.max_slots() and peak >= count
+    np.testing.assert_array_equal(body[0, :n], c["point"])
+    np.testing.assert_array_equal(body[1, :n], c["normal"])
+    assert not body[:, n:].any()

@@ -100,12 +100,17 @@ def test_learned_substep_matches_the_oracle_with_contact():
 
 def test_judge_falls_back_to_plain_jacobi():
     """A schedule that steps slightly backwards (one sweep with omega = -0.05: the residual
-    grows a little, the positions stay near the inertial prediction) fails the judge: every
-    substep is run again with the plain Jacobi global step, bit for bit the plain handle's
-    substep."""
+    grows a little, the positions stay near the inertial prediction) fails the judge on a
+    deformed cube: every substep is run again with the plain Jacobi global step, bit for bit
+    the plain handle's substep."""
     sc = _pin(scene.cube_on_ground(8))
     hj = B.Handle(sc)
     hl = B.Handle(sc, global_solver=3)
+    rng = np.random.default_rng(0)
+    x = sc.verts.copy()
+    x[:sc.n_dyn] += rng.normal(scale=2e-3, size=(sc.n_dyn, 3)).astype(np.float32)
+    hj.set_state(x)
+    hl.set_state(x)
     hl.set_learned(np.full(1, -0.05, np.float32), np.zeros(1, np.float32))
     for _ in range(3):
         hj.step(1, allow=ALLOW)
@@ -119,8 +124,20 @@ def test_judge_falls_back_to_plain_jacobi():
     hl.close()
 
 
-def _samples(h, sysm, tr, frames=3, iters=(3, 7, 12)):
-    S = gnn.global_samples(h, tr, frames, iters)
+def _impact_cube(n, seed=0):
+    """A cube 3 cm above the ground at the speed of a 1 m drop: contact from the first frame,
+    so the plain global solves leave real errors (free-fall solves converge to FP32 noise)."""
+    sc = _pin(scene.cube_on_ground(n, seed=seed, drop=0.0))
+    v0 = np.zeros_like(sc.verts)
+    v0[:sc.n_dyn, 1] = -np.sqrt(2 * 9.8 * 1.0)
+    x0 = sc.verts.copy()
+    x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.03
+    return sc, x0, v0
+
+
+def _samples(h, sysm, tr, count=3, iters=(3, 7, 12)):
+    S = gnn.global_samples(h, tr, count, iters)
+    assert S[0].shape[0] == count
     A = lambda v: sysm.matvec(v.astype(np.float64))
     for b, xs in zip(S[0], S[3]):
         assert np.linalg.norm(A(xs) - b) <= 1e-4 * np.linalg.norm(b)
@@ -128,10 +145,10 @@ def _samples(h, sysm, tr, frames=3, iters=(3, 7, 12)):
 
 
 def test_training_gradients_match_the_restatement():
-    sc = _pin(scene.cube_on_ground(5, seed=2))
+    sc, x0, v0 = _impact_cube(6, seed=2)
     h = B.Handle(sc)
+    h.set_state(x0, v0)
     sysm = gnn.system(h)
-    h.step(2, allow=ALLOW)
     tr = gnn.SweepTrainer(sysm)
     S = _samples(h, sysm, tr)
     assert np.abs(S[1] - S[2]).max() > 0  # x_cur and x_last differ
@@ -141,7 +158,7 @@ def test_training_gradients_match_the_restatement():
     samples = [tuple(d(a[k]) for a in S) for k in range(S[0].shape[0])]
     lo, go_, gb_, gm_, gt_ = G.sweeps_loss_grad(d(m), d(th), d(om), d(be), sysm.start, sysm.col, d(sysm.val),
                                                 d(sysm.diag), samples)
-    assert abs(loss - lo) <= 1e-4 * abs(lo), (loss, lo)
+    assert abs(loss - lo) <= 1e-3 * abs(lo), (loss, lo)
     for a, b_ in ((go, go_), (gb, gb_), (gm, gm_), (gt, gt_)):
         assert np.linalg.norm(a - b_) <= 2e-3 * np.linalg.norm(b_), np.linalg.norm(a - b_) / np.linalg.norm(b_)
     tr.close()
@@ -189,7 +206,7 @@ def test_training_gains_over_jacobi():
         x, ef = gnn.scene_features(sc, sysm)
         h.step(3, allow=ALLOW)
         tr = gnn.SweepTrainer(sysm)
-        data.append((sysm, x, ef, tr, gnn.global_samples(h, tr, 16, (1, 2, 4, 8, 15, 25))))
+        data.append((sysm, x, ef, tr, gnn.global_samples(h, tr, 16, (1, 2, 4, 8, 15, 25), max_substeps=60)))
         h.close()
     model = gnn.LearnedGlobalStep(K=8)
     model.init_chebyshev(gnn.jacobi_spectrum_top(data[0][0]))
@@ -204,7 +221,8 @@ def test_training_gains_over_jacobi():
         x, ef = gnn.scene_features(sc, sysm)
         h.step(3, allow=ALLOW)
         tr = gnn.SweepTrainer(sysm)
-        S = gnn.global_samples(h, tr, 8, (2, 5, 10, 20))
+        S = gnn.global_samples(h, tr, 8, (2, 5, 10, 20), max_substeps=40)
+        assert S[0].shape[0] > 0
         m, th = model.outputs(sysm, x, ef)
         jm = (1.0 / sysm.diag).astype(np.float32)
         z = np.zeros(sysm.n, np.float32)

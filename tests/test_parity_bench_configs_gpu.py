@@ -1,0 +1,144 @@
+"""Parity of the CUDA substep against the oracle at the sizes that are benchmarked.
+
+* the 20^3 cube (9261 vertices, 40000 tets): three free frames at impact speed against
+  the FP64 oracle (1e-5 per step), then seven impact frames one substep at a time against
+  the FP32 oracle (identical contact counts, 1e-4);
+* the 256-body batch at full size (1.45 M vertices, 6.07 M tets, contacts from the first
+  frame): two substeps one at a time against the FP32 oracle, with the plain Jacobi step
+  and with the learned step (same schedule on both sides);
+* two 256^2 cloth sheets on the sphere: one substep at impact against the FP32 oracle;
+* the 32x32 cloth on the box for 100 frames (through its contact with the box) against the
+  FP64 oracle, within 1e-3 relative.
+
+Relative errors are max |x_gpu - x_oracle| over the largest extent of the dynamic body
+(or 1 m, whichever is larger).  Contact frames are compared from a shared state, one
+substep at a time, against the FP32 oracle: contacts at the edge of the thickness band
+decide differently in FP32 and FP64, and the narrow phase is FP32 on both sides of the
+reference."""
+import numpy as np
+import pytest
+
+from parallel_admm_b200 import backend as B
+from parallel_admm_b200 import gnn, scene
+
+pytestmark = pytest.mark.gpu
+
+ALLOW = (B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW)
+
+
+_BATCH = {}
+
+
+def _batch256():
+    """The full batch, built once per test process (about a minute of set-up)."""
+    if "sc" not in _BATCH:
+        _BATCH["sc"] = scene.batch_bodies(256, seed=0)
+    return _BATCH["sc"]
+
+
+def _gpu_to_oracle(h, o):
+    x, v = h.get_state()
+    for buf, a in ((B.BUF_X0, x), (B.BUF_X, x), (B.BUF_V, v), (B.BUF_UE, h.read(B.BUF_UE)),
+                   (B.BUF_UC, h.read(B.BUF_UC))):
+        o.write(buf, a.astype(np.float64))
+
+
+def test_cube20_parity():
+    from oracle import oracle as O
+    sc = scene.cube_on_ground(20, drop=0.0)
+    v0 = np.zeros_like(sc.verts)
+    v0[:sc.n_dyn, 1] = -np.sqrt(2 * 9.8 * 1.0)
+    x0 = sc.verts.copy()
+    x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.03
+    h = B.Handle(sc)
+    o = O.Oracle(h.holder, double=True)
+    o32 = O.Oracle(h.holder, double=False)
+    h.set_state(x0, v0)
+    for orc in (o, o32):
+        orc.write(B.BUF_X0, x0)
+        orc.write(B.BUF_V, v0)
+        orc.write(B.BUF_X, x0)
+    ext = max(1.0, np.ptp(x0[:sc.n_dyn], axis=0).max())
+    ncs = []
+    for k in range(3):
+        sg = h.step(1, allow=ALLOW)
+        so = o.step(1)
+        o32.step(1)
+        ncs.append((sg["n_contacts"], so["n_contacts"]))
+        err = np.abs(h.get_state()[0] - o.read(B.BUF_X0)).max() / ext
+        assert err <= 1e-5 * (k + 1), (k, err, ncs)
+    for k in range(3, 10):
+        h.set_state(o32.read(B.BUF_X0), o32.read(B.BUF_V))
+        h.write(B.BUF_UE, o32.read(B.BUF_UE))
+        h.write(B.BUF_UC, o32.read(B.BUF_UC))
+        sg = h.step(1, allow=ALLOW)
+        so = o32.step(1)
+        ncs.append((sg["n_contacts"], so["n_contacts"]))
+        assert sg["n_contacts"] == so["n_contacts"], (k, ncs)
+        err = np.abs(h.get_state()[0] - o32.read(B.BUF_X0)).max() / ext
+        assert err <= 1e-4, (k, err, ncs)
+    assert min(c[0] for c in ncs[3:]) > 1000, ncs
+
+
+@pytest.mark.parametrize("solver", ["jacobi", "learned"])
+def test_batch256_full_size_parity(solver):
+    from oracle import oracle as O
+    sc = _batch256()
+    gs = 3 if solver == "learned" else 0
+    h = B.Handle(sc, global_solver=gs)
+    o = O.Oracle(h.holder, double=False)
+    if solver == "learned":
+        om, be = gnn.chebyshev_coefficients(10, 0.1 * 1.66, 1.7)
+        h.set_learned(om, be)
+        o.set_learned(om, be)
+    ncs = []
+    for k in range(2):
+        _gpu_to_oracle(h, o)
+        sg = h.step(1, allow=ALLOW)
+        so = o.step(1)
+        ncs.append((sg["n_contacts"], so["n_contacts"]))
+        assert sg["n_contacts"] == so["n_contacts"], (k, ncs)
+        err = np.abs(h.get_state()[0] - o.read(B.BUF_X0)).max()  # bodies of <= 0.6 m, extent 1 m floor
+        assert err <= 1e-4, (k, err, ncs)
+    assert min(c[0] for c in ncs) > 10000, ncs
+    if solver == "learned":
+        sg_, so_ = h.learned_stats(), o.learned_stats()
+        assert sg_["fallbacks"] == so_["fallbacks"], (sg_, so_)
+
+
+def test_sheets_small_impact_parity():
+    from oracle import oracle as O
+    sc = scene.sheets_on_sphere(256, layers=2, seed=0)
+    h = B.Handle(sc)
+    nc = 0
+    for f in range(80):
+        nc = h.step(1, allow=ALLOW)["n_contacts"]
+        if nc > 500:
+            break
+    assert nc > 500, nc
+    o = O.Oracle(h.holder, double=False)
+    _gpu_to_oracle(h, o)
+    sg = h.step(1, allow=ALLOW)
+    so = o.step(1)
+    assert sg["n_contacts"] == so["n_contacts"], (sg["n_contacts"], so["n_contacts"])
+    err = np.abs(h.get_state()[0] - o.read(B.BUF_X0)).max()
+    assert err <= 1e-4, err
+
+
+def test_cloth32_100_frames_within_1e3_of_fp64():
+    """The CPU-runnable cloth (32x32 over the unit box, 20 ADMM iterations, dt = 1/200) for
+    100 frames, free-running against the FP64 oracle: it meets the box near frame 64."""
+    from oracle import oracle as O
+    sc = scene.cloth_on_box(32, seed=0)
+    h = B.Handle(sc)
+    o = O.Oracle(h.holder, double=True)
+    worst, contacts = 0.0, 0
+    for f in range(100):
+        sg = h.step(1, allow=ALLOW)
+        o.step(1)
+        contacts = max(contacts, sg["n_contacts"])
+        err = np.abs(h.get_state()[0] - o.read(B.BUF_X0)).max()
+        worst = max(worst, err)
+    print(f"cloth 32x32, 100 frames: max |x_gpu - x_fp64| = {worst:.3e} m, peak contacts {contacts}")
+    assert contacts > 0
+    assert worst <= 1e-3, worst
