@@ -73,14 +73,21 @@ def test_damped_matrix_is_a_plus_damping():
 
 
 def test_cpu_backend_substeps_fp64_against_fp32():
-    """The pinned cloth over the box for 40 frames in the CPU backend's semantics: FP32 and
-    FP64 restatements agree (exact solves, serial Gauss-Seidel contact)."""
+    """The pinned cloth over the box in the CPU backend's semantics (exact solves, serial
+    Gauss-Seidel contact), 40 frames: every FP32 substep, started from the FP64 state, agrees
+    with the FP64 substep within 2e-5 m.  (Free-running, the two drift apart by ~1e-4 m per
+    frame: the pinned cloth is stiff, kappa(D^-1 A) ~ 700, and converged solves amplify the FP32
+    rounding of the reference's own float arithmetic.)"""
     sc = scene.cloth_on_box(16, seed=0)
     sc.params.backend_semantics = 1
     holder = B.DescHolder(sc)
     o64 = O.Oracle(holder, double=True)
     o32 = O.Oracle(holder, double=False)
+    worst = 0.0
     for _ in range(40):
+        for buf in (B.BUF_X0, B.BUF_X, B.BUF_V, B.BUF_UE, B.BUF_UC):
+            o32.write(buf, o64.read(buf).astype(np.float32).astype(np.float64))
         o64.step(1)
         o32.step(1)
-    assert np.abs(o64.read(B.BUF_X0) - o32.read(B.BUF_X0)).max() <= 1e-3
+        worst = max(worst, np.abs(o64.read(B.BUF_X0) - o32.read(B.BUF_X0)).max())
+    assert worst <= 2e-5, worst
