@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -417,6 +418,10 @@ int enqueue_contact(AdmmB200* h, bool dual) {
     // for odd j, s.du2 for even j.
     auto P = [&](int j) { return (j & 1) ? s.p2 : s.p; };
     auto D = [&](int j) { return (j & 1) ? s.du : s.du2; };
+    // k_contact_du, the passes and the last gather load detection data before their
+    // dependency wait; that is legal only because the kernel launched right before each of
+    // them (k_contact_p, then each pass) waits before it triggers (ADMM_PDL_WAIT_THEN_TRIGGER)
+    // -- keep k_contact_p directly before this launch.
     LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_du, h->contact_grid, kContactThreads, s);
     for (int g = 2; g <= G; g++)
         LAUNCH_P(ADMM_KERNEL_CONTACT_DU, k_contact_pass, h->pass_grid, kContactThreads, s, P(g - 2), P(g - 1),
@@ -1370,6 +1375,10 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     if (prop.major != 10) return fail(h, ADMM_ERR_NO_DEVICE, "device is not sm_100 (Blackwell B200)");
     CK(cudaSetDevice(device));
     h->device = device;
+    // ADMM_B200_PDL=0 launches every kernel of a substep without programmatic dependent
+    // launch (each kernel then starts after its predecessor completes); results are
+    // the same bits either way, which the tests check.
+    if (const char* e = std::getenv("ADMM_B200_PDL")) h->pdl = !(e[0] == '0' && e[1] == '\0');
 
     Assembly as;
     std::string why = assemble(*d, as);

@@ -115,7 +115,9 @@ __global__ void __launch_bounds__(128) k_dense_fwd_tc(const float* __restrict__ 
             umma::mma_tf32(td, umma::smem_desc(a0 + 256u * k, C), umma::smem_desc(b0 + 256u * k, C), idesc, k > 0);
         umma::commit(&mbar);
     }
-    const bool ok = umma::mbar_wait(&mbar, 0, 1 << 22);
+    bool ok = umma::mbar_wait(&mbar, 0, 1 << 22);
+    if (!ok) umma::mbar_wait(&mbar, 0, 1 << 22);  // the MMAs in flight, once more with a bound
+    ok = __syncthreads_and(ok) != 0;              // uniform: the TMEM loads below are warp-wide
     umma::fence_after();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = row0 + warp * 32 + lane;
@@ -145,6 +147,169 @@ __global__ void __launch_bounds__(128) k_dense_fwd_tc(const float* __restrict__ 
     if (threadIdx.x < 32) {
         umma::fence_after();
         umma::tmem_dealloc(td, kTcN);
+    }
+}
+
+// The backward products on the tensor cores (bf16 set), the same tcgen05 path as
+// k_dense_fwd_tc: operands rounded to TF32 (the weights to BF16 first) and staged in
+// shared memory in the canonical K-major layout, MMAs of 128 x NP x 8 issued by one
+// thread into FP32 accumulators in tensor memory, an mbarrier per batch of MMAs
+// (bounded waits: a wait that gives up sets err[0], waits once more with a bound for the
+// MMAs in flight, releases the TMEM and leaves without writing).
+//
+// dX[R x K] = dZ[R x N] W[N x K]: one CTA of 4 warps per 128 rows; A = the rows of dZ
+// (reduction over N, padded to NP8 = 8 * ceil(N / 8)), B = W^T (row k holds W[., k]),
+// the MMA's N = KP (K padded to 16).
+constexpr int kTcCols = 256;  // TMEM columns of a backward CTA (KP <= 256)
+
+// Every thread of the CTA waits (bounded); the result is the same in all threads (a
+// block-wide AND), so the warp-wide TMEM loads and the barriers after it stay convergent.
+__device__ __forceinline__ bool tc_wait_or_fail(uint64_t* mbar, uint32_t parity, int* err) {
+    bool ok = umma::mbar_wait(mbar, parity, 1 << 22);
+    if (!ok) umma::mbar_wait(mbar, parity, 1 << 22);  // the MMAs in flight, once more with a bound
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+    return ok;
+}
+
+__global__ void __launch_bounds__(128) k_dense_dx_tc(const float* __restrict__ dZ, int R, int N, int NP8,
+                                                     const float* __restrict__ W, int K, int KP,
+                                                     float* __restrict__ dX, int bf16, int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    const int C = NP8 / 4;
+    unsigned char* As = tc_smem;
+    unsigned char* Bs = tc_smem + (size_t)kTcRows * NP8 * 4;
+    const int row0 = blockIdx.x * kTcRows;
+    for (int i = threadIdx.x; i < kTcRows * NP8; i += blockDim.x) {
+        const int m = i / NP8, k = i % NP8;
+        const float v = (row0 + m < R && k < N) ? dZ[(size_t)(row0 + m) * N + k] : 0.f;
+        *(float*)(As + umma::core_offset(m, k >> 2, C) + (k & 3) * 4) = umma::tf32_round(v);
+    }
+    for (int i = threadIdx.x; i < KP * NP8; i += blockDim.x) {
+        const int j = i / NP8, n = i % NP8;
+        const float v = (j < K && n < N) ? wval(W, n * K + j, bf16) : 0.f;
+        *(float*)(Bs + umma::core_offset(j, n >> 2, C) + (n & 3) * 4) = umma::tf32_round(v);
+    }
+    umma::fence_operands();
+    if (threadIdx.x == 0) umma::mbar_init(&mbar, 1);
+    if (threadIdx.x < 32) umma::tmem_alloc(&tmem_base, kTcCols);
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t td = tmem_base;
+    if (threadIdx.x == 0) {
+        const uint32_t idesc = umma::idesc_tf32(kTcRows, KP);
+        const uint32_t a0 = umma::smem_u32(As), b0 = umma::smem_u32(Bs);
+        for (int k = 0; k < NP8 / 8; k++)
+            umma::mma_tf32(td, umma::smem_desc(a0 + 256u * k, C), umma::smem_desc(b0 + 256u * k, C), idesc, k > 0);
+        umma::commit(&mbar);
+    }
+    const bool ok = tc_wait_or_fail(&mbar, 0, err);
+    umma::fence_after();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = row0 + warp * 32 + lane;
+    if (ok) {
+        const uint32_t tw = td + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < KP; c0 += 16) {
+            uint32_t r[16];
+            umma::tmem_load16(tw + c0, r);
+            umma::tmem_wait16(r);
+            if (row < R) {
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    if (c0 + j < K) dX[(size_t)row * K + c0 + j] = __uint_as_float(r[j]);
+            }
+        }
+    }
+    umma::fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        umma::fence_after();
+        umma::tmem_dealloc(td, kTcCols);
+    }
+}
+
+// Partials of dW[N x K] = dZ^T X and db[N] = sum_r dZ over rows [blockIdx * kRowsPerBlockW, ...):
+// part[block][n * K + k], part[block][N * K + n] (the layout of k_dense_dw).  The D
+// accumulator is 128 x KP with rows n < N (N <= 64; rows N.. are zero), columns k < K
+// and column K = the row sum (a column of ones appended to X gives db); the block's rows
+// go through in chunks of kDwChunk, one MMA batch and mbarrier phase per chunk.
+constexpr int kDwChunk = 64;
+
+__global__ void __launch_bounds__(128) k_dense_dw_tc(const float* __restrict__ dZ, const float* __restrict__ X, int R,
+                                                     int N, int K, int KP, float* __restrict__ part,
+                                                     int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    constexpr int C = kDwChunk / 4;
+    unsigned char* As = tc_smem;
+    unsigned char* Bs = tc_smem + (size_t)kTcRows * kDwChunk * 4;
+    if (threadIdx.x == 0) umma::mbar_init(&mbar, 1);
+    if (threadIdx.x < 32) umma::tmem_alloc(&tmem_base, kTcCols);
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t td = tmem_base;
+    const int rbeg = blockIdx.x * kRowsPerBlockW, rend = min(R, rbeg + kRowsPerBlockW);
+    bool ok = true;
+    uint32_t phase = 0;
+    for (int rc = rbeg; rc < rend && ok; rc += kDwChunk) {
+        // operands of this chunk: A row n = dZ[rc.., n], B row k = X[rc.., k] (row K: ones)
+        for (int i = threadIdx.x; i < kTcRows * kDwChunk; i += blockDim.x) {
+            const int n = i / kDwChunk, r = i % kDwChunk;
+            const float v = (n < N && rc + r < rend) ? dZ[(size_t)(rc + r) * N + n] : 0.f;
+            *(float*)(As + umma::core_offset(n, r >> 2, C) + (r & 3) * 4) = umma::tf32_round(v);
+        }
+        for (int i = threadIdx.x; i < KP * kDwChunk; i += blockDim.x) {
+            const int k = i / kDwChunk, r = i % kDwChunk;
+            float v = 0.f;
+            if (rc + r < rend) v = k < K ? X[(size_t)(rc + r) * K + k] : (k == K ? 1.f : 0.f);
+            *(float*)(Bs + umma::core_offset(k, r >> 2, C) + (r & 3) * 4) = umma::tf32_round(v);
+        }
+        umma::fence_operands();
+        umma::fence_before();
+        __syncthreads();
+        umma::fence_after();
+        if (threadIdx.x == 0) {
+            const uint32_t idesc = umma::idesc_tf32(kTcRows, KP);
+            const uint32_t a0 = umma::smem_u32(As), b0 = umma::smem_u32(Bs);
+            for (int k = 0; k < kDwChunk / 8; k++)
+                umma::mma_tf32(td, umma::smem_desc(a0 + 256u * k, C), umma::smem_desc(b0 + 256u * k, C), idesc,
+                               (rc > rbeg || k > 0) ? 1u : 0u);
+            umma::commit(&mbar);
+        }
+        ok = tc_wait_or_fail(&mbar, phase, err);
+        phase ^= 1u;
+        umma::fence_after();
+        __syncthreads();  // the next chunk overwrites the operands
+    }
+    const int nout = N * K + N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = warp * 32 + lane;
+    if (ok && rbeg < rend) {
+        const uint32_t tw = td + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < KP; c0 += 16) {
+            uint32_t r[16];
+            umma::tmem_load16(tw + c0, r);
+            umma::tmem_wait16(r);
+            if (n < N) {
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const int k = c0 + j;
+                    if (k < K) part[(size_t)blockIdx.x * nout + n * K + k] = __uint_as_float(r[j]);
+                    else if (k == K) part[(size_t)blockIdx.x * nout + N * K + n] = __uint_as_float(r[j]);
+                }
+            }
+        }
+    }
+    umma::fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        umma::fence_after();
+        umma::tmem_dealloc(td, kTcCols);
     }
 }
 
@@ -431,6 +596,7 @@ struct AdmmGnn {
     float *part = nullptr, *r = nullptr, *zv = nullptr, *res = nullptr, *gzv = nullptr;
     double *dots = nullptr, *scal = nullptr;
     int* derr = nullptr;    // set by a tensor-core layer whose bounded wait gave up
+    bool failed = false;    // a tensor-core layer timed out: outputs undefined, the handle refuses work
     cudaStream_t st = nullptr;
     std::string err;
 };
@@ -488,7 +654,24 @@ void dense_fwd(AdmmGnn* g, const float* X, int R, int K, int wo, int bo, int N, 
     k_dense_fwd<<<nblk(R, 4), 256, sm, g->st>>>(X, R, K, g->theta + wo, g->theta + bo, N, Z, Y, res, act, g->bf16);
 }
 
+// With BF16 weights the backward products run on the tensor cores (N <= 64 outputs of the
+// layer, K + 1 <= 256 inputs plus the bias column), else on the SIMT kernels.
 void dense_bwd(AdmmGnn* g, const float* dZ, const float* X, int R, int K, int wo, int N, float* dX) {
+    const int KP = (K + 1 + 15) / 16 * 16;
+    if (g->bf16 && N <= kTcN && KP <= kTcCols && R > 0) {
+        const int NP8 = (N + 7) / 8 * 8;
+        if (dX) {
+            const int KPx = (K + 15) / 16 * 16;
+            const size_t sm = std::max<size_t>(sizeof(float) * (size_t)(kTcRows + KPx) * NP8, 100 * 1024);
+            k_dense_dx_tc<<<nblk(R, kTcRows), 128, sm, g->st>>>(dZ, R, N, NP8, g->theta + wo, K, KPx, dX, g->bf16,
+                                                              g->derr);
+        }
+        const int nparts = nblk(R, kRowsPerBlockW), nout = N * K + N;
+        const size_t sm = std::max<size_t>(sizeof(float) * (size_t)(kTcRows + KP) * kDwChunk, 100 * 1024);
+        k_dense_dw_tc<<<nparts, 128, sm, g->st>>>(dZ, X, R, N, K, KP, g->part, g->derr);
+        k_reduce_parts<<<nblk(nout, 256), 256, 0, g->st>>>(g->part, nparts, nout, g->grad + wo);
+        return;
+    }
     if (dX) {
         const size_t sm = sizeof(float) * (size_t)(N * K + 4 * N);
         k_dense_dx<<<nblk(R, 4), 256, sm, g->st>>>(dZ, R, N, g->theta + wo, K, dX, g->bf16);
@@ -518,7 +701,9 @@ int tc_status(AdmmGnn* g) {
     int e = 0;
     if (cudaMemcpy(&e, g->derr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return ADMM_ERR_CUDA;
     if (!e) return ADMM_OK;
-    cudaMemset(g->derr, 0, sizeof(int));
+    // a CTA that gave up may have left its MMAs reading shared memory and writing TMEM:
+    // the outputs of that launch are undefined and the handle takes no further work
+    g->failed = true;
     return ADMM_ERR_TIMEOUT;
 }
 
@@ -549,6 +734,8 @@ int admm_gnn_create(int bf16, AdmmGnn** out) {
     cudaFuncSetAttribute(k_dense_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     cudaFuncSetAttribute(k_dense_dx, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     cudaFuncSetAttribute(k_dense_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_dense_dx_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_dense_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     *out = g;
     return ADMM_OK;
 }
@@ -638,6 +825,7 @@ int admm_gnn_get_params(AdmmGnn* g, float* theta, int P) {
 // Forward pass; blocks9 (host, n x 9 row-major) receives B_i = L_i L_i^T / a_ii.
 int admm_gnn_forward(AdmmGnn* g, float* blocks9) {
     if (!g || g->n <= 0) return ADMM_ERR_INVALID;
+    if (g->failed) return ADMM_ERR_STATE;
     forward(g);
     if (blocks9 && cudaMemcpyAsync(blocks9, g->B, sizeof(float) * 9 * (size_t)g->n, cudaMemcpyDeviceToHost, g->st) != cudaSuccess)
         return ADMM_ERR_CUDA;
@@ -651,6 +839,7 @@ int admm_gnn_forward(AdmmGnn* g, float* blocks9) {
 // null) receives it.
 int admm_gnn_loss_grad(AdmmGnn* g, const float* R, int K, double* loss, float* grad) {
     if (!g || g->n <= 0 || !R || K <= 0) return ADMM_ERR_INVALID;
+    if (g->failed) return ADMM_ERR_STATE;
     const int n = g->n;
     forward(g);
     cudaMemsetAsync(g->grad, 0, sizeof(float) * g->P, g->st);
@@ -687,6 +876,7 @@ int admm_gnn_loss_grad(AdmmGnn* g, const float* R, int K, double* loss, float* g
 // Per-vertex outputs of the learned global step: m (n) and theta (n), host.
 int admm_gnn_outputs(AdmmGnn* g, float* m, float* theta) {
     if (!g || g->n <= 0 || !m || !theta) return ADMM_ERR_INVALID;
+    if (g->failed) return ADMM_ERR_STATE;
     forward(g);
     k_outputs<<<nblk(g->n, 256), 256, 0, g->st>>>(g->B, g->o, g->n, g->r, g->zv);
     cudaMemcpyAsync(m, g->r, sizeof(float) * g->n, cudaMemcpyDeviceToHost, g->st);
@@ -701,6 +891,7 @@ int admm_gnn_outputs(AdmmGnn* g, float* m, float* theta) {
 // next admm_gnn_adam applies it.
 int admm_gnn_backward(AdmmGnn* g, const float* gm, const float* gtheta, float* grad) {
     if (!g || g->n <= 0 || !gm || !gtheta) return ADMM_ERR_INVALID;
+    if (g->failed) return ADMM_ERR_STATE;
     const int n = g->n;
     forward(g);
     cudaMemsetAsync(g->grad, 0, sizeof(float) * g->P, g->st);

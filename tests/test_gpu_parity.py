@@ -579,9 +579,12 @@ def test_batch_with_per_body_friction_parity():
     with per-vertex friction coefficients: the first substep free against the FP64 oracle
     (1e-5), then three substeps one at a time from the FP32 oracle's state against it (equal
     contact counts, 1e-4): from the second frame on, contacts at the edge of the thickness
-    band decide differently in FP32 and FP64."""
+    band decide differently in FP32 and FP64.  One detection per substep."""
     sc = scene.batch_bodies(6, seed=3, vmin=300, vmax=3000)
     assert sc.vert_mu is not None and len(np.unique(sc.vert_mu[:sc.n_dyn])) > 1
+    # one detection per substep: identical pair sets on both sides from a shared state (with
+    # the two bodies at 2 m/s a pair flipped at a later detection moves vertices by millimetres)
+    sc.params.dcd_interval = sc.params.admm_max_iter
     # start every body just above the ground, moving down, so that contacts appear at once
     x0 = sc.verts.copy()
     x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.012
@@ -658,3 +661,47 @@ def test_cpu_semantics_contact_step_parity():
     o.contact_step()
     pg, po = h.read(B.BUF_P), o.read(B.BUF_P)
     assert _rel(pg[:sc.n_dyn], po[:sc.n_dyn]) <= 1e-4
+
+
+@pytest.mark.parametrize("case", ["cube_impact", "sheets_small"])
+def test_programmatic_launch_does_not_change_bits(case):
+    """The same contact substeps with programmatic dependent launch (the default) and with it
+    off (ADMM_B200_PDL=0, every kernel starts after its predecessor completes), in child
+    processes: identical bits.  The contact kernels load detection data before their
+    dependency wait, which is legal only because the kernel launched before each of them
+    waits before it triggers."""
+    import json
+    import os
+    import subprocess
+    import sys
+    code = f"""
+import sys, json, numpy as np
+sys.path.insert(0, {os.path.dirname(os.path.dirname(os.path.abspath(__file__)))!r})
+from parallel_admm_b200 import backend as B, scene
+case = {case!r}
+if case == "cube_impact":
+    sc = scene.cube_on_ground(10, drop=0.0)
+    v0 = np.zeros_like(sc.verts); v0[:sc.n_dyn, 1] = -4.0
+    x0 = sc.verts.copy(); x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.03
+else:
+    sc = scene.sheets_on_sphere(256, layers=2, seed=0)
+    x0, v0 = sc.verts.copy(), np.zeros_like(sc.verts)
+    v0[:sc.n_dyn, 1] = -3.0
+sc.params.ell_lanes = 4
+sc.params.jacobi_mode = 1
+h = B.Handle(sc)
+h.set_state(x0, v0)
+cs = [h.step(1, allow=(B.ERR_CONTACT_OVERFLOW,))["n_contacts"] for _ in range(10)]
+x, v = h.get_state()
+np.save(sys.argv[1], np.concatenate([x, v]))
+print(json.dumps(cs))
+"""
+    outs = []
+    for pdl in ("1", "0"):
+        path = f"/tmp/pdl_{case}_{pdl}.npy"
+        env = dict(os.environ, ADMM_B200_PDL=pdl)
+        r = subprocess.run([sys.executable, "-c", code, path], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append((json.loads(r.stdout.strip().splitlines()[-1]), np.load(path)))
+    assert outs[0][0] == outs[1][0] and max(outs[0][0]) > 0, (outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
