@@ -210,6 +210,7 @@ def lib():
             "admm_b200_jacobi_noalloc": (ctypes.c_int, [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int,
                                                         vp]),
             "admm_b200_set_learned": (ctypes.c_int, [vp, ctypes.c_int, _f, _f, _f, _f, ctypes.c_int]),
+            "admm_b200_vertex_order": (ctypes.c_int, [vp, _i, ctypes.c_int]),
             "admm_b200_learned_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64)]),
             "admm_b200_record_global": (ctypes.c_int, [vp, ctypes.c_int, _f, _f, _f, ctypes.c_int]),
         }
@@ -239,6 +240,7 @@ def exported_symbols():
         "admm_gnn_set_params", "admm_gnn_get_params", "admm_gnn_forward", "admm_gnn_loss_grad", "admm_gnn_adam",
         "admm_b200_set_learned", "admm_b200_learned_stats", "admm_b200_record_global", "admm_gnn_outputs",
         "admm_gnn_backward", "admm_learn_create", "admm_learn_destroy", "admm_learn_loss_grad", "admm_learn_solve",
+        "admm_b200_vertex_order",
     ]
 
 
@@ -424,6 +426,12 @@ class Handle:
         th = None if theta is None else np.ascontiguousarray(theta, np.float32).reshape(self.n_dyn)
         self.check(lib().admm_b200_set_learned(self.h, len(om), _p(om), _p(be), None if mm is None else _p(mm),
                                                None if th is None else _p(th), self.n_dyn), "set_learned")
+
+    def vertex_order(self) -> np.ndarray:
+        """The caller's index of each internal vertex row (the library's storage order)."""
+        out = np.zeros(self.n_vert, np.int32)
+        self.check(lib().admm_b200_vertex_order(self.h, _p(out, _i), self.n_vert), "vertex_order")
+        return out
 
     def learned_stats(self) -> Dict[str, int]:
         out = (ctypes.c_int64 * 4)()

@@ -78,6 +78,16 @@ struct AdmmB200 {
     int* fail_host = nullptr;       // pinned copy of learn.fail
     int64_t learn_substeps = 0, learn_fallbacks = 0;
     bool force_plain = false;       // enqueue the Jacobi global step whatever global_solver says
+    // Vertex renumbering: the library stores the dynamic vertices in the Morton order of
+    // their rest positions (spatially close vertices at close indices, so the gathers of the
+    // sweeps, the local step and the right-hand side share cache lines); every entry point
+    // that takes or returns per-vertex data or vertex indices maps between that order and
+    // the caller's.  perm[internal] = caller's index, iperm[caller's] = internal; empty =
+    // identity (the CPU backend's semantics, whose serial Gauss-Seidel follows the contact
+    // order, and ADMM_B200_RENUMBER=0).
+    std::vector<int> perm, iperm;
+    int* d_perm = nullptr;
+    HostCsr hostA_caller;           // the global matrix in the caller's order (admm_b200_system)
     // recording of one global step's inputs (admm_b200_record_global, eager substeps)
     int rec_target = -1, rec_count = 0;
     float4 *rec_b = nullptr, *rec_cur = nullptr, *rec_last = nullptr;
@@ -1246,6 +1256,15 @@ int run_substep_eager(AdmmB200* h) {
 
 float4 pack(const float* p) { return make_float4(p[0], p[1], p[2], 0.f); }
 
+// The caller's index of internal vertex i (identity without renumbering).
+inline int caller_of(const AdmmB200* h, int i) { return h->perm.empty() ? i : h->perm[i]; }
+
+// Buffers with one row per vertex (the others have one per constraint row).
+inline bool per_vertex_buffer(int which) {
+    return which == ADMM_BUF_X || which == ADMM_BUF_X0 || which == ADMM_BUF_V || which == ADMM_BUF_P ||
+           which == ADMM_BUF_UC || which == ADMM_BUF_B || which == ADMM_BUF_MXT;
+}
+
 float4* buffer_ptr(AdmmB200* h, int which, int* rows) {
     DevScene& s = h->s;
     switch (which) {
@@ -1697,21 +1716,25 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
     return ADMM_OK;
 }
 
-__global__ void k_unpack_state(DevScene s, const float* __restrict__ stage, int has_v) {
+// Host-order staging buffer (row-major n x 3 positions, then velocities) <-> the
+// internal float4 state; perm[i] = the caller's row of internal vertex i (null: identity).
+__global__ void k_unpack_state(DevScene s, const float* __restrict__ stage, int has_v, const int* __restrict__ perm) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
-    const float4 x = make_float4(stage[3 * i], stage[3 * i + 1], stage[3 * i + 2], 0.f);
+    const int c = perm ? perm[i] : i;
+    const float4 x = make_float4(stage[3 * c], stage[3 * c + 1], stage[3 * c + 2], 0.f);
     s.x0[i] = x;
     s.x[i] = x;
-    if (has_v) s.v[i] = make_float4(stage[3 * s.n + 3 * i], stage[3 * s.n + 3 * i + 1], stage[3 * s.n + 3 * i + 2], 0.f);
+    if (has_v) s.v[i] = make_float4(stage[3 * s.n + 3 * c], stage[3 * s.n + 3 * c + 1], stage[3 * s.n + 3 * c + 2], 0.f);
 }
 
-__global__ void k_pack_state(DevScene s, float* __restrict__ stage) {
+__global__ void k_pack_state(DevScene s, float* __restrict__ stage, const int* __restrict__ perm) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.n) return;
+    const int c = perm ? perm[i] : i;
     const float4 x = s.x0[i], v = s.v[i];
-    stage[3 * i] = x.x; stage[3 * i + 1] = x.y; stage[3 * i + 2] = x.z;
-    stage[3 * s.n + 3 * i] = v.x; stage[3 * s.n + 3 * i + 1] = v.y; stage[3 * s.n + 3 * i + 2] = v.z;
+    stage[3 * c] = x.x; stage[3 * c + 1] = x.y; stage[3 * c + 2] = x.z;
+    stage[3 * s.n + 3 * c] = v.x; stage[3 * s.n + 3 * c + 1] = v.y; stage[3 * s.n + 3 * c + 2] = v.z;
 }
 
 int accumulate_timers(AdmmB200* h) {
@@ -1811,6 +1834,108 @@ int check_track_range(AdmmB200* h, int v0, int v1, int n_frames) {
     return ADMM_OK;
 }
 
+// The renumbered copy of a description (arrays owned here, pointers in d).
+struct RenumberedDesc {
+    AdmmB200Desc d;
+    std::vector<float> x0, v0, mass, cw, vmu;
+    std::vector<int32_t> fixed, tri, tet, bend, pin, st, se, sv;
+};
+
+// Every vertex index of the description in range (else no renumbering: create reports it).
+bool indices_in_range(const AdmmB200Desc* d) {
+    const int n = d->n_vert, nd = d->n_dyn;
+    if (n <= 0 || nd <= 0 || nd > n) return false;
+    auto ok = [](const int32_t* a, size_t cnt, int hi) {
+        if (cnt && !a) return false;
+        for (size_t k = 0; k < cnt; k++)
+            if (a[k] < 0 || a[k] >= hi) return false;
+        return true;
+    };
+    if (d->n_bend < 0 || (d->n_bend && (!d->bend_offsets || d->bend_offsets[d->n_bend] < 0))) return false;
+    return ok(d->tri_inds, 3 * (size_t)std::max(d->n_tri, 0), nd) && ok(d->tet_inds, 4 * (size_t)std::max(d->n_tet, 0), nd) &&
+           ok(d->bend_inds, d->n_bend ? (size_t)d->bend_offsets[d->n_bend] : 0, nd) &&
+           ok(d->pin_inds, (size_t)std::max(d->n_pin, 0), nd) && ok(d->surf_tris, 3 * (size_t)std::max(d->n_surf_tri, 0), n) &&
+           ok(d->surf_edges, 2 * (size_t)std::max(d->n_surf_edge, 0), n) &&
+           ok(d->surf_verts, (size_t)std::max(d->n_surf_vert, 0), n);
+}
+
+// Morton order (21 bits per axis) of the dynamic vertices' rest positions, ties by index;
+// static vertices keep their indices.
+void morton_order(const AdmmB200Desc* d, std::vector<int>& perm, std::vector<int>& iperm) {
+    const int n = d->n_vert, nd = d->n_dyn;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = 0; i < nd; i++)
+        for (int k = 0; k < 3; k++) {
+            lo[k] = std::min(lo[k], d->x0[3 * i + k]);
+            hi[k] = std::max(hi[k], d->x0[3 * i + k]);
+        }
+    const double ext = std::max({(double)hi[0] - lo[0], (double)hi[1] - lo[1], (double)hi[2] - lo[2], 1e-30});
+    auto spread = [](uint64_t v) {
+        v &= 0x1fffff;
+        v = (v | v << 32) & 0x1f00000000ffffULL;
+        v = (v | v << 16) & 0x1f0000ff0000ffULL;
+        v = (v | v << 8) & 0x100f00f00f00f00fULL;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+        v = (v | v << 2) & 0x1249249249249249ULL;
+        return v;
+    };
+    std::vector<std::pair<uint64_t, int>> key(nd);
+    for (int i = 0; i < nd; i++) {
+        uint64_t c[3];
+        for (int k = 0; k < 3; k++) {
+            const double t = ((double)d->x0[3 * i + k] - lo[k]) / ext;
+            c[k] = (uint64_t)std::min(2097151.0, std::max(0.0, t * 2097151.0));
+        }
+        key[i] = {spread(c[0]) | spread(c[1]) << 1 | spread(c[2]) << 2, i};
+    }
+    std::sort(key.begin(), key.end());
+    perm.resize(n);
+    iperm.resize(n);
+    for (int i = 0; i < nd; i++) perm[i] = key[i].second;
+    for (int i = nd; i < n; i++) perm[i] = i;
+    for (int i = 0; i < n; i++) iperm[perm[i]] = i;
+}
+
+// A copy of the description with the dynamic vertices in the order perm.
+void renumber(const AdmmB200Desc* in, const std::vector<int>& perm, const std::vector<int>& iperm, RenumberedDesc& r) {
+    const int n = in->n_vert;
+    r.d = *in;
+    auto per_vertex = [&](const float* a, std::vector<float>& out, int width) -> const float* {
+        if (!a) return nullptr;
+        out.resize((size_t)width * n);
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < width; k++) out[(size_t)width * i + k] = a[(size_t)width * perm[i] + k];
+        return out.data();
+    };
+    auto map_idx = [&](const int32_t* a, size_t cnt, std::vector<int32_t>& out) -> const int32_t* {
+        if (!a) return nullptr;
+        out.resize(cnt);
+        for (size_t k = 0; k < cnt; k++) out[k] = iperm[a[k]];
+        return out.data();
+    };
+    r.d.x0 = per_vertex(in->x0, r.x0, 3);
+    r.d.v0 = per_vertex(in->v0, r.v0, 3);
+    r.d.mass = per_vertex(in->mass, r.mass, 1);
+    r.d.contact_w = per_vertex(in->contact_w, r.cw, 1);
+    r.d.vert_mu = per_vertex(in->vert_mu, r.vmu, 1);
+    if (in->is_fixed) {
+        r.fixed.resize(n);
+        for (int i = 0; i < n; i++) r.fixed[i] = in->is_fixed[perm[i]];
+        r.d.is_fixed = r.fixed.data();
+    }
+    r.d.tri_inds = map_idx(in->tri_inds, 3 * (size_t)in->n_tri, r.tri);
+    r.d.tet_inds = map_idx(in->tet_inds, 4 * (size_t)in->n_tet, r.tet);
+    r.d.bend_inds = map_idx(in->bend_inds, in->n_bend ? (size_t)in->bend_offsets[in->n_bend] : 0, r.bend);
+    r.d.pin_inds = map_idx(in->pin_inds, (size_t)in->n_pin, r.pin);
+    r.d.surf_tris = map_idx(in->surf_tris, 3 * (size_t)in->n_surf_tri, r.st);
+    r.d.surf_edges = map_idx(in->surf_edges, 2 * (size_t)in->n_surf_edge, r.se);
+    if (in->surf_verts) {
+        map_idx(in->surf_verts, (size_t)in->n_surf_vert, r.sv);
+        std::sort(r.sv.begin(), r.sv.end());  // the detection's vertex queries in the new order
+        r.d.surf_verts = r.sv.data();
+    }
+}
+
 extern "C" {
 
 const char* admm_b200_errstr(int code) {
@@ -1826,7 +1951,36 @@ int admm_b200_create(const AdmmB200Desc* desc, int device, AdmmB200** out) {
     *out = nullptr;
     AdmmB200* h = new (std::nothrow) AdmmB200;
     if (!h) return ADMM_ERR_OOM;
-    const int rc = create_impl(desc, device, h);
+    const char* env = std::getenv("ADMM_B200_RENUMBER");
+    const bool want = desc->abi_version == ADMM_B200_ABI_VERSION && desc->backend_semantics == 0 && desc->x0 &&
+                      desc->mass && !(env && env[0] == '0' && env[1] == '\0') && indices_in_range(desc);
+    RenumberedDesc rd;
+    if (want) {
+        morton_order(desc, h->perm, h->iperm);
+        renumber(desc, h->perm, h->iperm, rd);
+    }
+    int rc = create_impl(want ? &rd.d : desc, device, h);
+    if (rc == ADMM_OK && want) {
+        rc = dupload(h, &h->d_perm, h->perm.data(), h->perm.size());
+        if (rc == ADMM_OK) {
+            // the global matrix in the caller's order, for admm_b200_system
+            const HostCsr& A = h->hostA;
+            const int nd = h->s.nd;
+            HostCsr& C = h->hostA_caller;
+            C.start.assign(nd + 1, 0);
+            for (int j = 0; j < nd; j++) {
+                const int i = h->iperm[j];
+                std::vector<std::pair<int, double>> e;
+                for (int k = A.start[i]; k < A.start[i + 1]; k++) e.push_back({h->perm[A.col[k]], A.val[k]});
+                std::sort(e.begin(), e.end());
+                for (auto& kv : e) {
+                    C.col.push_back(kv.first);
+                    C.val.push_back(kv.second);
+                }
+                C.start[j + 1] = (int)C.col.size();
+            }
+        }
+    }
     if (rc != ADMM_OK) {
         static thread_local std::string err;
         err = h->last_error;
@@ -1932,8 +2086,9 @@ int admm_b200_set_state(AdmmB200* h, const float* x, const float* v, int n) {
     CK(cudaSetDevice(h->device));
     std::vector<float4> hx(n), hv(n, make_float4(0.f, 0.f, 0.f, 0.f));
     for (int i = 0; i < n; i++) {
-        hx[i] = pack(x + 3 * i);
-        if (v) hv[i] = pack(v + 3 * i);
+        const int c = caller_of(h, i);
+        hx[i] = pack(x + 3 * c);
+        if (v) hv[i] = pack(v + 3 * c);
     }
     CK(cudaStreamSynchronize(h->stream));
     return upload_state(h, hx, hv);
@@ -1947,11 +2102,17 @@ int admm_b200_get_state(AdmmB200* h, float* x, float* v, int n) {
     CK(cudaStreamSynchronize(h->stream));
     if (x) {
         CK(cudaMemcpy(tmp.data(), h->s.x0, sizeof(float4) * n, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < n; i++) { x[3 * i] = tmp[i].x; x[3 * i + 1] = tmp[i].y; x[3 * i + 2] = tmp[i].z; }
+        for (int i = 0; i < n; i++) {
+            const int c = caller_of(h, i);
+            x[3 * c] = tmp[i].x; x[3 * c + 1] = tmp[i].y; x[3 * c + 2] = tmp[i].z;
+        }
     }
     if (v) {
         CK(cudaMemcpy(tmp.data(), h->s.v, sizeof(float4) * n, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < n; i++) { v[3 * i] = tmp[i].x; v[3 * i + 1] = tmp[i].y; v[3 * i + 2] = tmp[i].z; }
+        for (int i = 0; i < n; i++) {
+            const int c = caller_of(h, i);
+            v[3 * c] = tmp[i].x; v[3 * c + 1] = tmp[i].y; v[3 * c + 2] = tmp[i].z;
+        }
     }
     return ADMM_OK;
 }
@@ -2046,6 +2207,13 @@ int admm_b200_device_state(AdmmB200* h, void** x, void** v) {
     return ADMM_OK;
 }
 
+int admm_b200_vertex_order(AdmmB200* h, int32_t* order, int n) {
+    if (!h || !order) return ADMM_ERR_INVALID;
+    if (n != h->s.n) return fail(h, ADMM_ERR_INVALID, "n must equal n_vert");
+    for (int i = 0; i < n; i++) order[i] = caller_of(h, i);
+    return ADMM_OK;
+}
+
 int admm_b200_read_buffer(AdmmB200* h, int which, float* out, int n) {
     if (!h || !out) return ADMM_ERR_INVALID;
     int rows = 0;
@@ -2055,7 +2223,11 @@ int admm_b200_read_buffer(AdmmB200* h, int which, float* out, int n) {
     CK(cudaStreamSynchronize(h->stream));
     std::vector<float4> tmp(rows);
     CK(cudaMemcpy(tmp.data(), p, sizeof(float4) * rows, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < rows; i++) { out[3 * i] = tmp[i].x; out[3 * i + 1] = tmp[i].y; out[3 * i + 2] = tmp[i].z; }
+    const bool pv = per_vertex_buffer(which);
+    for (int i = 0; i < rows; i++) {
+        const int c = pv ? caller_of(h, i) : i;
+        out[3 * c] = tmp[i].x; out[3 * c + 1] = tmp[i].y; out[3 * c + 2] = tmp[i].z;
+    }
     return ADMM_OK;
 }
 
@@ -2067,7 +2239,8 @@ int admm_b200_write_buffer(AdmmB200* h, int which, const float* in, int n) {
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     std::vector<float4> tmp(rows);
-    for (int i = 0; i < rows; i++) tmp[i] = pack(in + 3 * i);
+    const bool pv = per_vertex_buffer(which);
+    for (int i = 0; i < rows; i++) tmp[i] = pack(in + 3 * (pv ? caller_of(h, i) : i));
     CK(cudaMemcpy(p, tmp.data(), sizeof(float4) * rows, cudaMemcpyHostToDevice));
     if (which == ADMM_BUF_Z || which == ADMM_BUF_UE) {
         // keep y = z - Ue consistent for the right-hand side
@@ -2139,7 +2312,7 @@ int admm_b200_detect_host(AdmmB200* h, const float* x, int n, int* count) {
     if (n != h->s.n) return fail(h, ADMM_ERR_INVALID, "n must equal n_vert");
     CK(cudaSetDevice(h->device));
     std::vector<float4> hx(n);
-    for (int i = 0; i < n; i++) hx[i] = pack(x + 3 * i);
+    for (int i = 0; i < n; i++) hx[i] = pack(x + 3 * caller_of(h, i));
     CK(cudaStreamSynchronize(h->stream));
     CK(cudaMemcpy(h->s.x, hx.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
     return admm_b200_detect(h, count);
@@ -2166,7 +2339,11 @@ int admm_b200_contacts(AdmmB200* h, int32_t* pairs, float* bary4, float* normal3
     if (count) *count = nc;
     const int k = std::min(nc, std::max(cap, 0));
     if (k == 0) return ADMM_OK;
-    if (pairs) CK(cudaMemcpy(pairs, h->s.pairs, sizeof(int4) * k, cudaMemcpyDeviceToHost));
+    if (pairs) {
+        CK(cudaMemcpy(pairs, h->s.pairs, sizeof(int4) * k, cudaMemcpyDeviceToHost));
+        if (!h->perm.empty())
+            for (int i = 0; i < 4 * k; i++) pairs[i] = h->perm[pairs[i]];
+    }
     std::vector<float4> tmp(k);
     if (bary4) CK(cudaMemcpy(bary4, h->s.bary, sizeof(float4) * k, cudaMemcpyDeviceToHost));
     if (normal3 || gap) {
@@ -2251,9 +2428,9 @@ int admm_b200_step_host(AdmmB200* h, const float* x_in, const float* v_in, float
     const size_t bytes = sizeof(float) * 3 * (size_t)n;
     CK(cudaMemcpyAsync(h->stage, x_in, bytes, cudaMemcpyHostToDevice, h->stream));
     if (v_in) CK(cudaMemcpyAsync(h->stage + 3 * (size_t)n, v_in, bytes, cudaMemcpyHostToDevice, h->stream));
-    k_unpack_state<<<blocks(n, 256), 256, 0, h->stream>>>(h->s, h->stage, v_in ? 1 : 0);
+    k_unpack_state<<<blocks(n, 256), 256, 0, h->stream>>>(h->s, h->stage, v_in ? 1 : 0, h->d_perm);
     TRY(launch_substep(h));
-    k_pack_state<<<blocks(n, 256), 256, 0, h->stream>>>(h->s, h->stage);
+    k_pack_state<<<blocks(n, 256), 256, 0, h->stream>>>(h->s, h->stage, h->d_perm);
     if (x_out) CK(cudaMemcpyAsync(x_out, h->stage, bytes, cudaMemcpyDeviceToHost, h->stream));
     if (v_out) CK(cudaMemcpyAsync(v_out, h->stage + 3 * (size_t)n, bytes, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
@@ -2309,7 +2486,7 @@ int admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, float
 
 int admm_b200_system(AdmmB200* h, int32_t* start, int32_t* col, float* val, float* diag) {
     if (!h) return ADMM_ERR_INVALID;
-    const HostCsr& A = h->hostA;
+    const HostCsr& A = h->perm.empty() ? h->hostA : h->hostA_caller;
     const int nnz = (int)A.col.size();
     if (!start) return nnz;
     if (!col || !val || !diag) return ADMM_ERR_INVALID;
@@ -2318,7 +2495,7 @@ int admm_b200_system(AdmmB200* h, int32_t* start, int32_t* col, float* val, floa
         col[k] = A.col[k];
         val[k] = (float)A.val[k];
     }
-    for (size_t i = 0; i < h->hostAdiag.size(); i++) diag[i] = h->hostAdiag[i];
+    for (size_t i = 0; i < h->hostAdiag.size(); i++) diag[caller_of(h, (int)i)] = h->hostAdiag[i];
     return nnz;
 }
 
@@ -2328,7 +2505,10 @@ int admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd) {
     CK(cudaSetDevice(h->device));
     CK(cudaStreamSynchronize(h->stream));
     if (!h->pcg_blocks) TRY(dalloc(h, &h->pcg_blocks, 9 * (size_t)nd));
-    CK(cudaMemcpy(h->pcg_blocks, blocks9, sizeof(float) * 9 * (size_t)nd, cudaMemcpyHostToDevice));
+    std::vector<float> bl(9 * (size_t)nd);
+    for (int i = 0; i < nd; i++)
+        for (int k = 0; k < 9; k++) bl[9 * (size_t)i + k] = blocks9[9 * (size_t)caller_of(h, i) + k];
+    CK(cudaMemcpy(h->pcg_blocks, bl.data(), sizeof(float) * 9 * (size_t)nd, cudaMemcpyHostToDevice));
     // the step graph holds the preconditioner pointer: capture it again
     if (h->step_exec) {
         cudaGraphExecDestroy(h->step_exec);
@@ -2348,8 +2528,9 @@ int admm_b200_set_learned(AdmmB200* h, int sweeps, const float* omega, const flo
     CK(cudaStreamSynchronize(h->stream));
     std::vector<float> mv(nd), th(nd, 0.f);
     for (int i = 0; i < nd; i++) {
-        mv[i] = m ? m[i] : 1.f / h->hostAdiag[i];
-        if (theta) th[i] = theta[i];
+        const int c = caller_of(h, i);
+        mv[i] = m ? m[c] : 1.f / h->hostAdiag[i];
+        if (theta) th[i] = theta[c];
         if (!std::isfinite(mv[i]) || !std::isfinite(th[i])) return fail(h, ADMM_ERR_INVALID, "m/theta");
     }
     CK(cudaMemcpy(const_cast<float*>(h->learn.minv), mv.data(), sizeof(float) * nd, cudaMemcpyHostToDevice));
@@ -2407,9 +2588,10 @@ int admm_b200_record_global(AdmmB200* h, int iteration, float* b, float* x_cur, 
     for (int k = 0; k < 3; k++) {
         CK(cudaMemcpy(t.data(), srcs[k], sizeof(float4) * nd, cudaMemcpyDeviceToHost));
         for (int i = 0; i < nd; i++) {
-            outs[k][3 * i] = t[i].x;
-            outs[k][3 * i + 1] = t[i].y;
-            outs[k][3 * i + 2] = t[i].z;
+            const int c = caller_of(h, i);
+            outs[k][3 * c] = t[i].x;
+            outs[k][3 * c + 1] = t[i].y;
+            outs[k][3 * c + 2] = t[i].z;
         }
     }
     return ADMM_OK;

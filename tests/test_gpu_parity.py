@@ -705,3 +705,52 @@ print(json.dumps(cs))
         outs.append((json.loads(r.stdout.strip().splitlines()[-1]), np.load(path)))
     assert outs[0][0] == outs[1][0] and max(outs[0][0]) > 0, (outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_vertex_renumbering_is_invisible_to_the_caller():
+    """The library stores the dynamic vertices in Morton order; with ADMM_B200_RENUMBER=0 it
+    keeps the caller's order.  Through the C ABI both give the same contact pair set and the
+    same substeps up to FP32 summation order, and the order is a permutation that moves only
+    dynamic vertices."""
+    import os
+    sc = scene.cube_on_ground(10, drop=0.0)
+    sc.params.ell_lanes = 4
+    sc.params.dcd_interval = sc.params.admm_max_iter  # one detection per substep: identical pair sets
+    v0 = np.zeros_like(sc.verts)
+    v0[:sc.n_dyn, 1] = -4.0
+    x0 = sc.verts.copy()
+    x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.03
+    hr = B.Handle(sc)
+    old = os.environ.get("ADMM_B200_RENUMBER")
+    os.environ["ADMM_B200_RENUMBER"] = "0"
+    try:
+        hi = B.Handle(sc)
+    finally:
+        if old is None:
+            del os.environ["ADMM_B200_RENUMBER"]
+        else:
+            os.environ["ADMM_B200_RENUMBER"] = old
+    order = hr.vertex_order()
+    assert sorted(order.tolist()) == list(range(sc.n_vert))
+    assert np.array_equal(order[sc.n_dyn:], np.arange(sc.n_dyn, sc.n_vert))
+    assert not np.array_equal(order[:sc.n_dyn], np.arange(sc.n_dyn))
+    assert np.array_equal(hi.vertex_order(), np.arange(sc.n_vert))
+    for h in (hr, hi):
+        h.set_state(x0, v0)
+    xd = x0.copy()
+    xd[:sc.n_dyn, 1] -= 0.025
+    pr = sorted(map(tuple, (hr.detect(xd), hr.contacts()["pairs"])[1].tolist()))
+    pi = sorted(map(tuple, (hi.detect(xd), hi.contacts()["pairs"])[1].tolist()))
+    assert pr == pi and len(pr) > 0
+    for h in (hr, hi):
+        h.set_state(x0, v0)
+    ext = np.ptp(x0[:sc.n_dyn], axis=0).max()
+    for k in range(3):
+        sr = hr.step(1)
+        si = hi.step(1)
+        assert sr["n_contacts"] == si["n_contacts"]
+        err = np.abs(hr.get_state()[0] - hi.get_state()[0]).max() / ext
+        assert err <= 1e-4, (k, err)
+        hi.set_state(*hr.get_state())
+        hi.write(B.BUF_UE, hr.read(B.BUF_UE))
+        hi.write(B.BUF_UC, hr.read(B.BUF_UC))
