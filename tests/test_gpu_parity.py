@@ -578,8 +578,11 @@ def test_batch_with_per_body_friction_parity():
     """A batch of independent bodies (cubes and ellipsoids, per-body E and friction) in one scene,
     with per-vertex friction coefficients: the first substep free against the FP64 oracle
     (1e-5), then three substeps one at a time from the FP32 oracle's state against it (equal
-    contact counts, 1e-4): from the second frame on, contacts at the edge of the thickness
-    band decide differently in FP32 and FP64.  One detection per substep."""
+    contact counts; every vertex but at most 0.1% of them within 1e-4, none beyond 5e-3).  One
+    detection per substep.  The outliers are the scene's, not the kernels': the FP32 oracle run
+    on the same state in another vertex numbering moves one vertex by 1.3e-3 in one substep
+    (a contact on the edge of its active/separating switch over the ADMM iterations) while every
+    other vertex stays within 1e-5 (test_oracle_order.py)."""
     sc = scene.batch_bodies(6, seed=3, vmin=300, vmax=3000)
     assert sc.vert_mu is not None and len(np.unique(sc.vert_mu[:sc.n_dyn])) > 1
     # one detection per substep: identical pair sets on both sides from a shared state (with
@@ -612,8 +615,9 @@ def test_batch_with_per_body_friction_parity():
         sg = h.step(1)
         so = o32.step(1)
         assert sg["n_contacts"] == so["n_contacts"], (k, sg["n_contacts"], so["n_contacts"])
-        err = np.abs(h.get_state()[0] - o32.read(B.BUF_X0)).max() / ext
-        assert err <= 1e-4, (k, err)
+        d = np.abs(h.get_state()[0] - o32.read(B.BUF_X0)).max(axis=1)[:sc.n_dyn] / ext
+        n_out = int((d > 1e-4).sum())
+        assert n_out <= max(2, sc.n_dyn // 1000) and d.max() <= 5e-3, (k, n_out, d.max())
         seen = min(seen, sg["n_contacts"])
     assert seen > 0
 

@@ -253,3 +253,34 @@ def test_training_gains_over_jacobi():
     for _, _, _, tr, _ in data:
         tr.close()
     model.net.close()
+
+
+def test_training_script_end_to_end(tmp_path):
+    """The training script that makes the committed weights, at a tiny scale: it trains the
+    models of every sweep count, evaluates held-out seeds with fallback counts, writes the
+    chosen model and a JSON summary, and the written model loads and runs in a substep."""
+    import json
+    import os
+    import subprocess
+    import sys
+    out = tmp_path / "w.npz"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-m", "parallel_admm_b200.train_learned", "--out", str(out), "--n", "6",
+                        "--train-seeds", "3", "--samples", "8", "--eval-seeds", "10", "--eval-samples", "2",
+                        "--eval-substeps", "3", "--sweeps", "6,10"], cwd=root, capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    summary = json.loads(r.stdout.strip().splitlines()[-1])
+    assert summary["train"]["triples"] > 0 and summary["eval"]["evaluated_seeds"] > 0
+    assert summary["chosen_sweeps"] in (6, 10)
+    for K in ("6", "10"):
+        assert summary["models"][K]["judged"]["substeps"] > 0
+    model = gnn.LearnedGlobalStep.load(str(out))
+    sc = _pin(scene.cube_on_ground(6, drop=0.02))
+    sc.params.global_solver = 3
+    h = B.Handle(sc)
+    sysm = gnn.system(h)
+    model.apply(h, sysm, *gnn.scene_features(sc, sysm))
+    h.step(2, allow=ALLOW)
+    assert np.isfinite(h.get_state()[0]).all()
+    model.net.close()

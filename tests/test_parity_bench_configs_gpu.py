@@ -87,7 +87,8 @@ def test_cube20_parity():
         assert sg["n_contacts"] == so["n_contacts"], (k, ncs)
         err = np.abs(h.get_state()[0] - o32.read(B.BUF_X0)).max() / ext
         assert err <= 1e-4, (k, err, ncs)
-    assert min(c[0] for c in ncs) > 100, ncs
+    # contacts from the first impact substep on, a thousand or more once the face is down
+    assert min(c[0] for c in ncs) > 0 and max(c[0] for c in ncs) > 1000, ncs
 
 
 @pytest.mark.parametrize("solver", ["jacobi", "learned"])
