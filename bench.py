@@ -336,9 +336,8 @@ def run_arm(args, B, R, sc, local, world, arm, flush, nnz):
         st1 = h.learned_stats()
         d = {k: st1[k] - st0[k] for k in st1}
         out["learned"] = d
-        # a substep that fell back also ran the plain graph: count its launches
-        if d["fallbacks"]:
-            out["launches"] += d["fallbacks"] * launches // max(args.steps, 1)
+        # every failed learned solve ran the plain solve in its IF node: count those kernels
+        out["launches"] += d["fallbacks"] * h.kernels_fallback()
     return out
 
 

@@ -358,15 +358,18 @@ int  admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd);
  * warm start in a substep's first global step).  m [nd] scales the residual per
  * dynamic vertex (NULL: 1 / a_ii), theta [nd] is the warm-start coefficient (NULL:
  * 0); both come from the learned network (parallel_admm_b200/gnn.py).  Every solve is
- * judged: a solve whose |b - A x_K| exceeds |b - A x_0| fails, and a substep with a
- * failed solve is run again from its starting state with the plain Jacobi global
- * step.  A learned substep therefore synchronises the stream once (to read the
- * judge's count).  sweeps <= 32. */
+ * judged on the device: a solve whose |b - A x_K| exceeds |b - A x_0| (and 1e-5 |b|)
+ * fails and is replaced by the plain one (x as received, then jacobi_iter Jacobi
+ * sweeps), in a conditional node of the substep graph: no host synchronisation.
+ * sweeps <= 32. */
 int  admm_b200_set_learned(AdmmB200* h, int sweeps, const float* omega, const float* beta, const float* m,
                            const float* theta, int nd);
-/* out4: substeps run with the learned step, substeps run again with plain Jacobi,
- * learned solves judged, learned solves that failed. */
+/* out4: substeps run with the learned step, solves replaced by the plain Jacobi
+ * solve, learned solves judged, learned solves that failed (= out4[1]). */
 int  admm_b200_learned_stats(AdmmB200* h, int64_t* out4);
+/* Kernels the plain solve that replaces a failed learned solve launches (for launch
+ * accounting: a substep launches kernels_per_step plus this many per replaced solve). */
+int  admm_b200_kernels_fallback(AdmmB200* h, int* n);
 /* Training data: runs one substep (eagerly, with the handle's global solver) and
  * copies out, for its global step number `iteration` (1 .. admm_max_iter - 1,
  * counted from 0 over the substep), the right-hand side b, the iterate x_cur the

@@ -370,7 +370,7 @@ struct Oracle {
     // learned global step (global_solver 3): sweeps, coefficients, per-vertex m and theta
     int learn_K = 0;
     std::vector<R> learn_omega, learn_beta, learn_m, learn_theta, xl;
-    int learn_fail = 0;
+    bool warm_on = true;  // the warm start is still on in this substep (adaptive restart)
     long long learn_substeps = 0, learn_fallbacks = 0, learn_solves = 0, learn_failed = 0;
     // matrices
     Csr D;        // m x nd
@@ -925,7 +925,10 @@ struct Oracle {
     // Learned global step (the GPU's k_rhs_learn / k_lsweep / k_ljudge / k_ldecide):
     // warm start x += theta (x - xl) unless first, xl <- x received; K sweeps
     // x_{k+1} = x_k + omega_k m (b - A x_k) + beta_k (x_k - x_{k-1}); the solve fails
-    // when |b - A x_K|^2 > |b - A x_0|^2 and |b - A x_K| > 1e-5 |b| (FP64 sums).
+    // when |b - A x_K|^2 > |b - A x_c|^2 (x_c the received iterate) and |b - A x_K| >
+    // 1e-5 |b| (FP64 sums), and a failed solve is replaced by the plain one: x <- x_c,
+    // jacobi_iter sweeps.  The warm start restarts adaptively: once a warm start raised
+    // the residual (|b - A x_0| > |b - A x_c|) it stays off until the next substep.
     void learned_solve(bool first) {
         const int N = 3 * nd;
         if (learn_K == 0) {  // defaults: the Jacobi sweep
@@ -937,22 +940,33 @@ struct Oracle {
             learn_theta.assign(nd, R(0));
         }
         if ((int)xl.size() != N) xl.assign(N, R(0));
+        if (first) warm_on = true;
+        const bool extrap = !first && warm_on;
         for (int i = 0; i < nd; i++)
             for (int k = 0; k < 3; k++) {
                 const R xi = x[3 * i + k], xo = xl[3 * i + k];
                 xl[3 * i + k] = xi;
-                if (!first) x[3 * i + k] = learn_theta[i] * (xi - xo) + xi;
+                if (extrap) x[3 * i + k] = learn_theta[i] * (xi - xo) + xi;
             }
         std::vector<R> xp(x.begin(), x.begin() + N), xn(N), ax(N);
-        double r0 = 0, rK = 0, bb = 0;
+        double r0 = 0, rx0 = 0, rK = 0, bb = 0;
         for (int q = 0; q < N; q++) bb += (double)b[q] * (double)b[q];
+        if (extrap) {  // the received iterate's residual (x_0 = x_c without a warm start)
+            std::vector<R> xc(x.begin(), x.end()), axc(N);
+            std::copy(xl.begin(), xl.end(), xc.begin());
+            apply_A(xc, axc);
+            for (int q = 0; q < N; q++) {
+                const R r = b[q] - axc[q];
+                r0 += (double)r * (double)r;
+            }
+        }
         for (int s = 0; s < learn_K; s++) {
             apply_A(x, ax);
             for (int i = 0; i < nd; i++)
                 for (int k = 0; k < 3; k++) {
                     const int q = 3 * i + k;
                     const R r = b[q] - ax[q];
-                    if (s == 0) r0 += (double)r * (double)r;
+                    if (s == 0) rx0 += (double)r * (double)r;
                     const R bt = s == 0 ? R(0) : learn_beta[s];
                     xn[q] = (learn_omega[s] * learn_m[i]) * r + (bt * (x[q] - xp[q]) + x[q]);
                 }
@@ -966,10 +980,15 @@ struct Oracle {
             const R r = b[q] - ax[q];
             rK += (double)r * (double)r;
         }
+        if (!extrap) r0 = rx0;
+        // adaptive restart: a warm start that raised the residual stays off for the substep
+        if (extrap && rx0 > r0) warm_on = false;
         learn_solves++;
         if (!(rK <= r0 || rK <= 1e-10 * bb)) {
-            learn_fail++;
             learn_failed++;
+            learn_fallbacks++;
+            std::copy(xl.begin(), xl.end(), x.begin());
+            jacobi(jacobi_iter);
         }
     }
 
@@ -1006,21 +1025,11 @@ struct Oracle {
             }
     }
 
-    // A substep; with the learned global step, judged: a substep with a failed
-    // learned solve is run again from its starting state with the Jacobi sweeps.
+    // A substep (with the learned global step: every solve judged, a failed one replaced).
     int step() {
         if (global_solver != 3) return step_once(false);
-        const std::vector<R> sx0 = x0, sv = v, sue = Ue, suc = Uc;
-        learn_fail = 0;
-        const int it = step_once(true);
         learn_substeps++;
-        if (learn_fail == 0) return it;
-        x0 = sx0;
-        v = sv;
-        Ue = sue;
-        Uc = suc;
-        learn_fallbacks++;
-        return step_once(false);
+        return step_once(true);
     }
 
     // ADMMImplGPU::step (admm_impl_gpu.cu:256-344)

@@ -196,6 +196,7 @@ def lib():
             "admm_b200_last_step_device_ms": (ctypes.c_int, [vp, _f]),
             "admm_b200_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
             "admm_b200_kernels_per_step": (ctypes.c_int, [vp, _i]),
+            "admm_b200_kernels_fallback": (ctypes.c_int, [vp, _i]),
             "admm_b200_step_host": (ctypes.c_int, [vp, _f, _f, _f, _f, ctypes.c_int]),
             "admm_b200_phase_times": (ctypes.c_int, [vp, _d, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]),
             "admm_b200_set_probe": (ctypes.c_int, [vp, ctypes.c_int]),
@@ -232,7 +233,7 @@ def exported_symbols():
         "admm_b200_contact_step", "admm_b200_detect", "admm_b200_detect_host", "admm_b200_contacts",
         "admm_b200_contact_count", "admm_b200_max_slots", "admm_b200_peak_contact_count",
         "admm_b200_clear_contacts", "admm_b200_residuals", "admm_b200_last_step_device_ms",
-        "admm_b200_set_profiling", "admm_b200_kernels_per_step", "admm_b200_step_host",
+        "admm_b200_set_profiling", "admm_b200_kernels_per_step", "admm_b200_kernels_fallback", "admm_b200_step_host",
         "admm_b200_phase_times", "admm_b200_set_probe", "admm_b200_probe_time", "admm_b200_tuning",
         "admm_b200_jacobi_noalloc", "admm_b200_global_mode", "admm_b200_set_preconditioner",
         "admm_b200_set_rigid_track", "admm_b200_set_point_track", "admm_b200_clear_tracks",
@@ -375,6 +376,12 @@ class Handle:
     def kernels_per_step(self) -> int:
         n = ctypes.c_int32()
         self.check(lib().admm_b200_kernels_per_step(self.h, ctypes.byref(n)), "kernels_per_step")
+        return n.value
+
+    def kernels_fallback(self) -> int:
+        """Kernels of the plain solve that replaces a failed learned solve (0 unless learned)."""
+        n = ctypes.c_int32()
+        self.check(lib().admm_b200_kernels_fallback(self.h, ctypes.byref(n)), "kernels_fallback")
         return n.value
 
     def step_host(self, x_in: np.ndarray, v_in: Optional[np.ndarray], x_out: np.ndarray,
@@ -627,6 +634,12 @@ class BVHB200:
     def contact_count(self) -> int:
         n = ctypes.c_int32()
         self._h.check(lib().admm_b200_contact_count(self._h.h, ctypes.byref(n)), "contact_count")
+        return n.value
+
+    def kernels_fallback(self) -> int:
+        """Kernels of the plain solve that replaces a failed learned solve (0 unless learned)."""
+        n = ctypes.c_int32()
+        self.check(lib().admm_b200_kernels_fallback(self.h, ctypes.byref(n)), "kernels_fallback")
         return n.value
 
     def step_host(self, x_in: np.ndarray, v_in: Optional[np.ndarray], x_out: np.ndarray,

@@ -72,11 +72,10 @@ struct AdmmB200 {
     LearnDev learn;
     int learn_sweeps = 0;
     std::vector<float> learn_omega, learn_beta;
-    cudaGraphExec_t plain_exec = nullptr;   // the same substep with the Jacobi global step (fallback)
-    float4 *sv_x0 = nullptr, *sv_v = nullptr, *sv_ue = nullptr, *sv_uc = nullptr;  // substep start state
-    int* sv_anim = nullptr;
-    int* fail_host = nullptr;       // pinned copy of learn.fail
-    int64_t learn_substeps = 0, learn_fallbacks = 0;
+    int* fail_host = nullptr;       // pinned copy of learn.fail (eager substeps)
+    int64_t learn_substeps = 0;
+    int kernels_fallback = 0;       // kernels of the plain solve that replaces a failed learned one
+    cudaStream_t if_stream = nullptr;  // capture of the bodies of the fallback IF nodes
     bool force_plain = false;       // enqueue the Jacobi global step whatever global_solver says
     // Vertex renumbering: the library stores the dynamic vertices in the Morton order of
     // their rest positions (spatially close vertices at close indices, so the gathers of the
@@ -578,9 +577,78 @@ void enqueue_pcg(AdmmB200* h, int iters) {
 #undef PCG_T
 }
 
+// The decision on a learned solve and the plain solve that replaces a failed one:
+// x <- x as received (L.xl), then the jacobi_iter Jacobi sweeps on the same b.  In a
+// graph they are the body of an IF node after k_ldecide, which sets its condition
+// (inside the residual-tolerance WHILE body the IF node is nested in it); eagerly,
+// the host reads the decision (one stream synchronisation per solve).
+void enqueue_learned_decide(AdmmB200* h) {
+    DevScene& s = h->s;
+    LearnDev& L = h->learn;
+    const int vb = blocks(s.nd, kVertThreads);
+    cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamGetCaptureInfo(h->cstream, &cst, nullptr, &g, nullptr, nullptr);
+    if (e != cudaSuccess) {
+        if (h->enqueue_rc == ADMM_OK) h->enqueue_rc = fail(h, ADMM_ERR_CUDA, cudaGetErrorString(e));
+        return;
+    }
+    if (cst != cudaStreamCaptureStatusActive) {
+        LAUNCH(k_ldecide, 1, 256, L, cudaGraphConditionalHandle(0), 0);
+        int failed = 0;
+        if (cudaMemcpyAsync(h->fail_host, L.fail, sizeof(int), cudaMemcpyDeviceToHost, h->cstream) == cudaSuccess &&
+            cudaStreamSynchronize(h->cstream) == cudaSuccess)
+            failed = *h->fail_host;
+        if (failed) {
+            LAUNCH(k_copy_dyn, vb, kVertThreads, s, (const float4*)L.xl, s.x);
+            enqueue_jacobi(h, h->jac_iter);
+        }
+        return;
+    }
+    cudaGraphConditionalHandle cond;
+    e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault);
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    if (e == cudaSuccess) {
+        LAUNCH(k_ldecide, 1, 256, L, cond, 1);
+        e = cudaStreamGetCaptureInfo(h->cstream, &cst, nullptr, &g, &deps, &ndeps);
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
+    if (e != cudaSuccess) {
+        if (h->enqueue_rc == ADMM_OK) h->enqueue_rc = fail(h, ADMM_ERR_CUDA, std::string("fallback IF node: ") + cudaGetErrorString(e));
+        return;
+    }
+    cudaStream_t parent = h->cstream;
+    const bool was_in_body = h->in_body;
+    const int before = h->launch_counter;
+    h->cstream = h->if_stream;
+    h->in_body = true;
+    e = cudaStreamBeginCaptureToGraph(h->cstream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        LAUNCH(k_copy_dyn, vb, kVertThreads, s, (const float4*)L.xl, s.x);
+        enqueue_jacobi(h, h->jac_iter);
+        cudaGraph_t bg = nullptr;
+        e = cudaStreamEndCapture(h->cstream, &bg);
+    }
+    h->kernels_fallback = h->launch_counter - before;
+    h->launch_counter = before;
+    h->in_body = was_in_body;
+    h->cstream = parent;
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(h->cstream, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess && h->enqueue_rc == ADMM_OK)
+        h->enqueue_rc = fail(h, ADMM_ERR_CUDA, std::string("fallback IF body: ") + cudaGetErrorString(e));
+}
+
 // The learned global step: right-hand side with the warm start, learn_sweeps
 // second-order sweeps (x_k in {x, jac0, jac1}[k % 3]), the judge's pass that
-// leaves x_K in x, and the decision.
+// leaves x_K in x, and the decision with its fallback.
 void enqueue_learned(AdmmB200* h, bool save_prev, bool first) {
     DevScene& s = h->s;
     LearnDev& L = h->learn;
@@ -607,10 +675,10 @@ void enqueue_learned(AdmmB200* h, bool save_prev, bool first) {
         float4* dst = buf[(k + 1) % 3];                                                                    \
         if (k == 0)                                                                                        \
             LAUNCH_P(ADMM_KERNEL_JACOBI, (k_lsweep<T, true>), L.blocks, kVertThreads, s, L, src, prv, dst, \
-                     h->learn_omega[k], h->learn_beta[k]);                                                 \
+                     h->learn_omega[k], h->learn_beta[k], first ? (const float4*)nullptr : (const float4*)L.xl); \
         else                                                                                               \
             LAUNCH_P(ADMM_KERNEL_JACOBI, (k_lsweep<T, false>), L.blocks, kVertThreads, s, L, src, prv, dst, \
-                     h->learn_omega[k], h->learn_beta[k]);                                                 \
+                     h->learn_omega[k], h->learn_beta[k], (const float4*)nullptr);                          \
     }                                                                                                      \
     LAUNCH(k_ljudge<T>, L.blocks, kVertThreads, s, L, (const float4*)buf[K % 3]);
     switch (s.A.lanes) {
@@ -620,7 +688,7 @@ void enqueue_learned(AdmmB200* h, bool save_prev, bool first) {
         default: LS_CASE(8) break;
     }
 #undef LS_CASE
-    LAUNCH(k_ldecide, 1, 256, L);
+    enqueue_learned_decide(h);
 }
 
 // Copies of one global step's inputs for admm_b200_record_global (eager only):
@@ -1130,7 +1198,7 @@ int build_step_graph(AdmmB200* h) {
     if (rc == ADMM_OK || !h->persist) return rc;
     cudaStreamCaptureStatus cst;
     cudaGraph_t g = nullptr;
-    for (cudaStream_t st : {h->body_stream, h->stream})
+    for (cudaStream_t st : {h->if_stream, h->body_stream, h->stream})
         if (cudaStreamIsCapturing(st, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
             cudaStreamEndCapture(st, &g);
             if (g) cudaGraphDestroy(g);
@@ -1145,112 +1213,24 @@ int build_step_graph(AdmmB200* h) {
     return build_step_graph_once(h);
 }
 
-// The substep graph with the plain Jacobi global step, the fallback of a
-// learned substep whose judge failed (built once, beside the learned graph).
-int build_plain_graph(AdmmB200* h) {
-    if (h->plain_exec) return ADMM_OK;
-    cudaGraphExec_t keep = h->step_exec;
-    const int kps = h->kernels_per_step, kb = h->kernels_body, probe = h->probe_kernel;
-    const int pu = h->probe_used, pvu = h->pev_used, ph = h->phase;
-    h->step_exec = nullptr;
-    h->force_plain = true;
-    h->probe_kernel = 0;
-    const int rc = build_step_graph(h);
-    h->plain_exec = h->step_exec;
-    h->step_exec = keep;
-    h->force_plain = false;
-    h->probe_kernel = probe;
-    h->kernels_per_step = kps;
-    h->kernels_body = kb;
-    h->probe_used = pu;
-    h->pev_used = pvu;
-    h->phase = ph;
-    return rc;
-}
-
 bool learned_active(const AdmmB200* h) { return h->global_solver == 3; }
 
-// Substep starting state of a learned substep (what a re-run needs).
-int save_substep_state(AdmmB200* h) {
-    DevScene& s = h->s;
-    if (!h->sv_x0) {
-        TRY(dalloc(h, &h->sv_x0, s.n));
-        TRY(dalloc(h, &h->sv_v, s.n));
-        TRY(dalloc(h, &h->sv_ue, s.m));
-        TRY(dalloc(h, &h->sv_uc, s.nd));
-        TRY(dalloc(h, &h->sv_anim, 1));
-        CK(cudaHostAlloc((void**)&h->fail_host, sizeof(int), cudaHostAllocDefault));
-    }
-    CK(cudaMemcpyAsync(h->sv_x0, s.x0, sizeof(float4) * s.n, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->sv_v, s.v, sizeof(float4) * s.n, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->sv_ue, s.ue, sizeof(float4) * s.m, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->sv_uc, s.uc, sizeof(float4) * s.nd, cudaMemcpyDeviceToDevice, h->stream));
-    if (h->anim.counter) CK(cudaMemcpyAsync(h->sv_anim, h->anim.counter, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemsetAsync(h->learn.fail, 0, sizeof(int), h->stream));
-    return ADMM_OK;
-}
-
-int restore_substep_state(AdmmB200* h) {
-    DevScene& s = h->s;
-    CK(cudaMemcpyAsync(s.x0, h->sv_x0, sizeof(float4) * s.n, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(s.v, h->sv_v, sizeof(float4) * s.n, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(s.ue, h->sv_ue, sizeof(float4) * s.m, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(s.uc, h->sv_uc, sizeof(float4) * s.nd, cudaMemcpyDeviceToDevice, h->stream));
-    if (h->anim.counter) CK(cudaMemcpyAsync(h->anim.counter, h->sv_anim, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
-    return ADMM_OK;
-}
-
-// Failed learned solves of the substep just enqueued (synchronises the stream).
-int read_learn_fail(AdmmB200* h, int* failed) {
-    CK(cudaMemcpyAsync(h->fail_host, h->learn.fail, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    *failed = *h->fail_host;
-    return ADMM_OK;
-}
-
-// One substep from the graphs: a learned substep is judged and, when one of its
-// global solves failed to reduce the residual, run again from its starting state
-// with the plain Jacobi global step.
+// One substep from its graph (a learned substep judges and replaces its failed
+// solves inside the graph).
 int launch_substep(AdmmB200* h) {
-    if (!learned_active(h)) {
-        CK(cudaGraphLaunch(h->step_exec, h->stream));
-        return ADMM_OK;
-    }
-    TRY(build_plain_graph(h));
-    TRY(save_substep_state(h));
     CK(cudaGraphLaunch(h->step_exec, h->stream));
-    int failed = 0;
-    TRY(read_learn_fail(h, &failed));
-    h->learn_substeps++;
-    if (failed) {
-        TRY(restore_substep_state(h));
-        CK(cudaGraphLaunch(h->plain_exec, h->stream));
-        h->learn_fallbacks++;
-    }
+    if (learned_active(h)) h->learn_substeps++;
     return ADMM_OK;
 }
 
-// The eager (profiling / recording) substep, judged the same way.
+// The eager (profiling / recording) substep.
 int run_substep_eager(AdmmB200* h) {
     h->cstream = h->stream;
-    const bool learned = learned_active(h) && h->rec_target < 0;
-    if (learned) TRY(save_substep_state(h));
     if (h->residual_tol > 0.f) TRY(run_step_tol_eager(h, h->residual_tol));
     else enqueue_step(h);
     CK(cudaGetLastError());
-    if (learned) {
-        int failed = 0;
-        TRY(read_learn_fail(h, &failed));
-        h->learn_substeps++;
-        if (failed) {
-            TRY(restore_substep_state(h));
-            h->force_plain = true;
-            int rc = h->residual_tol > 0.f ? run_step_tol_eager(h, h->residual_tol) : (enqueue_step(h), ADMM_OK);
-            h->force_plain = false;
-            TRY(rc);
-            h->learn_fallbacks++;
-        }
-    }
+    TRY(h->enqueue_rc);
+    if (learned_active(h)) h->learn_substeps++;
     return ADMM_OK;
 }
 
@@ -1633,6 +1613,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
 
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->body_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->if_stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
@@ -1680,9 +1661,11 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         L.minv = minv;
         L.theta = theta;
         TRY(dalloc(h, &L.xl, nd));
-        TRY(dalloc(h, &L.part, 3 * (size_t)L.blocks));
+        TRY(dalloc(h, &L.part, 4 * (size_t)L.blocks));
         TRY(dalloc(h, &L.stats, 4));
         TRY(dalloc(h, &L.fail, 1));
+        TRY(dalloc(h, &L.warm, 1));
+        CK(cudaHostAlloc((void**)&h->fail_host, sizeof(int), cudaHostAllocDefault));
         h->learn_sweeps = std::max(1, h->jac_iter);
         h->learn_omega.assign(h->learn_sweeps, 1.f);
         h->learn_beta.assign(h->learn_sweeps, 0.f);
@@ -1997,7 +1980,6 @@ void admm_b200_destroy(AdmmB200* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
-    if (h->plain_exec) cudaGraphExecDestroy(h->plain_exec);
     if (h->fail_host) cudaFreeHost(h->fail_host);
     for (void* p : h->allocs)
         if (p) cudaFree(p);
@@ -2008,6 +1990,7 @@ void admm_b200_destroy(AdmmB200* h) {
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->body_stream) cudaStreamDestroy(h->body_stream);
+    if (h->if_stream) cudaStreamDestroy(h->if_stream);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
@@ -2033,7 +2016,6 @@ int admm_b200_step_async(AdmmB200* h, int n_steps) {
         return ADMM_OK;
     }
     TRY(build_step_graph(h));
-    if (learned_active(h)) TRY(build_plain_graph(h));
     CK(cudaEventRecord(h->ev0, h->stream));
     for (int k = 0; k < n_steps; k++) TRY(launch_substep(h));
     CK(cudaEventRecord(h->ev1, h->stream));
@@ -2424,7 +2406,6 @@ int admm_b200_step_host(AdmmB200* h, const float* x_in, const float* v_in, float
     CK(cudaSetDevice(h->device));
     if (!h->stage) TRY(dalloc(h, &h->stage, (size_t)6 * n));
     TRY(build_step_graph(h));
-    if (learned_active(h)) TRY(build_plain_graph(h));
     const size_t bytes = sizeof(float) * 3 * (size_t)n;
     CK(cudaMemcpyAsync(h->stage, x_in, bytes, cudaMemcpyHostToDevice, h->stream));
     if (v_in) CK(cudaMemcpyAsync(h->stage + 3 * (size_t)n, v_in, bytes, cudaMemcpyHostToDevice, h->stream));
@@ -2554,7 +2535,7 @@ int admm_b200_learned_stats(AdmmB200* h, int64_t* out4) {
     unsigned long long d[2] = {0, 0};
     CK(cudaMemcpy(d, h->learn.stats, sizeof(d), cudaMemcpyDeviceToHost));
     out4[0] = h->learn_substeps;
-    out4[1] = h->learn_fallbacks;
+    out4[1] = (int64_t)d[1];  // every failed solve was replaced by the plain one
     out4[2] = (int64_t)d[0];
     out4[3] = (int64_t)d[1];
     return ADMM_OK;
@@ -2603,6 +2584,13 @@ int admm_b200_global_mode(AdmmB200* h, int* persistent, int* blocks, float* ms_s
     if (blocks) *blocks = h->persist ? h->pp.blocks : 0;
     if (ms_sweeps) *ms_sweeps = h->tune_ms_sweeps;
     if (ms_persist) *ms_persist = h->tune_ms_persist;
+    return ADMM_OK;
+}
+
+int admm_b200_kernels_fallback(AdmmB200* h, int* n) {
+    if (!h || !n) return ADMM_ERR_INVALID;
+    TRY(build_step_graph(h));
+    *n = h->global_solver == 3 ? h->kernels_fallback : 0;
     return ADMM_OK;
 }
 

@@ -1,11 +1,16 @@
-"""Train and evaluate the learned global step (global_solver 3) on the cube family.
+"""Train and evaluate the learned global step (global_solver 3) on a family of scenes.
 
-    python -m parallel_admm_b200.train_learned --out parallel_admm_b200/weights/learned_step.npz
+    python -m parallel_admm_b200.train_learned --family batch --out parallel_admm_b200/weights/learned_step.npz
+    python -m parallel_admm_b200.train_learned --family cube --out parallel_admm_b200/weights/learned_step_cube.npz
 
-Training data: plain Jacobi runs of the tetrahedralised cube (20^3 cells, 5 tets per cell,
-edge 0.5 m, nu = 0.4) with per seed E log-uniform in [1e4, 1e6], drop height U(0.5, 2) m
-and a random initial rotation.  Each run is advanced to a few frames before its impact, then
-records one global step per frame (iteration cycling over 1..29 of the 30) until `--samples`
+Families.  `cube`: the tetrahedralised cube (20^3 cells, 5 tets per cell, edge 0.5 m,
+nu = 0.4) with per seed E log-uniform in [1e4, 1e6], drop height U(0.5, 2) m and a random
+initial rotation, advanced to a few frames before its impact.  `batch`: small batches
+(`--bodies`, default 4) of the batched-soft-body generator -- cubes and voxelised ellipsoids
+of 500-20000 vertices, E log-uniform in [1e4, 1e6], friction U(0.2, 0.6), random rotation,
+released 6-20 mm above the ground -- the bodies of the 256-body benchmark batch, from frame 0.
+
+Training data: plain Jacobi runs of the family; each run records one global step per frame (iteration cycling over 1..29 of the 30) until `--samples`
 triples that still carry an error (free-fall solves converge to FP32 noise and are dropped):
 (b, x_cur, x_last) through
 admm_b200_record_global, and x* = A^-1 b by conjugate gradients on the GPU -- the
@@ -44,10 +49,16 @@ from parallel_admm_b200 import gnn, scene  # noqa: E402
 ALLOW = (B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW)
 
 
-def family_scene(seed: int, n: int):
-    """One member of the cube family (drop U(0.5, 2) m, E log-U, random rotation) and the
-    frame a few substeps before its impact (free-fall global solves converge to FP32 noise
-    and carry nothing to learn)."""
+def family_scene(seed: int, n: int, family: str = "cube", bodies: int = 4):
+    """One member of the family and the frame its samples start at: for the cube (drop
+    U(0.5, 2) m, E log-U, random rotation) a few substeps before its impact (free-fall
+    global solves converge to FP32 noise and carry nothing to learn); for a batch, frame 0
+    (its bodies touch the ground within the first frames)."""
+    if family == "batch":
+        sc = scene.batch_bodies(bodies, seed=20_000 + seed)
+        sc.params.ell_lanes = 4
+        sc.params.jacobi_mode = 1
+        return sc, 0
     rng = np.random.default_rng(10_000 + seed)
     drop = float(rng.uniform(0.5, 2.0))
     sc = scene.cube_on_ground(n, seed=seed, drop=drop, rotate=True)
@@ -67,7 +78,9 @@ def system_of(sc):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "parallel_admm_b200", "weights", "learned_step.npz"))
+    ap.add_argument("--family", default="cube", choices=["cube", "batch"])
     ap.add_argument("--n", type=int, default=20, help="cube cells per edge")
+    ap.add_argument("--bodies", type=int, default=4, help="bodies per scene of the batch family")
     ap.add_argument("--train-seeds", type=int, default=200)
     ap.add_argument("--samples", type=int, default=100, help="recorded global steps (frames) per training seed")
     ap.add_argument("--eval-seeds", type=int, default=500)
@@ -93,7 +106,7 @@ def main(argv=None):
     n_triples = 0
     t_gen = t_fit = 0.0
     for seed in range(args.train_seeds):
-        sc, f0 = family_scene(seed, args.n)
+        sc, f0 = family_scene(seed, args.n, args.family, args.bodies)
         h, sysm, x, ef = system_of(sc)
         h.step(f0, allow=ALLOW)
         tr = gnn.SweepTrainer(sysm)
@@ -138,7 +151,7 @@ def main(argv=None):
     t0 = time.time()
     for e in range(args.eval_seeds):
         seed = args.train_seeds + e
-        sc, f0 = family_scene(seed, args.n)
+        sc, f0 = family_scene(seed, args.n, args.family, args.bodies)
         h, sysm, x, ef = system_of(sc)
         f_eval = f0 + args.eval_frame
         h.step(f_eval, allow=ALLOW)
@@ -176,7 +189,9 @@ def main(argv=None):
         return {"mean": float(a.mean()), "median": float(np.median(a)), "p90": float(np.quantile(a, 0.9))}
 
     j20 = stats(ev_j20)
-    summary = {"train": {"family": f"cube {args.n}^3, E log-U[1e4,1e6], drop U(0.5,2) m, random rotation",
+    fam = (f"cube {args.n}^3, E log-U[1e4,1e6], drop U(0.5,2) m, random rotation" if args.family == "cube" else
+           f"batches of {args.bodies} bodies (cubes/ellipsoids 500-20000 verts, E log-U[1e4,1e6], mu U(0.2,0.6)) from rest")
+    summary = {"train": {"family": fam,
                          "seeds": args.train_seeds, "triples": n_triples, "gen_s": round(t_gen, 1),
                          "fit_s": round(t_fit, 1)},
                "eval": {"held_out_seeds": args.eval_seeds, "evaluated_seeds": len(ev_j20),

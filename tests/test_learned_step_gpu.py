@@ -101,8 +101,10 @@ def test_learned_substep_matches_the_oracle_with_contact():
 def test_judge_falls_back_to_plain_jacobi():
     """A schedule that steps slightly backwards (one sweep with omega = -0.05: the residual
     grows a little, the positions stay near the inertial prediction) fails the judge on a
-    deformed cube: every substep is run again with the plain Jacobi global step, bit for bit
-    the plain handle's substep."""
+    deformed cube: every solve is replaced on the device (the IF node of the substep graph)
+    by the plain one from the iterate it received, so the substeps are the plain handle's
+    up to the summation order of the right-hand side (the learned step computes b in its own
+    kernel)."""
     sc = _pin(scene.cube_on_ground(8))
     hj = B.Handle(sc)
     hl = B.Handle(sc, global_solver=3)
@@ -117,9 +119,13 @@ def test_judge_falls_back_to_plain_jacobi():
         hl.step(1, allow=ALLOW)
         xj, vj = hj.get_state()
         xl, vl = hl.get_state()
-        assert np.array_equal(xj, xl) and np.array_equal(vj, vl)
+        ext = np.ptp(xj[:sc.n_dyn], axis=0).max()
+        assert np.abs(xj - xl).max() <= 1e-6 * ext, np.abs(xj - xl).max() / ext
+        assert np.abs(vj - vl).max() <= 1e-6 * ext / sc.params.dt
     st = hl.learned_stats()
-    assert st["substeps"] == 3 and st["fallbacks"] == 3 and st["failed_solves"] >= 3, st
+    n_solves = 3 * sc.params.admm_max_iter
+    assert st["substeps"] == 3 and st["solves"] == n_solves, st
+    assert st["fallbacks"] == st["failed_solves"] and st["failed_solves"] >= n_solves // 2, st
     hj.close()
     hl.close()
 
