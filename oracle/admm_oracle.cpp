@@ -336,6 +336,91 @@ struct EnvelopeCholesky {
 // ---------------------------------------------------------------------------
 // The ADMM oracle.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Per-contact and per-row pieces of the GPU backend's contact and global steps, shared by
+// the Oracle below and by the orc_*_f entry points that pin them to the reference's own
+// kernels (tests/test_oracle_golden.py).
+// ---------------------------------------------------------------------------
+
+// S_c, Gamma_c and K_c of one contact (compute_Scc_kernel, contact_solver.cu:188-232):
+// S_c = eps + sum_k bary_k^2 w_inv[v_k] n[v_k], Gamma_k = bary_k / (S_c w[v_k]),
+// K_c = dt_inv h_cN normal gamma.  cpu_backend: the CPU backend's form (compute_Scc,
+// admm_impl_cpu.cpp:361-380): no per-vertex counts, Gamma of static vertices (w > 1e7) zero.
+template <class R>
+static void scc_contact(const Contact& ct, const int* cnt, const R* w, const R* winv, R eps, R gam, R dt_inv,
+                        bool cpu_backend, R* Gam4, R* Kc3) {
+    R t[4];
+    for (int k = 0; k < 4; k++)
+        t[k] = (R)ct.bary[k] * (R)ct.bary[k] * winv[ct.v[k]] * (cpu_backend ? R(1) : (R)cnt[ct.v[k]]);
+    const R Sc = eps + (((t[0] + t[1]) + t[2]) + t[3]);
+    for (int k = 0; k < 4; k++) {
+        Gam4[k] = (R)ct.bary[k] / (Sc * w[ct.v[k]]);
+        if (cpu_backend && w[ct.v[k]] > R(1e7)) Gam4[k] = 0;
+    }
+    for (int k = 0; k < 3; k++) Kc3[k] = dt_inv * (R)ct.gap * (R)ct.normal[k] * gam;
+}
+
+// One friction-cone projection of a contact (get_delta_u_kernel, contact_solver.cu:337-379):
+// u = sum_k bary_k p[v_k] + K_c, u* = u - r_c split along the normal; a compressive u*
+// loses its normal part and its tangential part is scaled onto the cone of slope mu;
+// du = u*_new - u, r_c += du.
+template <class R>
+static void cone_step(const Contact& ct, R mu, const R* p, const R* Kc3, R* rc3, R* du3) {
+    R u[3];
+    for (int a = 0; a < 3; a++)
+        u[a] = (((R)ct.bary[0] * p[3 * ct.v[0] + a] + (R)ct.bary[1] * p[3 * ct.v[1] + a]) +
+                (R)ct.bary[2] * p[3 * ct.v[2] + a]) + (R)ct.bary[3] * p[3 * ct.v[3] + a] + Kc3[a];
+    R nrm[3] = {(R)ct.normal[0], (R)ct.normal[1], (R)ct.normal[2]};
+    R us[3];
+    for (int a = 0; a < 3; a++) us[a] = u[a] - rc3[a];
+    R uN = (nrm[0] * us[0] + nrm[1] * us[1]) + nrm[2] * us[2];
+    R uT[3];
+    for (int a = 0; a < 3; a++) uT[a] = us[a] - uN * nrm[a];
+    if (uN < 0) {
+        R tau = std::sqrt((uT[0] * uT[0] + uT[1] * uT[1]) + uT[2] * uT[2]);
+        R alpha = -mu * uN;
+        uN = 0;
+        if (tau <= alpha) uT[0] = uT[1] = uT[2] = 0;
+        else { R sc = R(1) - alpha / tau; for (int a = 0; a < 3; a++) uT[a] = sc * uT[a]; }
+    }
+    for (int a = 0; a < 3; a++) {
+        R un = uN * nrm[a] + uT[a];
+        du3[a] = un - u[a];
+        rc3[a] = rc3[a] + du3[a];
+    }
+}
+
+// p[v] += sum over v's contact slots of du_c Gamma_{c,k}, slots in list order
+// (update_p, contact_solver.cu:381-399); list entries are 4 c + k.
+template <class R>
+static void gather_p(int nv, const int* vstart, const int* vlist, const R* Gam, const R* du, R* p) {
+    for (int vi = 0; vi < nv; vi++) {
+        R d[3] = {0, 0, 0};
+        for (int s = vstart[vi]; s < vstart[vi + 1]; s++) {
+            int e = vlist[s];
+            int c = e >> 2, k = e & 3;
+            for (int a = 0; a < 3; a++) d[a] = d[a] + du[3 * c + a] * Gam[4 * c + k];
+        }
+        for (int a = 0; a < 3; a++) p[3 * vi + a] += d[a];
+    }
+}
+
+// One Jacobi sweep xn = D^-1 (b - (A - D) x) over CSR rows (JacobiFunctor,
+// jacobi_solver.cu:52-98), off-diagonal products summed in column order.
+template <class R, class V>
+static void jacobi_sweep(int rows, const int* start, const int* col, const V* val, const R* diag, const R* b,
+                         const R* x, R* xn) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < rows; i++) {
+        R acc[3] = {0, 0, 0};
+        for (int a = start[i]; a < start[i + 1]; a++) {
+            int j = col[a];
+            for (int k = 0; k < 3; k++) acc[k] += x[3 * j + k] * (R)val[a];
+        }
+        for (int k = 0; k < 3; k++) xn[3 * i + k] = (b[3 * i + k] - acc[k]) / diag[i];
+    }
+}
+
 template <class R>
 struct Oracle {
     // scene
@@ -699,20 +784,9 @@ struct Oracle {
         Kc.assign(3 * nc, R(0));
         rc.assign(3 * nc, R(0));
         du.assign(3 * nc, R(0));
-        for (int c = 0; c < nc; c++) {
-            const Contact& ct = cts[c];
-            R t[4];
-            // the CPU backend (compute_Scc, admm_impl_cpu.cpp:361-380): no per-vertex
-            // counts, Gamma of static vertices (w_c > 1e7) zero
-            for (int k = 0; k < 4; k++)
-                t[k] = (R)ct.bary[k] * (R)ct.bary[k] * cwinv[ct.v[k]] * (backend == 1 ? R(1) : (R)cnt[ct.v[k]]);
-            const R Sc = eps + (((t[0] + t[1]) + t[2]) + t[3]);
-            for (int k = 0; k < 4; k++) {
-                Gam[4 * c + k] = (R)ct.bary[k] / (Sc * cw[ct.v[k]]);
-                if (backend == 1 && cw[ct.v[k]] > R(1e7)) Gam[4 * c + k] = 0;
-            }
-            for (int k = 0; k < 3; k++) Kc[3 * c + k] = (R(1) / dt) * (R)ct.gap * (R)ct.normal[k] * gam;
-        }
+        for (int c = 0; c < nc; c++)
+            scc_contact<R>(cts[c], cnt.data(), cw.data(), cwinv.data(), eps, gam, R(1) / dt, backend == 1, &Gam[4 * c],
+                           &Kc[3 * c]);
         vstart.assign(n + 1, 0);
         for (int i = 0; i < n; i++) vstart[i + 1] = vstart[i] + cnt[i];
         vlist.assign(vstart[n], 0);
@@ -742,40 +816,8 @@ struct Oracle {
             return;
         }
         for (int it = 0; it < gs_max_iter; it++) {
-            for (int c = 0; c < nc; c++) {
-                const Contact& ct = cts[c];
-                R u[3];
-                for (int a = 0; a < 3; a++)
-                    u[a] = (((R)ct.bary[0] * p[3 * ct.v[0] + a] + (R)ct.bary[1] * p[3 * ct.v[1] + a]) +
-                            (R)ct.bary[2] * p[3 * ct.v[2] + a]) + (R)ct.bary[3] * p[3 * ct.v[3] + a] + Kc[3 * c + a];
-                R nrm[3] = {(R)ct.normal[0], (R)ct.normal[1], (R)ct.normal[2]};
-                R us[3];
-                for (int a = 0; a < 3; a++) us[a] = u[a] - rc[3 * c + a];
-                R uN = (nrm[0] * us[0] + nrm[1] * us[1]) + nrm[2] * us[2];
-                R uT[3];
-                for (int a = 0; a < 3; a++) uT[a] = us[a] - uN * nrm[a];
-                if (uN < 0) {
-                    R tau = std::sqrt((uT[0] * uT[0] + uT[1] * uT[1]) + uT[2] * uT[2]);
-                    R alpha = -cmu[c] * uN;
-                    uN = 0;
-                    if (tau <= alpha) uT[0] = uT[1] = uT[2] = 0;
-                    else { R s = R(1) - alpha / tau; for (int a = 0; a < 3; a++) uT[a] = s * uT[a]; }
-                }
-                for (int a = 0; a < 3; a++) {
-                    R un = uN * nrm[a] + uT[a];
-                    du[3 * c + a] = un - u[a];
-                    rc[3 * c + a] = rc[3 * c + a] + du[3 * c + a];
-                }
-            }
-            for (int vi = 0; vi < nd; vi++) {
-                R d[3] = {0, 0, 0};
-                for (int s = vstart[vi]; s < vstart[vi + 1]; s++) {
-                    int e = vlist[s];
-                    int c = e >> 2, k = e & 3;
-                    for (int a = 0; a < 3; a++) d[a] = d[a] + du[3 * c + a] * Gam[4 * c + k];
-                }
-                for (int a = 0; a < 3; a++) p[3 * vi + a] += d[a];
-            }
+            for (int c = 0; c < nc; c++) cone_step<R>(cts[c], cmu[c], p.data(), &Kc[3 * c], &rc[3 * c], &du[3 * c]);
+            gather_p<R>(nd, vstart.data(), vlist.data(), Gam.data(), du.data(), p.data());
         }
     }
 
@@ -798,15 +840,7 @@ struct Oracle {
     void jacobi(int sweeps) {
         std::vector<R> xn(3 * nd);
         for (int s = 0; s < sweeps; s++) {
-#pragma omp parallel for schedule(static)
-            for (int i = 0; i < nd; i++) {
-                R acc[3] = {0, 0, 0};
-                for (int a = A.start[i]; a < A.start[i + 1]; a++) {
-                    int j = A.col[a];
-                    for (int k = 0; k < 3; k++) acc[k] += x[3 * j + k] * (R)A.val[a];
-                }
-                for (int k = 0; k < 3; k++) xn[3 * i + k] = (b[3 * i + k] - acc[k]) / Adiag[i];
-            }
+            jacobi_sweep<R>(nd, A.start.data(), A.col.data(), A.val.data(), Adiag.data(), b.data(), x.data(), xn.data());
             for (int i = 0; i < 3 * nd; i++) x[i] = xn[i];
         }
     }
@@ -1419,6 +1453,42 @@ int orc_num_threads() {
 #else
     return 1;
 #endif
+}
+
+// The shared pieces on caller-given arrays (FP32), for pinning against the reference's
+// kernels.  Contacts: v4 [nc x 4], bary4 [nc x 4], normal3 [nc x 3], gap [nc].
+static Contact make_contact(const int* v4, const float* bary4, const float* normal3, float gap) {
+    Contact ct{};
+    for (int k = 0; k < 4; k++) {
+        ct.v[k] = v4[k];
+        ct.bary[k] = bary4[k];
+    }
+    for (int k = 0; k < 3; k++) ct.normal[k] = normal3[k];
+    ct.gap = gap;
+    return ct;
+}
+
+void orc_scc_f(int nc, const int* v4, const float* bary4, const float* gap, const float* normal3, const int* cnt,
+               const float* w, const float* winv, float eps, float gam, float dt_inv, float* Gam4, float* Kc3) {
+    for (int c = 0; c < nc; c++)
+        scc_contact<float>(make_contact(v4 + 4 * c, bary4 + 4 * c, normal3 + 3 * c, gap[c]), cnt, w, winv, eps, gam,
+                           dt_inv, false, Gam4 + 4 * c, Kc3 + 3 * c);
+}
+
+void orc_cone_step_f(int nc, const float* mu, const int* v4, const float* bary4, const float* normal3, const float* p,
+                     const float* Kc3, float* rc3, float* du3) {
+    for (int c = 0; c < nc; c++)
+        cone_step<float>(make_contact(v4 + 4 * c, bary4 + 4 * c, normal3 + 3 * c, 0.f), mu[c], p, Kc3 + 3 * c,
+                         rc3 + 3 * c, du3 + 3 * c);
+}
+
+void orc_gather_p_f(int nv, const int* vstart, const int* vlist, const float* Gam4, const float* du3, float* p) {
+    gather_p<float>(nv, vstart, vlist, Gam4, du3, p);
+}
+
+void orc_jacobi_sweep_f(int rows, const int* start, const int* col, const float* val, const float* diag, const float* b,
+                        const float* x, float* xn) {
+    jacobi_sweep<float, float>(rows, start, col, val, diag, b, x, xn);
 }
 
 }  // extern "C"

@@ -306,3 +306,108 @@ def prox_tri(z6, double: bool = True) -> np.ndarray:
 
 def num_threads() -> int:
     return lib().orc_num_threads()
+
+
+# --- per-contact / per-row pieces (FP32), pinned to the reference's kernels ---
+REF_SOLVER_PATH = os.path.join(HERE, "_ref", "libref_solver.so")
+_ref_solver = None
+
+
+def ref_solver():
+    """The reference's contact and Jacobi kernels run on the host (oracle/ref_pin_solver.cpp), or None."""
+    global _ref_solver
+    if _ref_solver is None:
+        if not os.path.exists(REF_SOLVER_PATH):
+            return None
+        _ref_solver = ctypes.CDLL(REF_SOLVER_PATH)
+    return _ref_solver
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dt)
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def contact_lists(v4: np.ndarray, nv: int):
+    """Per-vertex contact counts and CSR starts of a contact set (v4: nc x 4)."""
+    cnt = np.bincount(np.asarray(v4, np.int64).ravel(), minlength=nv).astype(np.int32)
+    start = np.zeros(nv + 1, np.int32)
+    start[1:] = np.cumsum(cnt)
+    return cnt, start
+
+
+def scc(v4, bary4, gap, normal3, w, winv, eps, gam, dt_inv, ref: bool = False):
+    """S_c / Gamma_c / K_c of every contact (GPU-backend form, with per-vertex counts).
+    Returns (Gamma [nc x 4], K_c [nc x 3]) and, for the reference, also its per-vertex
+    lists (involved contact, Gamma_i) in CSR order."""
+    v4, bary4, normal3 = _c(v4, np.int32), _c(bary4, np.float32), _c(normal3, np.float32)
+    gap, w, winv = _c(gap, np.float32), _c(w, np.float32), _c(winv, np.float32)
+    nc, nv = len(v4), len(w)
+    cnt, start = contact_lists(v4, nv)
+    G = np.zeros((nc, 4), np.float32)
+    K = np.zeros((nc, 3), np.float32)
+    f = ctypes.c_float
+    if ref:
+        R = ref_solver()
+        inv = np.zeros(max(int(start[-1]), 1), np.int32)
+        gi = np.zeros(max(int(start[-1]), 1), np.float32)
+        R.ref_scc_f(ctypes.c_int(nc), _ptr(v4), _ptr(bary4), _ptr(start), _ptr(cnt), _ptr(w), _ptr(winv), _ptr(gap),
+                    _ptr(normal3), f(gam), f(eps), f(dt_inv), ctypes.c_int(nv), _ptr(G), _ptr(K), _ptr(inv), _ptr(gi))
+        return G, K, inv[:start[-1]], gi[:start[-1]]
+    lib().orc_scc_f(ctypes.c_int(nc), _ptr(v4), _ptr(bary4), _ptr(gap), _ptr(normal3), _ptr(cnt), _ptr(w), _ptr(winv),
+                    f(eps), f(gam), f(dt_inv), _ptr(G), _ptr(K))
+    return G, K
+
+
+def cone_step(mu: float, v4, bary4, normal3, p, Kc3, rc3, ref: bool = False):
+    """One friction-cone projection of every contact: (du [nc x 3], r_c after)."""
+    v4, bary4, normal3 = _c(v4, np.int32), _c(bary4, np.float32), _c(normal3, np.float32)
+    p, Kc3 = _c(p, np.float32), _c(Kc3, np.float32)
+    rc = np.array(rc3, np.float32, copy=True, order="C")
+    nc = len(v4)
+    du = np.zeros((nc, 3), np.float32)
+    if ref:
+        ref_solver().ref_delta_u_f(ctypes.c_int(nc), ctypes.c_float(mu), _ptr(v4), _ptr(bary4), _ptr(p), _ptr(Kc3),
+                                   _ptr(normal3), _ptr(du), _ptr(rc))
+    else:
+        mus = np.full(nc, mu, np.float32)
+        lib().orc_cone_step_f(ctypes.c_int(nc), _ptr(mus), _ptr(v4), _ptr(bary4), _ptr(normal3), _ptr(p), _ptr(Kc3),
+                              _ptr(rc), _ptr(du))
+    return du, rc
+
+
+def gather_p(v4, Gam4, du3, p, ref_lists=None):
+    """p + the per-vertex gather of du Gamma over each vertex's contacts (contact order).
+    ref_lists = (involved, Gamma_i) runs the reference's update_p on its own lists."""
+    v4, Gam4, du3 = _c(v4, np.int32), _c(Gam4, np.float32), _c(du3, np.float32)
+    out = np.array(p, np.float32, copy=True, order="C")
+    nv = len(out) // 3 if out.ndim == 1 else len(out)
+    cnt, start = contact_lists(v4, nv)
+    if ref_lists is not None:
+        inv, gi = _c(ref_lists[0], np.int32), _c(ref_lists[1], np.float32)
+        ref_solver().ref_gather_p_f(ctypes.c_int(nv), _ptr(inv), _ptr(start), _ptr(gi), _ptr(du3), _ptr(out))
+        return out
+    # the oracle's list: entries 4 c + k in contact order
+    vlist = np.zeros(max(int(start[-1]), 1), np.int32)
+    fill = start[:-1].copy()
+    for c in range(len(v4)):
+        for k in range(4):
+            v = v4[c, k]
+            vlist[fill[v]] = 4 * c + k
+            fill[v] += 1
+    lib().orc_gather_p_f(ctypes.c_int(nv), _ptr(start), _ptr(vlist), _ptr(Gam4), _ptr(du3), _ptr(out))
+    return out
+
+
+def jacobi_sweep(start, col, val, diag, b, x, ref: bool = False):
+    """One Jacobi sweep over CSR rows (off-diagonal part), FP32."""
+    start, col = _c(start, np.int32), _c(col, np.int32)
+    val, diag, b, x = _c(val, np.float32), _c(diag, np.float32), _c(b, np.float32), _c(x, np.float32)
+    rows = len(diag)
+    xn = np.zeros((rows, 3), np.float32)
+    fn = ref_solver().ref_jacobi_sweep_f if ref else lib().orc_jacobi_sweep_f
+    fn(ctypes.c_int(rows), _ptr(start), _ptr(col), _ptr(val), _ptr(diag), _ptr(b), _ptr(x), _ptr(xn))
+    return xn

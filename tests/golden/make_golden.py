@@ -2,8 +2,10 @@
 
 Runs the reference's ``src/mutils/svd_fast3.cuh`` (3x3 SVD) and
 ``src/mutils/dist_g.cuh`` (dcdPT / dcdEE narrow phase), compiled for the host by
-``oracle/Makefile`` into ``oracle/_ref/libref_pin.so`` from the reference tree, on
-seeded inputs, and stores inputs and outputs as small .npz fixtures.  The tests
+``oracle/Makefile`` into ``oracle/_ref/libref_pin.so`` from the reference tree, and its
+contact and Jacobi kernels (``src/solver/contact_solver.cu``, ``jacobi_solver.cu``, run on
+the host from ``oracle/_ref/libref_solver.so``), on seeded inputs, and stores inputs and
+outputs as small .npz fixtures.  The tests
 compare the oracle against these files, so they need neither the reference tree
 nor the host build at test time.
 
@@ -80,6 +82,59 @@ def main():
     U, S, V = zip(*[O.svd3_ref(f) for f in F])
     np.savez_compressed(os.path.join(HERE, "ref_svd3.npz"), F=F, U=np.stack(U), S=np.stack(S), V=np.stack(V))
     print("wrote", len(X), "narrow-phase cases and", len(F), "SVD cases")
+    if O.ref_solver() is None:
+        raise SystemExit("oracle/_ref/libref_solver.so is missing: build it with `make -C oracle` next to the reference tree")
+    np.savez_compressed(os.path.join(HERE, "ref_contact_jacobi.npz"), **contact_jacobi_cases(rng))
+    print("wrote the contact and Jacobi cases")
+
+
+def contact_jacobi_cases(rng):
+    """Inputs and the reference kernels' outputs for S_c / Gamma / K_c (compute_Scc_kernel),
+    the friction-cone projection (get_delta_u_kernel), the per-vertex gather (update_p) and
+    one Jacobi sweep (JacobiFunctor): random contacts over 300 vertices (the last 50 static,
+    w = 1e8), normals of unit length, p and r_c spread so that separating, sticking and
+    sliding contacts all occur; a random sparse symmetric system of 500 rows."""
+    nv, nd, nc = 300, 250, 1000
+    v4 = np.stack([rng.choice(nv, 4, replace=False) for _ in range(nc)]).astype(np.int32)
+    bary = rng.normal(size=(nc, 4)).astype(np.float32)
+    nrm = rng.normal(size=(nc, 3))
+    nrm = (nrm / np.linalg.norm(nrm, axis=1, keepdims=True)).astype(np.float32)
+    gap = rng.uniform(-1e-3, 1e-3, nc).astype(np.float32)
+    w = rng.uniform(10.0, 1000.0, nv).astype(np.float32)
+    w[nd:] = 1e8
+    winv = (1.0 / w).astype(np.float32)
+    eps, gam, dt_inv, mu = np.float32(1e-6), np.float32(0.5), np.float32(100.0), np.float32(0.4)
+    G, K, inv, gi = O.scc(v4, bary, gap, nrm, w, winv, eps, gam, dt_inv, ref=True)
+    p = rng.normal(size=(nv, 3)).astype(np.float32)
+    rc = rng.normal(scale=0.5, size=(nc, 3)).astype(np.float32)
+    # the first 600 contacts: r_c chosen so that u* = u - r_c is compressive with a tangential
+    # part well inside (sticking) or well outside (sliding) the cone
+    u = np.einsum("ck,ckj->cj", bary.astype(np.float64), p[v4].astype(np.float64)) + K
+    t = rng.normal(size=(nc, 3))
+    t -= np.einsum("cj,cj->c", t, nrm)[:, None] * nrm
+    t /= np.linalg.norm(t, axis=1, keepdims=True)
+    a = rng.uniform(0.1, 1.0, nc)[:, None]
+    scale = np.where(np.arange(nc) < 300, 0.3, 3.0)[:, None] * float(mu)
+    target = -a * nrm + scale * a * t
+    rc[:600] = (u - target)[:600].astype(np.float32)
+    du, rc_after = O.cone_step(float(mu), v4, bary, nrm, p, K, rc, ref=True)
+    p_after = O.gather_p(v4, G, du, p, ref_lists=(inv, gi))
+    rows = 500
+    pairs = {(int(a), int(b)) for a, b in rng.integers(0, rows, size=(3000, 2)) if a != b}
+    pairs |= {(b, a) for a, b in pairs}
+    pairs = sorted(pairs)
+    start = np.zeros(rows + 1, np.int32)
+    np.add.at(start, np.array([a for a, _ in pairs]) + 1, 1)
+    start = np.cumsum(start).astype(np.int32)
+    col = np.array([b for _, b in pairs], np.int32)
+    val = (-rng.uniform(0.0, 1.0, len(col))).astype(np.float32)
+    diag = rng.uniform(20.0, 40.0, rows).astype(np.float32)
+    b = rng.normal(size=(rows, 3)).astype(np.float32)
+    x = rng.normal(size=(rows, 3)).astype(np.float32)
+    xn = O.jacobi_sweep(start, col, val, diag, b, x, ref=True)
+    return dict(v4=v4, bary=bary, normal=nrm, gap=gap, w=w, winv=winv, eps=eps, gam=gam, dt_inv=dt_inv, mu=mu,
+                Gamma=G, Kc=K, involved=inv, gamma_i=gi, p=p, rc=rc, du=du, rc_after=rc_after, p_after=p_after,
+                start=start, col=col, val=val, diag=diag, b=b, x=x, xn=xn)
 
 
 if __name__ == "__main__":

@@ -1,12 +1,16 @@
 """Pin the oracle to the reference's own code (golden vectors in tests/golden/).
 
 The fixtures were produced by ``tests/golden/make_golden.py`` from the reference's
-``svd_fast3.cuh`` and ``dist_g.cuh`` compiled for the host (``oracle/_ref``).
+``svd_fast3.cuh`` and ``dist_g.cuh`` compiled for the host, and from its contact and
+Jacobi kernels run on the host (``oracle/_ref``).
 """
 import os
+import sys
 
 import numpy as np
 import pytest
+
+from oracle import oracle as O
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -81,3 +85,50 @@ def test_svd_convention_and_prox_vs_reference(oracle_lib):
         if np.abs(f).max() == 0:
             P = 2 * np.stack([z[:3], z[3:]], 1)
             assert np.allclose(np.linalg.norm(P, axis=0), 1.0, atol=1e-9)
+
+
+def test_contact_and_jacobi_pieces_bitexact_vs_reference(oracle_lib):
+    """S_c / Gamma_c / K_c, the friction-cone projection, the per-vertex gather of the
+    projection and one Jacobi sweep: the oracle's code for each (the functions the Oracle
+    itself steps with) against the reference's compute_Scc_kernel, get_delta_u_kernel,
+    update_p (contact_solver.cu:188-232, 337-399) and JacobiFunctor (jacobi_solver.cu:52-98),
+    run on the host from the reference tree by tests/golden/make_golden.py.  Bit for bit."""
+    d = np.load(os.path.join(GOLDEN, "ref_contact_jacobi.npz"))
+    G, K = O.scc(d["v4"], d["bary"], d["gap"], d["normal"], d["w"], d["winv"], d["eps"], d["gam"], d["dt_inv"])
+    assert np.array_equal(G, d["Gamma"]) and np.array_equal(K, d["Kc"])
+    du, rc = O.cone_step(float(d["mu"]), d["v4"], d["bary"], d["normal"], d["p"], d["Kc"], d["rc"])
+    assert np.array_equal(du, d["du"]) and np.array_equal(rc, d["rc_after"])
+    assert np.array_equal(O.gather_p(d["v4"], G, du, d["p"]), d["p_after"])
+    xn = O.jacobi_sweep(d["start"], d["col"], d["val"], d["diag"], d["b"], d["x"])
+    assert np.array_equal(xn, d["xn"])
+
+
+def test_contact_pieces_cover_the_cone_branches():
+    """The fixture exercises the three cases of the projection: u*_N >= 0 (left alone),
+    a sticking contact (|u*_T| <= mu |u*_N|) and a sliding one."""
+    d = np.load(os.path.join(GOLDEN, "ref_contact_jacobi.npz"))
+    v4, bary, p, n = d["v4"], d["bary"].astype(np.float64), d["p"].astype(np.float64), d["normal"].astype(np.float64)
+    u = np.einsum("ck,ckj->cj", bary, p[v4]) + d["Kc"]
+    us = u - d["rc"]
+    un = np.einsum("cj,cj->c", us, n)
+    ut = np.linalg.norm(us - un[:, None] * n, axis=1)
+    sep = un >= 0
+    stick = (~sep) & (ut <= -float(d["mu"]) * un)
+    slide = (~sep) & ~stick
+    assert sep.sum() > 50 and stick.sum() > 50 and slide.sum() > 50, (sep.sum(), stick.sum(), slide.sum())
+
+
+def test_contact_and_jacobi_pieces_vs_reference_build():
+    """Where the reference tree was built here (oracle/_ref/libref_solver.so), the same
+    comparison on fresh seeded inputs."""
+    if O.ref_solver() is None:
+        pytest.skip("reference solver pin not built (no reference tree)")
+    sys.path.insert(0, GOLDEN)
+    import make_golden
+    d = make_golden.contact_jacobi_cases(np.random.default_rng(7))
+    G, K = O.scc(d["v4"], d["bary"], d["gap"], d["normal"], d["w"], d["winv"], d["eps"], d["gam"], d["dt_inv"])
+    assert np.array_equal(G, d["Gamma"]) and np.array_equal(K, d["Kc"])
+    du, rc = O.cone_step(float(d["mu"]), d["v4"], d["bary"], d["normal"], d["p"], d["Kc"], d["rc"])
+    assert np.array_equal(du, d["du"]) and np.array_equal(rc, d["rc_after"])
+    assert np.array_equal(O.gather_p(d["v4"], G, du, d["p"]), d["p_after"])
+    assert np.array_equal(O.jacobi_sweep(d["start"], d["col"], d["val"], d["diag"], d["b"], d["x"]), d["xn"])
