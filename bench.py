@@ -59,6 +59,9 @@ CONFIGS = {
                            "1.45 M verts, 6.07 M tets, E log-U[1e4,1e6], mu U(0.2,0.6) per body) released 6-20 mm "
                            "above the ground (contact from the first frames), self-contact, 30 ADMM iters/step, "
                            "DCD every 5, dt=1/100; each rank simulates its own batch (seed = rank)"),
+    "batch_prof": dict(fn="batch_bodies", kw=dict(n_bodies=192, seed=0),
+                       workload="192 bodies of the 256-body batch's distribution (about 1.1 M verts; the sweep's "
+                                "algorithmic bytes exceed L2): profiling stand-in for the batch workload"),
     "sheets_small": dict(fn="sheets_on_sphere", kw=dict(nx=256, layers=2, seed=0),
                          workload="2 x 256^2 cloth sheets on a sphere r=0.3, 40 ADMM iters/step, dt=1/300 "
                                   "(profiling stand-in for the sheets workload)"),
@@ -350,6 +353,31 @@ def arm_summary(args, r, sc, world):
             "kernels_launched": r["launches"]}
 
 
+def profile_only(args):
+    """The substeps an ncu capture looks at (ncu --profile-from-start off): the arm's handle as
+    the bench builds it, warm-up and start-frame substeps outside the range, then
+    --profile-steps substeps inside it."""
+    import torch
+    from parallel_admm_b200 import backend as B
+    torch.cuda.set_device(0)
+    sc = make_scene(args)
+    gs = {"learned": 3, "jacobi": 0, "pcg": 1}[args.solver]
+    h = B.Handle(sc, residual_tol=args.tol, global_solver=gs)
+    info = learned_model(args, h, sc) if args.solver == "learned" else {}
+    allow = (B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW)
+    for _ in range(args.warmup + args.start_frame):
+        h.step(1, allow=allow)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    for _ in range(max(1, args.profile_steps)):
+        st = h.step(1, allow=allow)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+    print("profiled", args.config, args.solver, info, st, "kernels per substep", h.kernels_per_step(), flush=True)
+    h.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -381,11 +409,16 @@ def main():
                     help="open a CUDA profiler range (cudaProfilerStart/Stop) around the first N timed steps, "
                          "for ncu --profile-from-start off")
     ap.add_argument("--phase-steps", type=int, default=10, help="substeps of the phase-probe pass (roofline)")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="profiling run: the --solver arm's warm-up and --start-frame substeps, then --profile-steps "
+                         "substeps inside a CUDA profiler range; no timing, no JSON line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_only:
+        return profile_only(args)
 
     import torch
     import torch.distributed as dist
