@@ -356,7 +356,9 @@ def arm_summary(args, r, sc, world):
 def profile_only(args):
     """The substeps an ncu capture looks at (ncu --profile-from-start off): the arm's handle as
     the bench builds it, warm-up and start-frame substeps outside the range, then
-    --profile-steps substeps inside it."""
+    --profile-steps substeps inside it, launched eagerly (the same kernels as the step graph:
+    ncu does not profile the kernel nodes of a graph that holds conditional nodes, which the
+    learned step's fallback and the residual test use)."""
     import torch
     from parallel_admm_b200 import backend as B
     torch.cuda.set_device(0)
@@ -367,6 +369,7 @@ def profile_only(args):
     allow = (B.ERR_CONTACT_OVERFLOW, B.ERR_STACK_OVERFLOW)
     for _ in range(args.warmup + args.start_frame):
         h.step(1, allow=allow)
+    h.set_profiling(True)
     torch.cuda.synchronize()
     torch.cuda.cudart().cudaProfilerStart()
     for _ in range(max(1, args.profile_steps)):
@@ -490,10 +493,17 @@ def main():
             hp.step(1, allow=allow)
         hp.set_probe("phases")
         hp.phase_times()
+        ls0 = hp.learned_stats() if args.solver == "learned" else None
         for _ in range(nph):
             hp.step(1, allow=allow)
         raw = hp.phase_times()
         phases = {k: {"ms_per_step": v["ms"] / nph, "launches_per_step": v["launches"] / nph} for k, v in raw.items()}
+        if ls0 is not None:
+            # the plain solves that replaced failed learned ones run inside the global step's phase
+            # (the IF node's body holds no event nodes): count their kernels with the phase's
+            replaced = hp.learned_stats()["fallbacks"] - ls0["fallbacks"]
+            phases["jacobi"]["replaced_solves_per_step"] = replaced / nph
+            phases["jacobi"]["launches_per_step"] += replaced * hp.kernels_fallback() / nph
         phases["scope"] = (f"frames {args.start_frame}..{args.start_frame + nph - 1}, whole step, "
                            f"{sc.params.admm_max_iter} ADMM iterations (no residual test)")
         hp.close()
@@ -553,7 +563,9 @@ def main():
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak_gbs) if achieved else None, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg, "mean_launch_ms": phase_ms,
-                     "mean_launch_ms_how": "device time of the kernel's phase in the step graph / its launches",
+                     "mean_launch_ms_how": "device time of the kernel's phase in the step graph / the kernels it ran "
+                                           "(with the learned step: its sweeps, judge and decision, and the plain "
+                                           "solves that replaced failed ones)",
                      "isolated_launch_ms": probe_ms, "isolated_launches": probe_n,
                      "isolated_how": "event pair around each of the first launches of the class (adds the "
                                      "event overhead, breaks the programmatic overlap)"},
