@@ -577,15 +577,35 @@ void enqueue_pcg(AdmmB200* h, int iters) {
 #undef PCG_T
 }
 
-// The decision on a learned solve and the plain solve that replaces a failed one:
-// x <- x as received (L.xl), then the jacobi_iter Jacobi sweeps on the same b.  In a
-// graph they are the body of an IF node after k_ldecide, which sets its condition
-// (inside the residual-tolerance WHILE body the IF node is nested in it); eagerly,
-// the host reads the decision (one stream synchronisation per solve).
-void enqueue_learned_decide(AdmmB200* h) {
+// The judge's pass over x (k_ljudge, lanes of A).
+void launch_ljudge(AdmmB200* h) {
     DevScene& s = h->s;
     LearnDev& L = h->learn;
-    const int vb = blocks(s.nd, kVertThreads);
+    switch (s.A.lanes) {
+        case 1: LAUNCH(k_ljudge<1>, L.blocks, kVertThreads, s, L); break;
+        case 2: LAUNCH(k_ljudge<2>, L.blocks, kVertThreads, s, L); break;
+        case 4: LAUNCH(k_ljudge<4>, L.blocks, kVertThreads, s, L); break;
+        default: LAUNCH(k_ljudge<8>, L.blocks, kVertThreads, s, L); break;
+    }
+}
+
+// The plain solve that replaces a failed learned one: x <- x as received (L.xl), the
+// jacobi_iter Jacobi sweeps on the same b, and the judge's pass to refresh A x for the
+// next global step.
+void enqueue_learned_replacement(AdmmB200* h) {
+    DevScene& s = h->s;
+    LAUNCH(k_copy_dyn, blocks(s.nd, kVertThreads), kVertThreads, s, (const float4*)h->learn.xl, s.x);
+    enqueue_jacobi(h, h->jac_iter);
+    launch_ljudge(h);
+}
+
+// The decision on a learned solve and the plain solve that replaces a failed one.  In a
+// graph the replacement is the body of an IF node after k_ldecide, which sets its
+// condition (inside the residual-tolerance WHILE body the IF node is nested in it);
+// eagerly, the host reads the decision (one stream synchronisation per solve).
+void enqueue_learned_decide(AdmmB200* h, bool first) {
+    LearnDev& L = h->learn;
+    const int fi = first ? 1 : 0;
     cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamGetCaptureInfo(h->cstream, &cst, nullptr, &g, nullptr, nullptr);
@@ -594,15 +614,12 @@ void enqueue_learned_decide(AdmmB200* h) {
         return;
     }
     if (cst != cudaStreamCaptureStatusActive) {
-        LAUNCH(k_ldecide, 1, 256, L, cudaGraphConditionalHandle(0), 0);
+        LAUNCH(k_ldecide, 1, kDecideThreads, L, cudaGraphConditionalHandle(0), 0, fi);
         int failed = 0;
         if (cudaMemcpyAsync(h->fail_host, L.fail, sizeof(int), cudaMemcpyDeviceToHost, h->cstream) == cudaSuccess &&
             cudaStreamSynchronize(h->cstream) == cudaSuccess)
             failed = *h->fail_host;
-        if (failed) {
-            LAUNCH(k_copy_dyn, vb, kVertThreads, s, (const float4*)L.xl, s.x);
-            enqueue_jacobi(h, h->jac_iter);
-        }
+        if (failed) enqueue_learned_replacement(h);
         return;
     }
     cudaGraphConditionalHandle cond;
@@ -610,7 +627,7 @@ void enqueue_learned_decide(AdmmB200* h) {
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
     if (e == cudaSuccess) {
-        LAUNCH(k_ldecide, 1, 256, L, cond, 1);
+        LAUNCH(k_ldecide, 1, kDecideThreads, L, cond, 1, fi);
         e = cudaStreamGetCaptureInfo(h->cstream, &cst, nullptr, &g, &deps, &ndeps);
     }
     cudaGraphNodeParams cp = {};
@@ -632,8 +649,7 @@ void enqueue_learned_decide(AdmmB200* h) {
     e = cudaStreamBeginCaptureToGraph(h->cstream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        LAUNCH(k_copy_dyn, vb, kVertThreads, s, (const float4*)L.xl, s.x);
-        enqueue_jacobi(h, h->jac_iter);
+        enqueue_learned_replacement(h);
         cudaGraph_t bg = nullptr;
         e = cudaStreamEndCapture(h->cstream, &bg);
     }
@@ -646,18 +662,20 @@ void enqueue_learned_decide(AdmmB200* h) {
         h->enqueue_rc = fail(h, ADMM_ERR_CUDA, std::string("fallback IF body: ") + cudaGetErrorString(e));
 }
 
-// The learned global step: right-hand side with the warm start, learn_sweeps
-// second-order sweeps (x_k in {x, jac0, jac1}[k % 3]), the judge's pass that
-// leaves x_K in x, and the decision with its fallback.
+// The learned global step: right-hand side with the start of the solve, learn_sweeps
+// second-order sweeps (x_k in {x, jac0, jac1}[(s0 + k) % 3], s0 = -K mod 3, so that x_K
+// lands in x), the judge's pass and the decision with its fallback.
 void enqueue_learned(AdmmB200* h, bool save_prev, bool first) {
     DevScene& s = h->s;
     LearnDev& L = h->learn;
+    const int K = h->learn_sweeps;
+    const int s0 = (3 - K % 3) % 3;
+    float4* buf[3] = {s.x, s.jac[0], s.jac[1]};
     set_phase(h, ADMM_PHASE_RHS);
-    const int gr = blocks(s.R.nslices * 32, kVertThreads);
     const int ex = first ? 0 : 1;
-#define RHSL_CASE(T)                                                                                \
-    if (save_prev) LAUNCH_P(ADMM_KERNEL_RHS, (k_rhs_learn<T, true>), gr, kVertThreads, s, L, ex);   \
-    else LAUNCH_P(ADMM_KERNEL_RHS, (k_rhs_learn<T, false>), gr, kVertThreads, s, L, ex);
+#define RHSL_CASE(T)                                                                                             \
+    if (save_prev) LAUNCH_P(ADMM_KERNEL_RHS, (k_rhs_learn<T, true>), L.rblocks, kVertThreads, s, L, ex, buf[s0]); \
+    else LAUNCH_P(ADMM_KERNEL_RHS, (k_rhs_learn<T, false>), L.rblocks, kVertThreads, s, L, ex, buf[s0]);
     switch (s.R.lanes) {
         case 1: RHSL_CASE(1) break;
         case 2: RHSL_CASE(2) break;
@@ -666,21 +684,18 @@ void enqueue_learned(AdmmB200* h, bool save_prev, bool first) {
     }
 #undef RHSL_CASE
     set_phase(h, ADMM_PHASE_JACOBI);
-    const int K = h->learn_sweeps;
-    float4* buf[3] = {s.x, s.jac[0], s.jac[1]};
 #define LS_CASE(T)                                                                                         \
     for (int k = 0; k < K; k++) {                                                                          \
-        const float4* src = buf[k % 3];                                                                    \
-        const float4* prv = buf[(k + 2) % 3];                                                              \
-        float4* dst = buf[(k + 1) % 3];                                                                    \
+        const float4* src = buf[(s0 + k) % 3];                                                             \
+        const float4* prv = buf[(s0 + k + 2) % 3];                                                         \
+        float4* dst = buf[(s0 + k + 1) % 3];                                                               \
         if (k == 0)                                                                                        \
             LAUNCH_P(ADMM_KERNEL_JACOBI, (k_lsweep<T, true>), L.blocks, kVertThreads, s, L, src, prv, dst, \
-                     h->learn_omega[k], h->learn_beta[k], first ? (const float4*)nullptr : (const float4*)L.xl); \
+                     h->learn_omega[k], h->learn_beta[k]);                                                 \
         else                                                                                               \
             LAUNCH_P(ADMM_KERNEL_JACOBI, (k_lsweep<T, false>), L.blocks, kVertThreads, s, L, src, prv, dst, \
-                     h->learn_omega[k], h->learn_beta[k], (const float4*)nullptr);                          \
-    }                                                                                                      \
-    LAUNCH(k_ljudge<T>, L.blocks, kVertThreads, s, L, (const float4*)buf[K % 3]);
+                     h->learn_omega[k], h->learn_beta[k]);                                                 \
+    }
     switch (s.A.lanes) {
         case 1: LS_CASE(1) break;
         case 2: LS_CASE(2) break;
@@ -688,7 +703,8 @@ void enqueue_learned(AdmmB200* h, bool save_prev, bool first) {
         default: LS_CASE(8) break;
     }
 #undef LS_CASE
-    enqueue_learned_decide(h);
+    launch_ljudge(h);
+    enqueue_learned_decide(h, first);
 }
 
 // Copies of one global step's inputs for admm_b200_record_global (eager only):
@@ -1661,7 +1677,10 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         L.minv = minv;
         L.theta = theta;
         TRY(dalloc(h, &L.xl, nd));
-        TRY(dalloc(h, &L.part, 4 * (size_t)L.blocks));
+        L.rblocks = blocks(s.R.nslices * 32, kVertThreads);
+        TRY(dalloc(h, &L.ax, nd));
+        TRY(dalloc(h, &L.part, 3 * (size_t)L.blocks));
+        TRY(dalloc(h, &L.part_c, (size_t)L.rblocks));
         TRY(dalloc(h, &L.stats, 4));
         TRY(dalloc(h, &L.fail, 1));
         TRY(dalloc(h, &L.warm, 1));

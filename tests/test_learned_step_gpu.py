@@ -108,6 +108,10 @@ def test_judge_falls_back_to_plain_jacobi():
     sc = _pin(scene.cube_on_ground(8))
     sc.params.ell_lanes = 4
     sc.params.jacobi_mode = 1
+    # one ADMM iteration per substep: its global solve starts from the prediction, whose
+    # residual lies far above the judge's FP32 noise floor (1e-5 |b|), so every solve fails;
+    # later iterations of a converging substep may start below the floor, where any solve passes
+    sc.params.admm_max_iter = 1
     hj = B.Handle(sc)
     hl = B.Handle(sc, global_solver=3)
     rng = np.random.default_rng(0)
@@ -123,9 +127,8 @@ def test_judge_falls_back_to_plain_jacobi():
         xl, vl = hl.get_state()
         assert np.array_equal(xj, xl) and np.array_equal(vj, vl), np.abs(xj - xl).max()
     st = hl.learned_stats()
-    n_solves = 3 * sc.params.admm_max_iter
-    assert st["substeps"] == 3 and st["solves"] == n_solves, st
-    assert st["fallbacks"] == st["failed_solves"] and st["failed_solves"] >= n_solves // 2, st
+    assert st["substeps"] == 3 and st["solves"] == 3, st
+    assert st["fallbacks"] == st["failed_solves"] == 3, st
     hj.close()
     hl.close()
 
