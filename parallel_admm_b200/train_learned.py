@@ -2,6 +2,7 @@
 
     python -m parallel_admm_b200.train_learned --family batch --out parallel_admm_b200/weights/learned_step.npz
     python -m parallel_admm_b200.train_learned --family cube --out parallel_admm_b200/weights/learned_step_cube.npz
+    python -m parallel_admm_b200.train_learned --family sheets --out parallel_admm_b200/weights/learned_step_sheets.npz
 
 Families.  `cube`: the tetrahedralised cube (20^3 cells, 5 tets per cell, edge 0.5 m,
 nu = 0.4) with per seed E log-uniform in [1e4, 1e6], drop height U(0.5, 2) m and a random
@@ -9,6 +10,9 @@ initial rotation, advanced to a few frames before its impact.  `batch`: small ba
 (`--bodies`, default 4) of the batched-soft-body generator -- cubes and voxelised ellipsoids
 of 500-20000 vertices, E log-uniform in [1e4, 1e6], friction U(0.2, 0.6), random rotation,
 released 6-20 mm above the ground -- the bodies of the 256-body benchmark batch, from frame 0.
+`sheets`: two 128 x 128 cloth sheets of side 0.25 m (the 1.96 mm edge of the 4 x 512^2
+sheets), random in-plane rotations, dropped onto the sphere of the sheets scene, from a few
+frames before they reach it.
 
 Training data: plain Jacobi runs of the family; each run records one global step per frame (iteration cycling over 1..29 of the 30) until `--samples`
 triples that still carry an error (free-fall solves converge to FP32 noise and are dropped):
@@ -34,6 +38,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import sys
 import time
@@ -61,6 +66,13 @@ def family_scene(seed: int, n: int, family: str = "cube", bodies: int = 4):
         sc.params.ell_lanes = 4
         sc.params.jacobi_mode = 1
         return sc, 0
+    if family == "sheets":
+        sc = scene.sheets_on_sphere(nx=128, layers=2, seed=30_000 + seed, side=0.25)
+        sc.params.ell_lanes = 4
+        sc.params.jacobi_mode = 1
+        # the lower sheet starts 5 cm above the sphere's top
+        impact = int(math.sqrt(2.0 * 0.05 / sc.params.g) / sc.params.dt)
+        return sc, max(0, impact - 3)
     rng = np.random.default_rng(10_000 + seed)
     drop = float(rng.uniform(0.5, 2.0))
     sc = scene.cube_on_ground(n, seed=seed, drop=drop, rotate=True)
@@ -80,7 +92,7 @@ def system_of(sc):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "parallel_admm_b200", "weights", "learned_step.npz"))
-    ap.add_argument("--family", default="cube", choices=["cube", "batch"])
+    ap.add_argument("--family", default="cube", choices=["cube", "batch", "sheets"])
     ap.add_argument("--n", type=int, default=20, help="cube cells per edge")
     ap.add_argument("--bodies", type=int, default=4, help="bodies per scene of the batch family")
     ap.add_argument("--train-seeds", type=int, default=200)
@@ -192,8 +204,10 @@ def main(argv=None):
         return {"mean": float(a.mean()), "median": float(np.median(a)), "p90": float(np.quantile(a, 0.9))}
 
     j20 = stats(ev_j20)
-    fam = (f"cube {args.n}^3, E log-U[1e4,1e6], drop U(0.5,2) m, random rotation" if args.family == "cube" else
-           f"batches of {args.bodies} bodies (cubes/ellipsoids 500-20000 verts, E log-U[1e4,1e6], mu U(0.2,0.6)) from rest")
+    fam = {"cube": f"cube {args.n}^3, E log-U[1e4,1e6], drop U(0.5,2) m, random rotation",
+           "batch": f"batches of {args.bodies} bodies (cubes/ellipsoids 500-20000 verts, E log-U[1e4,1e6], "
+                    f"mu U(0.2,0.6)) from rest",
+           "sheets": "two 128^2 sheets of side 0.25 m (1.96 mm edge) onto the sphere"}[args.family]
     summary = {"train": {"family": fam,
                          "seeds": args.train_seeds, "triples": n_triples, "gen_s": round(t_gen, 1),
                          "fit_s": round(t_fit, 1)},
