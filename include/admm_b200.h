@@ -206,13 +206,13 @@ int  admm_b200_reset(AdmmB200* h);
  * that keep data on the GPU; valid until destroy.  The rows are in the library's
  * vertex order (below), not necessarily the caller's. */
 int  admm_b200_device_state(AdmmB200* h, void** x_float4, void** v_float4);
-/* The library stores the dynamic vertices in the Morton order of their rest positions
- * (spatially close vertices at close indices, so that the gathers of the sweeps, the
- * local step and the right-hand side share cache lines); every other entry point takes
- * and returns per-vertex data and vertex indices in the caller's order.  order[i]
- * receives the caller's index of internal row i (the identity with backend_semantics 1,
- * whose serial Gauss-Seidel follows the contact order, or when the environment sets
- * ADMM_B200_RENUMBER=0); static vertices keep their indices.  No reference counterpart. */
+/* With ADMM_B200_RENUMBER=1 in the environment at create, the library stores the dynamic
+ * vertices in the Morton order of their rest positions (spatially close vertices at close
+ * indices, for meshes whose own numbering has no locality); by default, and always with
+ * backend_semantics 1 (whose serial Gauss-Seidel follows the contact order), it keeps the
+ * caller's order.  Every other entry point takes and returns per-vertex data and vertex
+ * indices in the caller's order.  order[i] receives the caller's index of internal row i;
+ * static vertices keep their indices.  No reference counterpart. */
 int  admm_b200_vertex_order(AdmmB200* h, int32_t* order, int n);
 
 /* --- scripted static meshes (ScriptAnimator, src/solver/animator.cpp:9-204; applied at the

@@ -77,13 +77,14 @@ struct AdmmB200 {
     int kernels_fallback = 0;       // kernels of the plain solve that replaces a failed learned one
     cudaStream_t if_stream = nullptr;  // capture of the bodies of the fallback IF nodes
     bool force_plain = false;       // enqueue the Jacobi global step whatever global_solver says
-    // Vertex renumbering: the library stores the dynamic vertices in the Morton order of
-    // their rest positions (spatially close vertices at close indices, so the gathers of the
-    // sweeps, the local step and the right-hand side share cache lines); every entry point
-    // that takes or returns per-vertex data or vertex indices maps between that order and
-    // the caller's.  perm[internal] = caller's index, iperm[caller's] = internal; empty =
-    // identity (the CPU backend's semantics, whose serial Gauss-Seidel follows the contact
-    // order, and ADMM_B200_RENUMBER=0).
+    // Vertex renumbering (ADMM_B200_RENUMBER=1): the library stores the dynamic vertices in
+    // the Morton order of their rest positions (spatially close vertices at close indices,
+    // for meshes whose own numbering has no locality); every entry point that takes or
+    // returns per-vertex data or vertex indices maps between that order and the caller's.
+    // perm[internal] = caller's index, iperm[caller's] = internal; empty = identity, the
+    // default (a lattice numbering gives each warp of the sweeps contiguous neighbour rows,
+    // which the Morton order breaks up) and always with the CPU backend's semantics, whose
+    // serial Gauss-Seidel follows the contact order.
     std::vector<int> perm, iperm;
     int* d_perm = nullptr;
     HostCsr hostA_caller;           // the global matrix in the caller's order (admm_b200_system)
@@ -691,10 +692,10 @@ void enqueue_learned(AdmmB200* h, bool save_prev, bool first) {
         float4* dst = buf[(s0 + k + 1) % 3];                                                               \
         if (k == 0)                                                                                        \
             LAUNCH_P(ADMM_KERNEL_JACOBI, (k_lsweep<T, true>), L.blocks, kVertThreads, s, L, src, prv, dst, \
-                     h->learn_omega[k], h->learn_beta[k]);                                                 \
+                     h->learn_omega[k], h->learn_beta[k], ex);                                             \
         else                                                                                               \
             LAUNCH_P(ADMM_KERNEL_JACOBI, (k_lsweep<T, false>), L.blocks, kVertThreads, s, L, src, prv, dst, \
-                     h->learn_omega[k], h->learn_beta[k]);                                                 \
+                     h->learn_omega[k], h->learn_beta[k], 0);                                              \
     }
     switch (s.A.lanes) {
         case 1: LS_CASE(1) break;
@@ -1680,7 +1681,7 @@ int create_impl(const AdmmB200Desc* d, int device, AdmmB200* h) {
         L.rblocks = blocks(s.R.nslices * 32, kVertThreads);
         TRY(dalloc(h, &L.ax, nd));
         TRY(dalloc(h, &L.part, 3 * (size_t)L.blocks));
-        TRY(dalloc(h, &L.part_c, (size_t)L.rblocks));
+        TRY(dalloc(h, &L.part_c, (size_t)L.blocks));
         TRY(dalloc(h, &L.stats, 4));
         TRY(dalloc(h, &L.fail, 1));
         TRY(dalloc(h, &L.warm, 1));
@@ -1955,7 +1956,7 @@ int admm_b200_create(const AdmmB200Desc* desc, int device, AdmmB200** out) {
     if (!h) return ADMM_ERR_OOM;
     const char* env = std::getenv("ADMM_B200_RENUMBER");
     const bool want = desc->abi_version == ADMM_B200_ABI_VERSION && desc->backend_semantics == 0 && desc->x0 &&
-                      desc->mass && !(env && env[0] == '0' && env[1] == '\0') && indices_in_range(desc);
+                      desc->mass && env && env[0] == '1' && env[1] == '\0' && indices_in_range(desc);
     RenumberedDesc rd;
     if (want) {
         morton_order(desc, h->perm, h->iperm);

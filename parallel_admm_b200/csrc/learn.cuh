@@ -19,8 +19,9 @@
 // iterate, not x_0, also catches a warm start that made things worse.  The sums: the
 // first sweep adds up |b - A x_0|^2 and |b|^2, the judge's pass (k_ljudge) |b - A x_K|^2;
 // the judge's pass also keeps A x_K, which is A x_c of the substep's next global step (the
-// local and contact steps in between do not move x), so k_rhs_learn sums |b - A x_c|^2
-// with the new b without a pass over A.  In the substep's first global step x_0 = x_c.
+// local and contact steps in between do not move x), so the first sweep sums
+// |b - A x_c|^2 with the new b without a second pass over A.  In the substep's first
+// global step x_0 = x_c.
 // The warm start restarts adaptively (the function-value restart of accelerated methods,
 // O'Donoghue and Candes 2015, on the residual norm): once a warm start raised the
 // residual, |b - A x_0| > |b - A x_c|, it stays off until the substep's next first global
@@ -44,7 +45,7 @@ struct LearnDev {
     float4* xl = nullptr;          // [nd] x received by the previous global step
     float4* ax = nullptr;          // [nd] A x after the last global step (judge's pass or fallback)
     double* part = nullptr;        // [3 x blocks] block partials of |r_0|^2, |r_K|^2 and |b|^2
-    double* part_c = nullptr;      // [rblocks] block partials of |r_c|^2 (k_rhs_learn)
+    double* part_c = nullptr;      // [blocks] block partials of |r_c|^2 (first sweep)
     int blocks = 0;                // grid of the sweeps and the judge
     int rblocks = 0;               // grid of k_rhs_learn
     unsigned long long* stats = nullptr;  // [4] solves judged, solves failed (device counters)
@@ -54,67 +55,52 @@ struct LearnDev {
 
 // Right-hand side (as k_rhs) plus the start of the solve: xl <- x_c (the received x),
 // x0buf <- x_c + theta (x_c - xl_old) while L.warm is set, else x_c (not rewritten when
-// x0buf is x itself).  Not in the substep's first global step (extrap = 0, where the warm
-// start is switched on for the substep): the block partials of |b - A x_c|^2 from L.ax.
+// x0buf is x itself).  extrap = 0 in the substep's first global step, where the warm start
+// is switched on for the substep.
 template <int T, bool SAVE_PREV>
 __global__ void __launch_bounds__(kVertThreads) k_rhs_learn(DevScene s, LearnDev L, int extrap,
                                                             float4* __restrict__ x0buf) {
     ADMM_PDL_TRIGGER();
-    __shared__ double sh[kVertThreads / 32];
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    double rc = 0.0;
-    if (w < s.R.nslices) {
-        EllRowPf<T, true> r;
-        r.load(s.R, w, lane);
-        const int i = r.row;
-        const bool own = i < s.nd, c = own && s.contact;
-        const float wc = c ? __ldg(&s.dt2wc[i]) : 0.f;
-        const float th = own && extrap ? __ldg(&L.theta[i]) : 0.f;
-        ADMM_PDL_WAIT();
-        if (!extrap && blockIdx.x == 0 && threadIdx.x == 0) *L.warm = 1;  // nobody reads it in this launch
-        const bool warm = extrap && *L.warm;
-        const float4 z = f4(0.f, 0.f, 0.f);
-        const float4 m = own ? s.mxt[i] : z, p = c ? s.p[i] : z, x0 = c ? s.x0[i] : z, uc = c ? s.uc[i] : z;
-        const float4 xi = own ? s.x[i] : z;
-        const float4 xo = own && warm ? L.xl[i] : z;
-        const float4 ai = own && extrap ? L.ax[i] : z;
-        const float4 acc = r.sum(s.R, s.y, lane);
-        if (lane < 32 / T && own) {
-            const float4 bi = rhs_value(s, acc, m, p, x0, uc, wc);
-            s.b[i] = bi;
-            if (SAVE_PREV) s.xprev[i] = xi;
-            L.xl[i] = xi;
-            if (warm)
-                x0buf[i] = f4(fmaf(th, xi.x - xo.x, xi.x), fmaf(th, xi.y - xo.y, xi.y), fmaf(th, xi.z - xo.z, xi.z));
-            else if (x0buf != s.x)
-                x0buf[i] = xi;
-            if (extrap) {
-                const float cx = bi.x - ai.x, cy = bi.y - ai.y, cz = bi.z - ai.z;
-                rc = (double)cx * cx + (double)cy * cy + (double)cz * cz;
-            }
-        }
-    } else {
-        ADMM_PDL_WAIT();
-    }
-    if (extrap) {
-        rc = block_sum(rc, sh);
-        if (threadIdx.x == 0) L.part_c[blockIdx.x] = rc;
-    }
+    if (w >= s.R.nslices) return;
+    EllRowPf<T, true> r;
+    r.load(s.R, w, lane);
+    const int i = r.row;
+    const bool own = i < s.nd, c = own && s.contact;
+    const float wc = c ? __ldg(&s.dt2wc[i]) : 0.f;
+    const float th = own && extrap ? __ldg(&L.theta[i]) : 0.f;
+    ADMM_PDL_WAIT();
+    if (!extrap && blockIdx.x == 0 && threadIdx.x == 0) *L.warm = 1;  // nobody reads it in this launch
+    const bool warm = extrap && *L.warm;
+    const float4 z = f4(0.f, 0.f, 0.f);
+    const float4 m = own ? s.mxt[i] : z, p = c ? s.p[i] : z, x0 = c ? s.x0[i] : z, uc = c ? s.uc[i] : z;
+    const float4 xi = own ? s.x[i] : z;
+    const float4 xo = own && warm ? L.xl[i] : z;
+    const float4 acc = r.sum(s.R, s.y, lane);
+    if (lane >= 32 / T || !own) return;
+    s.b[i] = rhs_value(s, acc, m, p, x0, uc, wc);
+    if (SAVE_PREV) s.xprev[i] = xi;
+    L.xl[i] = xi;
+    if (warm)
+        x0buf[i] = f4(fmaf(th, xi.x - xo.x, xi.x), fmaf(th, xi.y - xo.y, xi.y), fmaf(th, xi.z - xo.z, xi.z));
+    else if (x0buf != s.x)
+        x0buf[i] = xi;
 }
 
 // One learned sweep k: dst = src + omega m (b - A src) + beta (src - prev); the first
 // sweep (FIRST) also writes the block partials of |b - A x_0|^2 into L.part[0..) and of
-// |b|^2 into L.part[2 blocks..).
+// |b|^2 into L.part[2 blocks..), and, outside the substep's first global step (extrap),
+// of |b - A x_c|^2 into L.part_c, A x_c from L.ax.
 template <int T, bool FIRST>
 __global__ void __launch_bounds__(kVertThreads) k_lsweep(DevScene s, LearnDev L, const float4* __restrict__ src,
                                                          const float4* __restrict__ prev, float4* __restrict__ dst,
-                                                         float omega, float beta) {
+                                                         float omega, float beta, int extrap) {
     ADMM_PDL_TRIGGER();
     __shared__ double sh[kVertThreads / 32];
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    double rr = 0.0, bb = 0.0;
+    double rr = 0.0, bb = 0.0, rc = 0.0;
     if (w < s.A.nslices) {
         EllRowPf<T> r;
         r.load(s.A, w, lane);
@@ -136,6 +122,11 @@ __global__ void __launch_bounds__(kVertThreads) k_lsweep(DevScene s, LearnDev L,
             if (FIRST) {
                 rr = (double)rx * rx + (double)ry * ry + (double)rz * rz;
                 bb = (double)bi.x * bi.x + (double)bi.y * bi.y + (double)bi.z * bi.z;
+                if (extrap) {
+                    const float4 ai = L.ax[i];
+                    const float cx = bi.x - ai.x, cy = bi.y - ai.y, cz = bi.z - ai.z;
+                    rc = (double)cx * cx + (double)cy * cy + (double)cz * cz;
+                }
             }
         }
     } else {
@@ -144,9 +135,11 @@ __global__ void __launch_bounds__(kVertThreads) k_lsweep(DevScene s, LearnDev L,
     if (FIRST) {
         rr = block_sum(rr, sh);
         bb = block_sum(bb, sh);
+        if (extrap) rc = block_sum(rc, sh);
         if (threadIdx.x == 0) {
             L.part[blockIdx.x] = rr;
             L.part[2 * L.blocks + blockIdx.x] = bb;
+            if (extrap) L.part_c[blockIdx.x] = rc;
         }
     }
 }
@@ -211,7 +204,7 @@ __global__ void __launch_bounds__(kDecideThreads) k_ldecide(LearnDev L, cudaGrap
     double e = strided_sum(L.part, L.blocks);
     double b = strided_sum(L.part + L.blocks, L.blocks);
     double c = strided_sum(L.part + 2 * L.blocks, L.blocks);
-    double a = first ? 0.0 : strided_sum(L.part_c, L.rblocks);
+    double a = first ? 0.0 : strided_sum(L.part_c, L.blocks);
     e = block_sum(e, sh);
     b = block_sum(b, sh);
     c = block_sum(c, sh);

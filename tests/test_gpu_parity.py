@@ -712,8 +712,8 @@ print(json.dumps(cs))
 
 
 def test_vertex_renumbering_is_invisible_to_the_caller():
-    """The library stores the dynamic vertices in Morton order; with ADMM_B200_RENUMBER=0 it
-    keeps the caller's order.  Through the C ABI both give the same contact pair set and the
+    """With ADMM_B200_RENUMBER=1 the library stores the dynamic vertices in Morton order; by
+    default it keeps the caller's order.  Through the C ABI both give the same contact pair set and the
     same substeps up to FP32 summation order (every vertex but at most 1% within 1e-4, none
     beyond 5e-3: a contact on the edge of its switch can decide differently, as the oracle
     itself does in another numbering, test_oracle_order.py), and the order is a permutation
@@ -726,11 +726,11 @@ def test_vertex_renumbering_is_invisible_to_the_caller():
     v0[:sc.n_dyn, 1] = -4.0
     x0 = sc.verts.copy()
     x0[:sc.n_dyn, 1] -= x0[:sc.n_dyn, 1].min() - 0.03
-    hr = B.Handle(sc)
+    hi = B.Handle(sc)
     old = os.environ.get("ADMM_B200_RENUMBER")
-    os.environ["ADMM_B200_RENUMBER"] = "0"
+    os.environ["ADMM_B200_RENUMBER"] = "1"
     try:
-        hi = B.Handle(sc)
+        hr = B.Handle(sc)
     finally:
         if old is None:
             del os.environ["ADMM_B200_RENUMBER"]
