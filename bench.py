@@ -95,12 +95,20 @@ def make_scene(args, rank=0, only=None):
     sc.params.ell_lanes = args.ell_lanes
     sc.params.pcg_iter = args.pcg_iter
     sc.params.query_lanes = args.query_lanes
+    if args.semantics == "cpu":
+        # the reference CPU backend's solver: damped system, exact global solve (the GPU arm:
+        # PCG with --pcg-iter iterations), serial Gauss-Seidel contact, CPU contact predicates
+        sc.params.backend_semantics = 1
+        sc.params.contact_semantics = 1
     return sc
 
 
-def metric_name(tol, cap, arm):
+def metric_name(tol, cap, arm, semantics="gpu"):
     how = {"learned": "learned global step (Jacobi fallback)", "jacobi": "plain Jacobi",
            "pcg": "PCG diag(A)"}[arm]
+    if semantics == "cpu":
+        how = ("the CPU backend's solver (damped system, exact global solve, serial Gauss-Seidel contact)"
+               if arm == "jacobi" else f"the CPU backend's solver with {how} as the global step")
     if tol > 0:
         return f"sim steps/s to ADMM residual {tol:g}: {how}, cap {cap} ADMM iterations = reference count"
     return f"sim steps/s: {how}, fixed {cap} ADMM iterations = reference count"
@@ -217,7 +225,7 @@ def oracle_sample_rate(args, rank, frames, budget_s):
     """The oracle (FP32 restatement of the reference GPU-backend algorithm, plain Jacobi, all
     host threads) over frames 0.. of the workload, stopping once budget_s of CPU time is spent;
     for the batch a size-stratified 16-body sample scaled to the whole batch by its work share.
-    Returns (steps/s, threads, description)."""
+    Returns (steps/s, threads, description, ADMM iteration cap)."""
     from oracle import oracle as O
     from parallel_admm_b200 import backend as B
     frac = 1.0
@@ -237,6 +245,8 @@ def oracle_sample_rate(args, rank, frames, budget_s):
         sc = make_scene(args, rank)
     holder = B.DescHolder(sc, residual_tol=args.tol, global_solver=0)
     o = O.Oracle(holder, double=False)
+    if args.semantics == "cpu":
+        what += "; the CPU backend's semantics (damped system solved exactly by an FP64 Cholesky, serial Gauss-Seidel contact)"
     secs, k, iters = 0.0, 0, 0
     for _ in range(frames):
         t = time.perf_counter()
@@ -248,7 +258,7 @@ def oracle_sample_rate(args, rank, frames, budget_s):
     rate = k / (secs / frac)
     desc = (f"{what}; frames 0..{k - 1} ({secs:.1f} s of CPU time), mean {iters / max(k, 1):.1f} ADMM iterations "
             f"per step, oracle FP32, OpenMP")
-    return rate, O.num_threads(), desc
+    return rate, O.num_threads(), desc, sc.params.admm_max_iter
 
 
 def run_reference(args):
@@ -256,9 +266,9 @@ def run_reference(args):
     if rank != 0:
         return 0
     frames = args.start_frame + min(args.steps, args.ref_steps)
-    rate, cores, desc = oracle_sample_rate(args, 0, frames, budget_s=args.ref_budget)
+    rate, cores, desc, cap = oracle_sample_rate(args, 0, frames, budget_s=args.ref_budget)
     line = {
-        "impl": "reference", "metric": metric_name(args.tol, 30, "jacobi"),
+        "impl": "reference", "metric": metric_name(args.tol, cap, "jacobi", args.semantics),
         "value": rate, "unit": "steps/s", "n_gpus": args.gpus, "steps": min(args.steps, args.ref_steps),
         "warmup": 0, "ms_per_step": 1e3 / rate, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -412,6 +422,10 @@ def main():
                     help="open a CUDA profiler range (cudaProfilerStart/Stop) around the first N timed steps, "
                          "for ncu --profile-from-start off")
     ap.add_argument("--phase-steps", type=int, default=10, help="substeps of the phase-probe pass (roofline)")
+    ap.add_argument("--semantics", default="gpu", choices=["gpu", "cpu"],
+                    help="the reference backend whose solver runs: the GPU backend's (default) or the CPU "
+                         "backend's (damping, exact global solve, serial Gauss-Seidel contact; with "
+                         "--solver pcg --pcg-iter N on the GPU)")
     ap.add_argument("--profile-only", action="store_true",
                     help="profiling run: the --solver arm's warm-up and --start-frame substeps, then --profile-steps "
                          "substeps inside a CUDA profiler range; no timing, no JSON line")
@@ -537,7 +551,7 @@ def main():
             traffic = json.load(f).get(args.config, {}).get(pk)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        rate, cores, desc = oracle_sample_rate(args, rank, args.start_frame + args.steps, args.cpu_budget)
+        rate, cores, desc, _ = oracle_sample_rate(args, rank, args.start_frame + args.steps, args.cpu_budget)
         cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port", "sample": desc}
     tn, gm = h.tuning(), h.global_mode()
     tuned = {"jacobi_lanes": tn["jacobi_lanes"], "rhs_lanes": tn["rhs_lanes"], "global_mode": gm["mode"]}
@@ -552,7 +566,7 @@ def main():
         cfg["plain_jacobi"] = pj
         cfg["learned_over_plain"] = main_r["value"] / pj["steps_per_s"] if pj["steps_per_s"] else None
     line = {
-        "metric": metric_name(args.tol, sc.params.admm_max_iter, args.solver),
+        "metric": metric_name(args.tol, sc.params.admm_max_iter, args.solver, args.semantics),
         "value": main_r["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": main_r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "config": cfg,
