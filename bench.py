@@ -77,7 +77,11 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-WEIGHTS = os.path.join(ROOT, "parallel_admm_b200", "weights", "learned_step.npz")
+WEIGHTS_DIR = os.path.join(ROOT, "parallel_admm_b200", "weights")
+# the trained learned step of each workload's family (train_learned.py --family ...)
+WEIGHTS = {"batch": "learned_step.npz", "batch_prof": "learned_step.npz", "cube": "learned_step_cube.npz",
+           "sheets": "learned_step_sheets.npz", "sheets_small": "learned_step_sheets.npz",
+           "cloth": "learned_step_sheets.npz"}
 
 
 def make_scene(args, rank=0, only=None):
@@ -400,7 +404,8 @@ def main():
     ap.add_argument("--config", default="batch", choices=sorted(CONFIGS))
     ap.add_argument("--solver", default="learned", choices=["learned", "jacobi", "pcg"],
                     help="the arm reported as value; with learned, plain Jacobi runs beside it")
-    ap.add_argument("--weights", default=WEIGHTS, help="trained learned-step weights (npz)")
+    ap.add_argument("--weights", default=None,
+                    help="trained learned-step weights (npz; default: the model of the workload's family)")
     ap.add_argument("--learned-sweeps", type=int, default=10, help="sweeps of the untrained learned step")
     ap.add_argument("--probe", default="jacobi", choices=["local", "jacobi", "rhs"])
     ap.add_argument("--tol", type=float, default=1e-4, help="ADMM residual tolerance (0 = fixed iteration count)")
@@ -430,6 +435,8 @@ def main():
                     help="profiling run: the --solver arm's warm-up and --start-frame substeps, then --profile-steps "
                          "substeps inside a CUDA profiler range; no timing, no JSON line")
     args = ap.parse_args()
+    if args.weights is None:
+        args.weights = os.path.join(WEIGHTS_DIR, WEIGHTS[args.config])
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
