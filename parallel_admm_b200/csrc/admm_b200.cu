@@ -1344,7 +1344,6 @@ int setup_grid(AdmmB200* h, const AdmmB200Desc* d) {
     TRY(dalloc(h, &g.ent_lo, g.cap));
     TRY(dalloc(h, &g.ent_up, g.cap));
     TRY(dalloc(h, &g.ent_key, g.cap));
-    TRY(dalloc(h, &g.ent_ids, g.cap));
     TRY(dalloc(h, &g.ctr, 4));
     TRY(dalloc(h, &g.big_tri, std::max(s.nst, 1)));
     TRY(dalloc(h, &g.big_edge, std::max(s.nse, 1)));

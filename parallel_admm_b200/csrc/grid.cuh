@@ -11,11 +11,9 @@
 // Layout: every surface triangle and edge whose box spans at most kGridMaxSpan
 // cells per axis is inserted into each cell it overlaps, in a hash table of
 // (cell, type) buckets built by count -> scan -> scatter; each entry carries
-// the element's box, the key of the cell it was entered for (other cells sharing
-// the bucket are rejected by one 8-byte compare) and the element's vertices (an
-// element sharing a vertex with the query is rejected before the narrow phase,
-// which would reject it after loading its indices: about half of the candidates
-// that pass the box test on a tet surface), so the tests need no further load.  Larger
+// the element's box and the key of the cell it was entered for, so that other
+// cells sharing the bucket are rejected by one 8-byte compare and the box test
+// needs no further load.  Larger
 // elements (and any that do not fit the entry capacity) go to a per-type "big"
 // list that the queries scan directly.
 //
@@ -168,14 +166,6 @@ __global__ void __launch_bounds__(256) k_grid_scatter(DevScene s) {
     int3 a, b;
     grid_range(lo, up, g.inv_c, a, b);
     lo.w = __int_as_float(id);
-    int4 ids;
-    if (type == 0) {
-        const int4 t = s.st[id];
-        ids = make_int4(t.x, t.y, t.z, -1);
-    } else {
-        const int2 e = s.se[id];
-        ids = make_int4(e.x, e.y, -1, -1);
-    }
     grid_for_cells(a, b, type, g.hmask, [&](int4 c, int bk) {
         const int pos = g.start[bk] + atomicSub(&g.cnt[bk], 1) - 1;
         // w of up: for each axis, whether this cell is the element's first
@@ -183,7 +173,6 @@ __global__ void __launch_bounds__(256) k_grid_scatter(DevScene s) {
         g.ent_lo[pos] = lo;
         g.ent_up[pos] = make_float4(up.x, up.y, up.z, __int_as_float(first));
         g.ent_key[pos] = grid_cell_key(c.x, c.y, c.z);
-        g.ent_ids[pos] = ids;
     });
 }
 
@@ -309,12 +298,10 @@ ADMM_DEV void grid_queue_drain(const QueryGroup<G>& grp, GridQueue& q, F& narrow
 // against the triangles.  Edge query: edge e with box [lo, up] against grid
 // edges with a larger index (grid edge e), every big edge (grid edge e) or big
 // edges with a larger index (big edge e).  Grid part: the cells of the query's
-// range, or every grid element of the type when the range is too large.  qa, qb:
-// the query's vertices (qb = -2 for a vertex query), for the adjacency test of
-// grid entries.
+// range, or every grid element of the type when the range is too large.
 template <int G, class F>
-ADMM_DEV void grid_walk(const DevScene& s, const QueryGroup<G>& grp, bool vf, int e, int qa, int qb, float4 lo,
-                        float4 up, GridQueue& q, F& narrow) {
+ADMM_DEV void grid_walk(const DevScene& s, const QueryGroup<G>& grp, bool vf, int e, float4 lo, float4 up,
+                        GridQueue& q, F& narrow) {
     const GridDev& g = s.grid;
     const float gap = s.thickness;
     const int sub = grp.sub;
@@ -363,15 +350,11 @@ ADMM_DEV void grid_walk(const DevScene& s, const QueryGroup<G>& grp, bool vf, in
                         const unsigned long long ek = g.ent_key[ent];
                         const float4 eup = g.ent_up[ent];
                         const float4 elo = g.ent_lo[ent];
-                        const int4 eid = g.ent_ids[ent];
                         partner = __float_as_int(elo.w);
-                        const bool adjacent = qa == eid.x || qa == eid.y || qa == eid.z || qb == eid.x ||
-                                              qb == eid.y || qb == eid.z;
                         // same cell (not another of the bucket); larger edge index; once per pair:
-                        // this cell is the first of the query's or of the element's range on every axis;
-                        // no shared vertex
+                        // this cell is the first of the query's or of the element's range on every axis
                         ok = ek == kj && (vf || partner > e) && ((fj | __float_as_int(eup.w)) & 7) == 7 &&
-                             !adjacent && (s.cpu_contact || box_overlap(lo, up, elo, eup, gap));
+                             (s.cpu_contact || box_overlap(lo, up, elo, eup, gap));
                     }
                     grid_queue_push(grp, q, ok, partner, narrow);
                 }
@@ -546,18 +529,13 @@ ADMM_DEV void grid_query(DevScene& s) {
     if (q >= s.nsv + s.nse) return;  // whole groups leave together
     const bool vf = q < s.nsv;
     const int e = q - s.nsv;
-    int v = 0, qa, qb;
+    int v = 0;
     float4 lo, up;
     if (vf) {
         v = s.sv[q];
         lo = up = s.x[v];
-        qa = v;
-        qb = -2;
     } else {
         lo = edge_box_lo(s, e, up);
-        const int2 ed = s.se[e];
-        qa = ed.x;
-        qb = ed.y;
     }
     GridQueue gq{qbuf + 2 * (threadIdx.x - grp.sub), 0};
     int* qh = s.grid.qhits + (size_t)q * kQueryHitsMax;
@@ -572,7 +550,7 @@ ADMM_DEV void grid_query(DevScene& s) {
             if (hit && k < kQueryHitsMax) qh[k] = partner;
             nhit += __popc(m);
         };
-        grid_walk(s, grp, vf, e, qa, qb, lo, up, gq, narrow);
+        grid_walk(s, grp, vf, e, lo, up, gq, narrow);
         if (grp.sub == 0) s.qcount[q] = nhit;
         return;
     }
@@ -604,7 +582,7 @@ ADMM_DEV void grid_query(DevScene& s) {
         }
         nhit += __popc(m);
     };
-    grid_walk(s, grp, vf, e, qa, qb, lo, up, gq, emit);
+    grid_walk(s, grp, vf, e, lo, up, gq, emit);
     __syncwarp(grp.mask);
     if (grp.sub == 0) {
         const int end = min(base + total, s.cap);

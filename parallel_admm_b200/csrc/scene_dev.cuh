@@ -71,7 +71,6 @@ struct GridDev {
     float4* ent_lo = nullptr;      // [cap] element box lo, w = element index (int bits)
     float4* ent_up = nullptr;      // [cap] element box up, w = first-cell bits (x 1, y 2, z 4)
     unsigned long long* ent_key = nullptr;  // [cap] key of the cell the entry was made for
-    int4* ent_ids = nullptr;       // [cap] vertices of the entry's element (-1 padded)
     int* ctr = nullptr;            // [4] entries reserved, big triangles, big edges
     int* big_tri = nullptr;        // [n surface triangles]
     int* big_edge = nullptr;       // [n surface edges]
