@@ -92,8 +92,10 @@ __global__ void __launch_bounds__(kVertThreads) k_rhs_learn(DevScene s, LearnDev
 // sweep (FIRST) also writes the block partials of |b - A x_0|^2 into L.part[0..) and of
 // |b|^2 into L.part[2 blocks..), and, outside the substep's first global step (extrap),
 // of |b - A x_c|^2 into L.part_c, A x_c from L.ax.
+// The sweep and the judge's pass are capped at 40 registers (12 blocks per SM) for the same
+// reason as k_jacobi (batch: 65.4 -> 56.0 us per learned sweep in the step graph).
 template <int T, bool FIRST>
-__global__ void __launch_bounds__(kVertThreads) k_lsweep(DevScene s, LearnDev L, const float4* __restrict__ src,
+__global__ void __launch_bounds__(kVertThreads, 12) k_lsweep(DevScene s, LearnDev L, const float4* __restrict__ src,
                                                          const float4* __restrict__ prev, float4* __restrict__ dst,
                                                          float omega, float beta, int extrap) {
     ADMM_PDL_TRIGGER();
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(kVertThreads) k_lsweep(DevScene s, LearnDev L,
 // The judge's pass over x (= x_K, or the plain solve's result in a fallback): block
 // partials of |b - A x|^2 into L.part[blocks..) and L.ax <- A x.
 template <int T>
-__global__ void __launch_bounds__(kVertThreads) k_ljudge(DevScene s, LearnDev L) {
+__global__ void __launch_bounds__(kVertThreads, 12) k_ljudge(DevScene s, LearnDev L) {
     ADMM_PDL_TRIGGER();
     __shared__ double sh[kVertThreads / 32];
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
