@@ -419,8 +419,9 @@ int  admm_gnn_backward(AdmmGnn* g, const float* gm, const float* gtheta, float* 
  * diagonal).  admm_learn_loss_grad runs K sweeps of the learned global step from
  * the warm start x_c + theta (x_c - x_l) on each of nsamp samples (b, x_c, x_l, x*:
  * host, nsamp x n x 3, x* the converged solution of A x = b) and returns the mean
- * of |x_K - x*|_A^2 / |x_c - x*|_A^2 and its gradients with respect to omega, beta
- * (K each), m and theta (n each); any gradient pointer may be NULL.
+ * of |x_K - x*|_A^2 / |x_c - x*|_A^2 (+ mu |b - A x_K|^2 / |b - A x_c|^2 after
+ * admm_learn_set_residual_weight, mu = 0 by default) and its gradients with respect to
+ * omega, beta (K each), m and theta (n each); any gradient pointer may be NULL.
  * admm_learn_solve: conjugate gradients (diag(A) preconditioner) from x (host, in
  * and out) until |r|_{D^-1} <= rel_tol |r_0|_{D^-1} or max_iter iterations. */
 typedef struct AdmmLearn AdmmLearn;
@@ -432,6 +433,7 @@ int  admm_learn_loss_grad(AdmmLearn* L, int K, const float* omega, const float* 
                           const float* x_star, double* loss, float* g_omega, float* g_beta, float* g_m,
                           float* g_theta);
 int  admm_learn_solve(AdmmLearn* L, const float* b, float* x, double rel_tol, int max_iter, int* iters);
+int  admm_learn_set_residual_weight(AdmmLearn* L, double mu);
 
 /* The global-step matrix A of a handle: nnz of the off-diagonal part when start
  * is NULL, else its CSR (start[n_dyn+1], col, val) and diagonal (host). */

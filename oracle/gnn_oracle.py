@@ -204,10 +204,12 @@ def sweeps(m, th, omega, beta, start, col, val, adiag, b, xc, xl):
     return X, Rs
 
 
-def sweeps_loss_grad(m, th, omega, beta, start, col, val, adiag, samples):
-    """Mean over samples (b, x_c, x_l, x*) of |x_K - x*|_A^2 / |x_c - x*|_A^2 and its
-    gradients (omega, beta, m, theta).  Adjoint (A symmetric):
-        g_K = 2 A (x_K - x*) / E_c,
+def sweeps_loss_grad(m, th, omega, beta, start, col, val, adiag, samples, mu=0.0):
+    """Mean over samples (b, x_c, x_l, x*) of |x_K - x*|_A^2 / |x_c - x*|_A^2
+    + mu |b - A x_K|^2 / |b - A x_c|^2 and its gradients (omega, beta, m, theta).  The second
+    term (the residual that the judge checks; b - A x = -A (x - x*)) is off by default.
+    Adjoint (A symmetric):
+        g_K = 2 A (x_K - x*) / E_c + mu 2 A A (x_K - x*) / R_c,
         g_k = (1 + beta_k) g_{k+1} - omega_k A (m g_{k+1}) - beta_{k+1} g_{k+2},
         dL/domega_k = g_{k+1} . m r_k,  dL/dbeta_k = g_{k+1} . (x_k - x_{k-1}) (k >= 1),
         dL/dm_i = sum_k omega_k g_{k+1,i} . r_{k,i},  dL/dtheta_i = g_{0,i} . (x_c - x_l)_i."""
@@ -218,15 +220,20 @@ def sweeps_loss_grad(m, th, omega, beta, start, col, val, adiag, samples):
     S = len(samples)
     for (b, xc, xl, xs) in samples:
         ec = xc - xs
-        Ec = np.sum(ec * spmv(start, col, val, adiag, ec))
+        Aec = spmv(start, col, val, adiag, ec)
+        Ec = np.sum(ec * Aec)
         if not Ec > 0:
             continue
+        Rc = np.sum(Aec * Aec)
         X, Rs = sweeps(m, th, omega, beta, start, col, val, adiag, b, xc, xl)
         eK = X[K] - xs
         AeK = spmv(start, col, val, adiag, eK)
         loss += np.sum(eK * AeK) / Ec / S
         g = [None] * (K + 2)
         g[K] = 2.0 * AeK / Ec / S
+        if mu > 0.0 and Rc > 0.0:
+            loss += mu * np.sum(AeK * AeK) / Rc / S
+            g[K] = g[K] + mu * 2.0 * spmv(start, col, val, adiag, AeK) / Rc / S
         for k in range(K - 1, -1, -1):
             bk = beta[k] if k > 0 else 0.0
             gk = (1.0 + bk) * g[k + 1] - omega[k] * spmv(start, col, val, adiag, m[:, None] * g[k + 1])

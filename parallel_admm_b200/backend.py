@@ -241,6 +241,7 @@ def exported_symbols():
         "admm_gnn_set_params", "admm_gnn_get_params", "admm_gnn_forward", "admm_gnn_loss_grad", "admm_gnn_adam",
         "admm_b200_set_learned", "admm_b200_learned_stats", "admm_b200_record_global", "admm_gnn_outputs",
         "admm_gnn_backward", "admm_learn_create", "admm_learn_destroy", "admm_learn_loss_grad", "admm_learn_solve",
+        "admm_learn_set_residual_weight",
         "admm_b200_vertex_order",
     ]
 

@@ -4,12 +4,13 @@
 //     x_0 = x_c + theta (x_c - x_l),
 //     x_{k+1} = x_k + omega_k m (b - A x_k) + beta_k (x_k - x_{k-1})   (beta_0 = 0),
 //
-// L = (x_K - x*)^T A (x_K - x*) / ((x_c - x*)^T A (x_c - x*)), averaged over
-// samples (b, x_c, x_l, x*) that plain runs produce, and its gradient with
+// L = (x_K - x*)^T A (x_K - x*) / ((x_c - x*)^T A (x_c - x*))
+//     + mu |b - A x_K|^2 / |b - A x_c|^2   (mu = 0 unless set: the residual the judge checks),
+// averaged over samples (b, x_c, x_l, x*) that plain runs produce, and its gradient with
 // respect to omega, beta (per sweep), m and theta (per vertex) by the adjoint
-// recursion (A symmetric):
+// recursion (A symmetric, b - A x = -A (x - x*)):
 //
-//     g_K = 2 A (x_K - x*) / E_c,
+//     g_K = 2 A (x_K - x*) / E_c + mu 2 A A (x_K - x*) / R_c,
 //     g_k = (1 + beta_k) g_{k+1} - omega_k A (m g_{k+1}) - beta_{k+1} g_{k+2},
 //     dL/domega_k = g_{k+1} . m r_k,   dL/dbeta_k = g_{k+1} . (x_k - x_{k-1}),
 //     dL/dm_i = sum_k omega_k g_{k+1,i} . r_{k,i},   dL/dtheta_i = g_{0,i} . (x_c - x_l)_i.
@@ -108,10 +109,29 @@ __global__ void k_t_anorm2(const int* __restrict__ start, const int* __restrict_
     if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
-// v = s * v
-__global__ void k_t_scale(float* __restrict__ v, size_t cnt, const double* __restrict__ s) {
+// block partials of v . v
+__global__ void k_t_sq(const float* __restrict__ v, size_t cnt, double* __restrict__ part) {
+    __shared__ double sh[kT];
+    double acc = 0.0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += (size_t)gridDim.x * blockDim.x)
+        acc += (double)v[t] * (double)v[t];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// g = s1 a (+ s2 c when c is given)
+__global__ void k_t_seed(float* __restrict__ g, const float* __restrict__ a, const float* __restrict__ c, size_t cnt,
+                         double s1, double s2) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < cnt) v[t] = (float)((double)v[t] * s[0]);
+    if (t >= cnt) return;
+    double v = (double)a[t] * s1;
+    if (c) v += (double)c[t] * s2;
+    g[t] = (float)v;
 }
 
 // One adjoint step k: gk = (1 + beta_k) g1 - omega_k A (m g1) - beta_{k+1} g2 (g2 may be
@@ -264,6 +284,8 @@ struct AdmmLearn {
     float* X = nullptr;  // [(kMaxK + 1) * 3n] iterates
     float* Rk = nullptr; // [kMaxK * 3n] residuals
     float *g[3] = {nullptr, nullptr, nullptr}, *e = nullptr, *ae = nullptr;
+    float* a2e = nullptr;  // A A e for the residual term
+    double mu = 0.0;       // weight of the residual term
     float *gm = nullptr, *gth = nullptr;
     float *cr = nullptr, *cp = nullptr, *cq = nullptr;
     double* part = nullptr;  // [3 * kParts]
@@ -314,6 +336,7 @@ int admm_learn_create(int n, const int32_t* start, const int32_t* col, const flo
         (rc = lalloc(L, &L->xs, N3)) || (rc = lalloc(L, &L->X, (kMaxK + 1) * N3)) ||
         (rc = lalloc(L, &L->Rk, kMaxK * N3)) || (rc = lalloc(L, &L->g[0], N3)) || (rc = lalloc(L, &L->g[1], N3)) ||
         (rc = lalloc(L, &L->g[2], N3)) || (rc = lalloc(L, &L->e, N3)) || (rc = lalloc(L, &L->ae, N3)) ||
+        (rc = lalloc(L, &L->a2e, N3)) ||
         (rc = lalloc(L, &L->gm, n)) || (rc = lalloc(L, &L->gth, n)) || (rc = lalloc(L, &L->cr, N3)) ||
         (rc = lalloc(L, &L->cp, N3)) || (rc = lalloc(L, &L->cq, N3)) || (rc = lalloc(L, &L->part, 3 * kParts))) {
         admm_learn_destroy(L);
@@ -376,6 +399,12 @@ int admm_learn_loss_grad(AdmmLearn* L, int K, const float* omega, const float* b
         if (int rc = sum_parts(L, L->part, kParts, &Ec)) return rc;
         if (!(Ec > 0.0)) continue;
         used++;
+        // R_c = |A (xc - x*)|^2 = |b - A xc|^2
+        double Rc = 0.0;
+        if (L->mu > 0.0) {
+            k_t_sq<<<kParts, kT, 0, st>>>(L->ae, N3, L->part);
+            if (int rc = sum_parts(L, L->part, kParts, &Rc)) return rc;
+        }
         // forward
         k_t_init<<<gb, kT, 0, st>>>(L->xc, L->xl, L->th, n, L->X);
         for (int k = 0; k < K; k++) {
@@ -389,12 +418,19 @@ int admm_learn_loss_grad(AdmmLearn* L, int K, const float* omega, const float* b
         double EK = 0.0;
         if (int rc = sum_parts(L, L->part, kParts, &EK)) return rc;
         total += EK / Ec;
-        // adjoint: g_K = 2 A e_K / (E_c nsamp), in g[K % 3]
+        // adjoint: g_K = 2 A e_K / (E_c nsamp) (+ mu 2 A A e_K / (R_c nsamp)), in g[K % 3]
         const double sc = 2.0 / (Ec * nsamp);
-        cudaMemcpyAsync(L->part + 2 * kParts, &sc, sizeof(double), cudaMemcpyHostToDevice, st);
         float* gK = L->g[K % 3];
-        cudaMemcpyAsync(gK, L->ae, sizeof(float) * N3, cudaMemcpyDeviceToDevice, st);
-        k_t_scale<<<nblk(N3, kT), kT, 0, st>>>(gK, N3, L->part + 2 * kParts);
+        if (L->mu > 0.0 && Rc > 0.0) {
+            double RK = 0.0;
+            k_t_sq<<<kParts, kT, 0, st>>>(L->ae, N3, L->part);
+            if (int rc = sum_parts(L, L->part, kParts, &RK)) return rc;
+            total += L->mu * RK / Rc;
+            k_t_anorm2<<<kParts, kT, 0, st>>>(L->start, L->col, L->val, L->diag, L->ae, n, L->a2e, L->part);
+            k_t_seed<<<nblk(N3, kT), kT, 0, st>>>(gK, L->ae, L->a2e, N3, sc, L->mu * 2.0 / (Rc * nsamp));
+        } else {
+            k_t_seed<<<nblk(N3, kT), kT, 0, st>>>(gK, L->ae, nullptr, N3, sc, 0.0);
+        }
         for (int k = K - 1; k >= 0; k--) {
             const float* g1 = L->g[(k + 1) % 3];
             const float* g2 = k + 2 <= K ? L->g[(k + 2) % 3] : nullptr;
@@ -426,6 +462,12 @@ int admm_learn_loss_grad(AdmmLearn* L, int K, const float* omega, const float* b
     if (g_m && cudaMemcpy(g_m, L->gm, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess) return ADMM_ERR_CUDA;
     if (g_theta && cudaMemcpy(g_theta, L->gth, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
         return ADMM_ERR_CUDA;
+    return ADMM_OK;
+}
+
+int admm_learn_set_residual_weight(AdmmLearn* L, double mu) {
+    if (!L || !(mu >= 0.0) || !std::isfinite(mu)) return ADMM_ERR_INVALID;
+    L->mu = mu;
     return ADMM_OK;
 }
 

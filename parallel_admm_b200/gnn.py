@@ -52,6 +52,7 @@ def _lib():
             "admm_learn_loss_grad": (ctypes.c_int, [vp, ctypes.c_int, _f, _f, _f, _f, ctypes.c_int, _f, _f, _f, _f,
                                                     _d, _f, _f, _f, _f]),
             "admm_learn_solve": (ctypes.c_int, [vp, _f, _f, ctypes.c_double, ctypes.c_int, _i]),
+            "admm_learn_set_residual_weight": (ctypes.c_int, [vp, ctypes.c_double]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -298,13 +299,17 @@ class LearnedPreconditioner:
 class SweepTrainer:
     """GPU context of the learned global step's training on one system (learn.cu)."""
 
-    def __init__(self, sysm: System):
+    def __init__(self, sysm: System, residual_weight: float = 0.0):
         self.sysm = sysm
         self.L = vp()
         rc = _lib().admm_learn_create(sysm.n, _p(sysm.start, _i), _p(sysm.col, _i), _p(sysm.val, _f),
                                       _p(sysm.diag, _f), ctypes.byref(self.L))
         if rc != B.OK:
             raise B.AdmmError(rc, "admm_learn_create")
+        if residual_weight:
+            rc = _lib().admm_learn_set_residual_weight(self.L, float(residual_weight))
+            if rc != B.OK:
+                raise B.AdmmError(rc, "admm_learn_set_residual_weight")
 
     def close(self):
         if self.L:
@@ -328,8 +333,8 @@ class SweepTrainer:
         return x, it.value
 
     def loss_grad(self, omega, beta, m, theta, b, xc, xl, xs):
-        """Mean |x_K - x*|_A^2 / |x_c - x*|_A^2 over the samples and its gradients
-        (omega, beta, m, theta)."""
+        """Mean |x_K - x*|_A^2 / |x_c - x*|_A^2 (+ residual_weight |b - A x_K|^2 / |b - A x_c|^2)
+        over the samples and its gradients (omega, beta, m, theta)."""
         K = len(omega)
         om = np.ascontiguousarray(omega, np.float32)
         be = np.ascontiguousarray(beta, np.float32)

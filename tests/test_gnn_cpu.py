@@ -1,6 +1,7 @@
 """The learned preconditioner's CPU restatement: gradients against finite differences, and the
 package's feature builder against it (no GPU)."""
 import numpy as np
+import pytest
 
 from oracle import gnn_oracle as G
 from parallel_admm_b200 import gnn
@@ -88,9 +89,11 @@ def _samples(start, col, val, adiag, rng, k=2):
     return out
 
 
-def test_learned_step_adjoint_matches_finite_differences():
+@pytest.mark.parametrize("mu", [0.0, 0.7])
+def test_learned_step_adjoint_matches_finite_differences(mu):
     """Gradients of the unrolled learned sweeps (omega, beta, m, theta) by the adjoint
-    recursion against central differences of the FP64 loss."""
+    recursion against central differences of the FP64 loss, without and with the residual
+    term mu |b - A x_K|^2 / |b - A x_c|^2."""
     start, col, val, adiag, rng = _graph(n=14, seed=5)
     n = len(adiag)
     K = 5
@@ -99,12 +102,12 @@ def test_learned_step_adjoint_matches_finite_differences():
     m = rng.uniform(0.7, 1.3, n) / adiag
     th = rng.uniform(-0.5, 0.8, n)
     S = _samples(start, col, val, adiag, rng)
-    loss, go, gb, gm, gt = G.sweeps_loss_grad(m, th, omega, beta, start, col, val, adiag, S)
+    loss, go, gb, gm, gt = G.sweeps_loss_grad(m, th, omega, beta, start, col, val, adiag, S, mu=mu)
     assert loss > 0
     eps = 1e-6
 
     def f(o=omega, b=beta, mm=m, t=th):
-        return G.sweeps_loss_grad(mm, t, o, b, start, col, val, adiag, S)[0]
+        return G.sweeps_loss_grad(mm, t, o, b, start, col, val, adiag, S, mu=mu)[0]
 
     for k in range(K):
         for arr, grad in ((omega, go), (beta, gb)):

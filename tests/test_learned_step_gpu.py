@@ -153,12 +153,15 @@ def _samples(h, sysm, tr, count=3, iters=(3, 7, 12)):
     return S
 
 
-def test_training_gradients_match_the_restatement():
+@pytest.mark.parametrize("mu", [0.0, 0.5])
+def test_training_gradients_match_the_restatement(mu):
+    """The GPU loss and gradients of the unrolled sweeps (learn.cu) against the FP64
+    restatement, without and with the residual term of weight mu."""
     sc, x0, v0 = _impact_cube(6, seed=2)
     h = B.Handle(sc)
     h.set_state(x0, v0)
     sysm = gnn.system(h)
-    tr = gnn.SweepTrainer(sysm)
+    tr = gnn.SweepTrainer(sysm, residual_weight=mu)
     S = _samples(h, sysm, tr)
     assert np.abs(S[1] - S[2]).max() > 0  # x_cur and x_last differ
     om, be, m, th = _schedule(sysm, K=6, seed=3)
@@ -166,7 +169,7 @@ def test_training_gradients_match_the_restatement():
     d = lambda a: np.asarray(a, np.float64)
     samples = [tuple(d(a[k]) for a in S) for k in range(S[0].shape[0])]
     lo, go_, gb_, gm_, gt_ = G.sweeps_loss_grad(d(m), d(th), d(om), d(be), sysm.start, sysm.col, d(sysm.val),
-                                                d(sysm.diag), samples)
+                                                d(sysm.diag), samples, mu=mu)
     assert abs(loss - lo) <= 1e-3 * abs(lo), (loss, lo)
     for a, b_ in ((go, go_), (gb, gb_), (gm, gm_), (gt, gt_)):
         assert np.linalg.norm(a - b_) <= 2e-3 * np.linalg.norm(b_), np.linalg.norm(a - b_) / np.linalg.norm(b_)
