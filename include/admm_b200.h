@@ -348,7 +348,7 @@ int  admm_b200_tuning(AdmmB200* h, int* lanes_a, int* lanes_r, float* ms_a, floa
  * vertex) for global_solver 2, e.g. the output of the learned preconditioner.
  * No reference counterpart. */
 int  admm_b200_set_preconditioner(AdmmB200* h, const float* blocks9, int nd);
-/* --- learned global step (global_solver 3; north-star addition, no reference
+/* --- learned global step (global_solver 3; an addition with no reference
  * counterpart).  Replaces the jacobi_iter sweeps of cu_jacobi_global
  * (jacobi_solver.cu:141-180, called from admm_impl_gpu.cu:364) by `sweeps`
  * second-order sweeps
@@ -382,7 +382,7 @@ int  admm_b200_record_global(AdmmB200* h, int iteration, float* b, float* x_cur,
  * kernel per sweep and with the persistent kernel (0 when not timed). */
 int  admm_b200_global_mode(AdmmB200* h, int* persistent, int* blocks, float* ms_sweeps, float* ms_persist);
 
-/* --- learned block preconditioner (north-star addition, no reference counterpart) ---
+/* --- learned block preconditioner (an addition with no reference counterpart) ---
  * A 3-layer message-passing network (width 64) over the graph of the global
  * matrix A predicts per dynamic vertex a 3x3 SPD block B_i = L_i L_i^T / a_ii
  * for admm_b200_set_preconditioner (global_solver 2); o = 0 gives diag(A)^-1.
@@ -414,7 +414,7 @@ int  admm_gnn_outputs(AdmmGnn* g, float* m, float* theta);
  * admm_gnn_adam applies it. */
 int  admm_gnn_backward(AdmmGnn* g, const float* gm, const float* gtheta, float* grad);
 
-/* --- training of the learned global step (north-star addition, no reference counterpart) ---
+/* --- training of the learned global step (an addition with no reference counterpart) ---
  * A context over one system A (off-diagonal CSR with start[n] entries, and the
  * diagonal).  admm_learn_loss_grad runs K sweeps of the learned global step from
  * the warm start x_c + theta (x_c - x_l) on each of nsamp samples (b, x_c, x_l, x*:

@@ -3,7 +3,7 @@ and its gradients.
 
 TEST INFRASTRUCTURE: only the tests use this module, as the checker of the CUDA forward
 and backward kernels in parallel_admm_b200/csrc/gnn.cu.  The network has no counterpart
-in the reference (a north-star addition).
+in the reference (an addition beyond it).
 
 Graph: the dynamic vertices, with the off-diagonal pattern of the global-step matrix A as
 directed edges (row i, column j: message j -> i).  Parameters, in this order (each weight

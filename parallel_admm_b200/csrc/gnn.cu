@@ -1,7 +1,7 @@
 // gnn.cu -- the learned per-vertex block preconditioner of the PCG global step:
 // a 3-layer message-passing network (width 64) over the graph of the global
 // matrix A, its loss and gradients, and an Adam update, all on the GPU with
-// the project's own kernels.  A north-star addition with no reference
+// the project's own kernels.  An addition with no reference
 // counterpart; the network and loss are specified in the header of the CPU
 // restatement that the tests check these kernels against.
 //

@@ -586,7 +586,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_global_persist(DevScene 
 
 // ---------------------------------------------------------------------------
 // Preconditioned conjugate gradients for the global step (global_solver > 0),
-// a north-star addition with no counterpart in the reference.  A (x) I3 is
+// an addition with no counterpart in the reference.  A (x) I3 is
 // solved for the three coordinate columns at once (one 3nd-vector CG, so that
 // a 3x3 block preconditioner may couple them), warm-started from the current x.
 // Chronopoulos-Gear form: one reduction pair per iteration, two kernels:

@@ -1,4 +1,4 @@
-// learn.cu -- training of the learned global step (north-star addition, no
+// learn.cu -- training of the learned global step (an addition with no
 // reference counterpart): the loss of K unrolled sweeps of
 //
 //     x_0 = x_c + theta (x_c - x_l),

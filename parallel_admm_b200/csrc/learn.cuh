@@ -1,4 +1,4 @@
-// learn.cuh -- the learned global step (global_solver 3), a north-star addition
+// learn.cuh -- the learned global step (global_solver 3), an addition
 // with no counterpart in the reference.  It replaces the jacobi_iter Jacobi sweeps
 // of an ADMM iteration (cu_jacobi_global, jacobi_solver.cu:141-180, called from
 // admm_impl_gpu.cu:364) by K sweeps of a second-order iteration

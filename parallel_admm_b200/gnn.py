@@ -1,6 +1,6 @@
 """Learned per-vertex block preconditioner for the PCG global step (global_solver 2).
 
-A north-star addition with no counterpart in the reference.  The network (3 message-passing
+An addition with no counterpart in the reference.  The network (3 message-passing
 layers of width 64 over the graph of the global matrix A) and its training run on the GPU in
 the library's own kernels (csrc/gnn.cu, C ABI ``admm_gnn_*``); this module builds the inputs,
 drives training and hands the predicted blocks to a solver handle:
