@@ -43,3 +43,15 @@ def test_fewer_than_three_warmup_steps_are_refused():
     r = _bench("--impl", "reference", "--steps", "2", "--warmup", "2", timeout=120)
     assert r.returncode == 2
     assert "--warmup must be >= 3" in r.stderr
+
+
+def test_reference_arm_with_the_cpu_backend_semantics():
+    """--semantics cpu: the reference arm times the oracle's restatement of the CPU backend
+    (damped system, exact FP64 Cholesky, serial Gauss-Seidel contact) and says so."""
+    r = _bench("--impl", "reference", "--config", "cloth", "--semantics", "cpu", "--tol", "0", "--steps", "3",
+               "--warmup", "3", timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads([l for l in r.stdout.splitlines() if l.strip()][0])
+    assert d["impl"] == "reference" and d["value"] > 0
+    assert "CPU backend's solver" in d["metric"] and "fixed 20 ADMM iterations" in d["metric"]
+    assert "Cholesky" in d["cpu_baseline"]["sample"]
